@@ -1,0 +1,240 @@
+// BitVoxel collision counting: map vs map, list vs map (single and batched),
+// list vs list.
+//
+// A BitVoxel<256> is 32 bytes.  Two adjacent lanes share one voxel, each
+// loading one 16-byte half, so a warp instruction reads 512 contiguous bytes.
+// DefaultCollider::collide(BitVoxel, BitVoxel) (GV/voxel/DefaultCollider.hpp:76-81)
+// is "both voxels hold a meaning other than eBVM_FREE" (BitVector::noneButEmpty,
+// GV/helpers/BitVector.h:184-198): OR the 8 words with bit 0 masked.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "gvx_internal.cuh"
+
+namespace gvx {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+int g_sms = 0;
+int sms() {
+  if (g_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms;
+}
+
+// Non-empty test of one 16-byte half; `low` marks the half holding bit 0.
+__device__ __forceinline__ uint32_t half_bits(uint4 v, bool low) {
+  return ((low ? (v.x & ~1u) : v.x) | v.y | v.z | v.w);
+}
+
+__device__ __forceinline__ void block_count_add(unsigned long long local, unsigned long long* dst) {
+  __shared__ unsigned long long s_sum;
+  if (threadIdx.x == 0) s_sum = 0ull;
+  __syncthreads();
+  local = __reduce_add_sync(kFull, (unsigned)local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(&s_sum, local);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_sum) atomicAdd(dst, s_sum);
+}
+
+// kernelCollideVoxelMapsDebug (GV/voxelmap/kernels/VoxelMapOperations.hpp:129-184):
+// count i where self[i+off] and other[i] collide; mark self with eBVM_COLLISION.
+__global__ void __launch_bounds__(256) bvm_collide_kernel(uint32_t* __restrict__ self, const uint32_t* __restrict__ other,
+                                                          uint64_t n, int64_t off, int mark,
+                                                          unsigned long long* __restrict__ count) {
+  const int lane = threadIdx.x & 31;
+  const bool low = (lane & 1) == 0;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  unsigned long long hits = 0;
+  constexpr int kUnroll = 4;
+  for (uint64_t base = gw * 16 * kUnroll; base < n; base += warps * 16 * kUnroll) {
+    uint4 a[kUnroll], b[kUnroll];
+    bool ok[kUnroll];
+    int64_t j[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const uint64_t i = base + u * 16 + (lane >> 1);
+      j[u] = (int64_t)i + off;
+      ok[u] = i < n && j[u] >= 0 && j[u] < (int64_t)n;
+      a[u] = make_uint4(0, 0, 0, 0);
+      b[u] = make_uint4(0, 0, 0, 0);
+      if (ok[u]) {
+        a[u] = __ldcs(reinterpret_cast<const uint4*>(self + (uint64_t)j[u] * kBitVoxelWords) + (lane & 1));
+        b[u] = __ldcs(reinterpret_cast<const uint4*>(other + i * kBitVoxelWords) + (lane & 1));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      uint32_t ma = half_bits(a[u], low), mb = half_bits(b[u], low);
+      ma |= __shfl_xor_sync(kFull, ma, 1);
+      mb |= __shfl_xor_sync(kFull, mb, 1);
+      const bool hit = ok[u] && ma != 0u && mb != 0u;
+      if (hit && low) {
+        ++hits;
+        if (mark) self[(uint64_t)j[u] * kBitVoxelWords] = a[u].x | (1u << kCollisionBit);
+      }
+    }
+  }
+  block_count_add(hits, count);
+}
+
+// kernelCollideWithVoxelMap (GV/voxellist/kernels/VoxelListOperations.hpp:146-197):
+// list entry k collides with map voxel ids[k] + off when that lies in the map.
+__global__ void __launch_bounds__(256) list_collide_map_kernel(const uint32_t* __restrict__ ids, uint32_t* __restrict__ lvox,
+                                                               uint64_t n, const uint32_t* __restrict__ map,
+                                                               uint64_t map_n, int64_t off, int mark,
+                                                               unsigned long long* __restrict__ count) {
+  const int lane = threadIdx.x & 31;
+  const bool low = (lane & 1) == 0;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  unsigned long long hits = 0;
+  for (uint64_t base = gw * 16; base < n; base += warps * 16) {
+    const uint64_t k = base + (lane >> 1);
+    bool ok = k < n;
+    int64_t j = 0;
+    uint4 a = make_uint4(0, 0, 0, 0), b = make_uint4(0, 0, 0, 0);
+    if (ok) {
+      j = (int64_t)__ldg(ids + k) + off;
+      ok = j >= 0 && j < (int64_t)map_n;
+    }
+    if (ok) {
+      a = *(reinterpret_cast<const uint4*>(lvox + k * kBitVoxelWords) + (lane & 1));
+      b = __ldg(reinterpret_cast<const uint4*>(map + (uint64_t)j * kBitVoxelWords) + (lane & 1));
+    }
+    uint32_t ma = half_bits(a, low), mb = half_bits(b, low);
+    ma |= __shfl_xor_sync(kFull, ma, 1);
+    mb |= __shfl_xor_sync(kFull, mb, 1);
+    const bool hit = ok && ma != 0u && mb != 0u;
+    if (hit && low) {
+      ++hits;
+      if (mark) lvox[k * kBitVoxelWords] = a.x | (1u << kCollisionBit);
+    }
+  }
+  block_count_add(hits, count);
+}
+
+// Batched form: many CSR lists in one launch, per-list counts.  A warp walks
+// 16 entries per step; the list of each entry is found from the list of the
+// warp's first entry, and hits are aggregated per list before the atomic.
+__global__ void __launch_bounds__(256) lists_collide_map_kernel(const uint32_t* __restrict__ ids, uint32_t* __restrict__ lvox,
+                                                                const uint64_t* __restrict__ offsets, uint32_t n_lists,
+                                                                uint64_t n_total, const uint32_t* __restrict__ map,
+                                                                uint64_t map_n, int mark,
+                                                                unsigned long long* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const bool low = (lane & 1) == 0;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (uint64_t base = gw * 16; base < n_total; base += warps * 16) {
+    // list of the warp's first entry: last k with offsets[k] <= base
+    uint32_t lo = 0, hi = n_lists;  // invariant: offsets[lo] <= base < offsets[hi]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(offsets + mid) <= base) lo = mid; else hi = mid;
+    }
+    const uint64_t k = base + (lane >> 1);
+    bool ok = k < n_total;
+    uint32_t list = lo;
+    if (ok) {
+      while (list + 1 < n_lists && __ldg(offsets + list + 1) <= k) ++list;
+    }
+    int64_t j = 0;
+    uint4 a = make_uint4(0, 0, 0, 0), b = make_uint4(0, 0, 0, 0);
+    if (ok) {
+      j = (int64_t)__ldg(ids + k);
+      ok = j < (int64_t)map_n;
+    }
+    if (ok) {
+      a = *(reinterpret_cast<const uint4*>(lvox + k * kBitVoxelWords) + (lane & 1));
+      b = __ldg(reinterpret_cast<const uint4*>(map + (uint64_t)j * kBitVoxelWords) + (lane & 1));
+    }
+    uint32_t ma = half_bits(a, low), mb = half_bits(b, low);
+    ma |= __shfl_xor_sync(kFull, ma, 1);
+    mb |= __shfl_xor_sync(kFull, mb, 1);
+    const bool hit = ok && ma != 0u && mb != 0u && low;
+    if (hit && mark) lvox[k * kBitVoxelWords] = a.x | (1u << kCollisionBit);
+    // aggregate hits of lanes that share a list
+    const unsigned hit_mask = __ballot_sync(kFull, hit);
+    if (hit_mask) {
+      const unsigned same = __match_any_sync(kFull, list);
+      const unsigned mine = same & hit_mask;
+      if (hit && (__ffs(mine) - 1) == lane) atomicAdd(counts + list, (unsigned long long)__popc(mine));
+    }
+  }
+}
+
+// collideVoxellists (GV/voxellist/TemplateVoxelList.hpp:231-289): count of ids
+// of `a` found in the sorted list `b` (thrust::binary_search semantics).
+__global__ void __launch_bounds__(256) list_collide_list_kernel(const uint32_t* __restrict__ a, uint64_t na,
+                                                                const uint32_t* __restrict__ b, uint64_t nb,
+                                                                unsigned long long* __restrict__ count) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long hits = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < na; i += stride) {
+    const uint32_t key = __ldg(a + i);
+    uint64_t lo = 0, hi = nb;
+    while (lo < hi) {
+      const uint64_t mid = lo + ((hi - lo) >> 1);
+      if (__ldg(b + mid) < key) lo = mid + 1; else hi = mid;
+    }
+    hits += (lo < nb && __ldg(b + lo) == key);
+  }
+  block_count_add(hits, count);
+}
+
+unsigned grid_cap(uint64_t work_items, int per_block) {
+  const uint64_t want = (work_items + per_block - 1) / per_block;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sms() * 8));
+}
+
+}  // namespace
+
+cudaError_t launch_bvm_collide(uint8_t* d_self, const uint8_t* d_other, uint64_t n, int64_t off, int mark,
+                               unsigned long long* d_count, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess || n == 0) return e;
+  bvm_collide_kernel<<<grid_cap(n, 8 * 16 * 4), 256, 0, s>>>(reinterpret_cast<uint32_t*>(d_self),
+                                                             reinterpret_cast<const uint32_t*>(d_other), n, off, mark,
+                                                             d_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_list_collide_map(const uint32_t* d_ids, uint8_t* d_list_vox, uint64_t n, const uint8_t* d_map,
+                                    uint64_t map_n, int64_t off, int mark, unsigned long long* d_count, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess || n == 0) return e;
+  list_collide_map_kernel<<<grid_cap(n, 8 * 16), 256, 0, s>>>(d_ids, reinterpret_cast<uint32_t*>(d_list_vox), n,
+                                                              reinterpret_cast<const uint32_t*>(d_map), map_n, off,
+                                                              mark, d_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lists_collide_map(const uint32_t* d_ids, uint8_t* d_vox, const uint64_t* d_offsets, uint32_t n_lists,
+                                     uint64_t n_total, const uint8_t* d_map, uint64_t map_n, int mark,
+                                     unsigned long long* d_counts, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * n_lists, s);
+  if (e != cudaSuccess || n_total == 0 || n_lists == 0) return e;
+  lists_collide_map_kernel<<<grid_cap(n_total, 8 * 16), 256, 0, s>>>(
+      d_ids, reinterpret_cast<uint32_t*>(d_vox), d_offsets, n_lists, n_total, reinterpret_cast<const uint32_t*>(d_map),
+      map_n, mark, d_counts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_list_collide_list(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
+                                     unsigned long long* d_count, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess || na == 0 || nb == 0) return e;
+  list_collide_list_kernel<<<grid_cap(na, 256), 256, 0, s>>>(d_a, na, d_b, nb, d_count);
+  return cudaGetLastError();
+}
+
+}  // namespace gvx

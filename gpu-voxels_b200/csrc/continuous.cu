@@ -1,0 +1,359 @@
+// Continuous distance queries on an EDT'd DistanceVoxel map (no counterpart
+// in gpu-voxels, whose queries stop at integer voxel distances): trilinear
+// distance + spatial gradient and its adjoint, sphere-model clearance per arm
+// configuration, and a hinge trajectory cost with a hand-written adjoint that
+// recomputes the forward kinematics.
+//
+// Distance field: corner value D(i,j,k) = sqrt(squaredObstacleDistance) in
+// voxel units at voxel centres (i + 0.5) * side (getVoxelCenter,
+// GV/voxelmap/kernels/VoxelMapOperations.h:175-182); D = sqrt(INT32_MAX) where
+// the map holds no site.  The interpolant is trilinear on the centre lattice,
+// points are clamped to it (zero gradient along a clamped axis).
+//
+// Kinematics: the reference's DH convention (DHParameters::convertDHtoM,
+// GV/robot/dh_robot/KinematicLink.cu:24-79) chained as
+// KinematicChain::setConfiguration (GV/robot/dh_robot/KinematicChain.cu:104-124).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "gvx_internal.cuh"
+
+namespace gvx {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct MapView {
+  const uint32_t* vox;
+  int X, Y, Z;
+  float side;
+};
+
+__device__ __forceinline__ float corner_dist(const MapView& m, int i, int j, int k) {
+  const uint32_t v = __ldg(m.vox + ((uint64_t)k * m.Y + j) * m.X + i);
+  const int ox = (int)dv_x(v), oy = (int)dv_y(v), oz = (int)dv_z(v);
+  if (ox == (int)kUninit || oy == (int)kUninit || oz == (int)kUninit) return sqrtf((float)kMaxObstacleDistance);
+  const int dx = i - ox, dy = j - oy, dz = k - oz;
+  return sqrtf((float)(dx * dx + dy * dy + dz * dz));
+}
+
+// Lattice coordinate along one axis: u = p/side - 0.5 clamped to [0, n-1];
+// returns the lower corner, the fraction and whether the axis is free.  The
+// fraction is taken from the residual p - (i0 + 0.5) * side (one fused
+// rounding) rather than from u, which keeps it accurate far from the origin.
+__device__ __forceinline__ void axis_setup(float p, float side, int n, int& i0, int& i1, float& f, bool& free_axis) {
+  const float u = __fsub_rn(__fdiv_rn(p, side), 0.5f);
+  const float hi = (float)(n - 1);
+  free_axis = (u >= 0.0f) && (u <= hi);
+  const float uc = fminf(fmaxf(u, 0.0f), hi);  // NaN -> 0
+  i0 = min((int)floorf(uc), max(n - 2, 0));
+  i1 = min(i0 + 1, n - 1);
+  if (free_axis) {
+    f = __fdiv_rn(fmaf(-((float)i0 + 0.5f), side, p), side);
+    f = fminf(fmaxf(f, 0.0f), 1.0f);
+  } else {
+    f = uc - (float)i0;
+  }
+}
+
+struct Tri {
+  float d;           // voxel units
+  float gx, gy, gz;  // d(distance)/d(position), dimensionless
+};
+
+__device__ __forceinline__ Tri trilinear(const MapView& m, float px, float py, float pz) {
+  int i0, i1, j0, j1, k0, k1;
+  float fx, fy, fz;
+  bool ax, ay, az;
+  axis_setup(px, m.side, m.X, i0, i1, fx, ax);
+  axis_setup(py, m.side, m.Y, j0, j1, fy, ay);
+  axis_setup(pz, m.side, m.Z, k0, k1, fz, az);
+  const float d000 = corner_dist(m, i0, j0, k0), d100 = corner_dist(m, i1, j0, k0);
+  const float d010 = corner_dist(m, i0, j1, k0), d110 = corner_dist(m, i1, j1, k0);
+  const float d001 = corner_dist(m, i0, j0, k1), d101 = corner_dist(m, i1, j0, k1);
+  const float d011 = corner_dist(m, i0, j1, k1), d111 = corner_dist(m, i1, j1, k1);
+  // interpolate along x, then y, then z
+  const float e00 = fmaf(fx, d100 - d000, d000), e10 = fmaf(fx, d110 - d010, d010);
+  const float e01 = fmaf(fx, d101 - d001, d001), e11 = fmaf(fx, d111 - d011, d011);
+  const float g0 = fmaf(fy, e10 - e00, e00), g1 = fmaf(fy, e11 - e01, e01);
+  Tri t;
+  t.d = fmaf(fz, g1 - g0, g0);
+  // partial derivatives of the interpolant in lattice units
+  const float sx0 = fmaf(fy, (d110 - d010) - (d100 - d000), d100 - d000);
+  const float sx1 = fmaf(fy, (d111 - d011) - (d101 - d001), d101 - d001);
+  t.gx = ax ? fmaf(fz, sx1 - sx0, sx0) : 0.0f;
+  const float sy0 = e10 - e00, sy1 = e11 - e01;
+  t.gy = ay ? fmaf(fz, sy1 - sy0, sy0) : 0.0f;
+  t.gz = az ? (g1 - g0) : 0.0f;
+  return t;
+}
+
+__global__ void trilinear_kernel(MapView m, const float* __restrict__ xyz, uint64_t n, float* __restrict__ dist,
+                                 float* __restrict__ grad) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const Tri t = trilinear(m, __ldg(xyz + 3 * i), __ldg(xyz + 3 * i + 1), __ldg(xyz + 3 * i + 2));
+    dist[i] = t.d * m.side;
+    if (grad != nullptr) {
+      grad[3 * i] = t.gx;
+      grad[3 * i + 1] = t.gy;
+      grad[3 * i + 2] = t.gz;
+    }
+  }
+}
+
+__global__ void trilinear_bwd_kernel(MapView m, const float* __restrict__ xyz, uint64_t n,
+                                     const float* __restrict__ gout, float* __restrict__ gxyz) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const Tri t = trilinear(m, __ldg(xyz + 3 * i), __ldg(xyz + 3 * i + 1), __ldg(xyz + 3 * i + 2));
+    const float g = __ldg(gout + i);
+    gxyz[3 * i] = g * t.gx;
+    gxyz[3 * i + 1] = g * t.gy;
+    gxyz[3 * i + 2] = g * t.gz;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Forward kinematics: frames F_0 = base, F_{j+1} = F_j * A_j(q_j),
+// A_j = Rz(theta_j + q_j) Tz(d_j) Tx(a_j) Rx(alpha_j).  Link j spans origin
+// o_j -> o_{j+1}; joint j turns about z_j (third column of F_j) through o_j.
+// ---------------------------------------------------------------------------
+struct Frame {
+  float r[9];  // row-major rotation
+  float o[3];
+};
+
+__device__ __forceinline__ Frame base_frame(const gvx_arm& arm) {
+  Frame f;
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) f.r[3 * i + j] = arm.base[4 * i + j];
+    f.o[i] = arm.base[4 * i + 3];
+  }
+  return f;
+}
+
+__device__ __forceinline__ Frame dh_step(const Frame& F, const gvx_arm& arm, int j, float q) {
+  float st, ct, sa, ca;
+  sincosf(arm.theta[j] + q, &st, &ct);
+  sincosf(arm.alpha[j], &sa, &ca);
+  const float A[9] = {ct, -st * ca, st * sa, st, ct * ca, -ct * sa, 0.0f, sa, ca};
+  const float t[3] = {arm.a[j] * ct, arm.a[j] * st, arm.d[j]};
+  Frame G;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      G.r[3 * i + k] = F.r[3 * i] * A[k] + F.r[3 * i + 1] * A[3 + k] + F.r[3 * i + 2] * A[6 + k];
+    G.o[i] = F.r[3 * i] * t[0] + F.r[3 * i + 1] * t[1] + F.r[3 * i + 2] * t[2] + F.o[i];
+  }
+  return G;
+}
+
+// Per-warp FK into shared memory: origins o[0..J] and joint axes z[0..J-1].
+struct WarpFK {
+  float o[GVX_MAX_JOINTS + 1][3];
+  float z[GVX_MAX_JOINTS][3];
+};
+
+__device__ __forceinline__ void warp_fk(const gvx_arm& arm, const float* q, WarpFK& fk) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    Frame F = base_frame(arm);
+    for (int j = 0; j < arm.n_joints; ++j) {
+      fk.o[j][0] = F.o[0]; fk.o[j][1] = F.o[1]; fk.o[j][2] = F.o[2];
+      fk.z[j][0] = F.r[2]; fk.z[j][1] = F.r[5]; fk.z[j][2] = F.r[8];
+      F = dh_step(F, arm, j, __ldg(q + j));
+    }
+    fk.o[arm.n_joints][0] = F.o[0]; fk.o[arm.n_joints][1] = F.o[1]; fk.o[arm.n_joints][2] = F.o[2];
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void sphere_centre(const gvx_arm& arm, const WarpFK& fk, int s, float c[3]) {
+  const int j = arm.link[s];
+  const float t = arm.t[s];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) c[i] = fmaf(t, fk.o[j + 1][i] - fk.o[j][i], fk.o[j][i]);
+}
+
+constexpr int kWarpsPerBlock = 8;
+
+// Min clearance per configuration; one warp per configuration, lanes over spheres.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) sphere_clearance_kernel(MapView m, gvx_arm arm,
+                                                                              const float* __restrict__ q, uint64_t n_cfg,
+                                                                              float* __restrict__ out) {
+  __shared__ WarpFK s_fk[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint64_t total_warps = (uint64_t)gridDim.x * kWarpsPerBlock;
+  for (uint64_t cfg = (uint64_t)blockIdx.x * kWarpsPerBlock + warp; cfg < n_cfg; cfg += total_warps) {
+    warp_fk(arm, q + cfg * arm.n_joints, s_fk[warp]);
+    float best = __int_as_float(0x7f800000);  // +inf
+    for (int s = lane; s < arm.n_spheres; s += 32) {
+      float c[3];
+      sphere_centre(arm, s_fk[warp], s, c);
+      const Tri t = trilinear(m, c[0], c[1], c[2]);
+      best = fminf(best, t.d * m.side - arm.r[s]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = fminf(best, __shfl_xor_sync(kFull, best, o));
+    if (lane == 0) out[cfg] = best;
+    __syncwarp();
+  }
+}
+
+// Hinge cost: one block per trajectory, warp w takes waypoints w, w+8, ...;
+// fixed-order reductions keep the result deterministic.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_kernel(MapView m, gvx_arm arm, const float* __restrict__ q,
+                                                                       uint64_t n_traj, uint32_t n_wp, float margin,
+                                                                       float* __restrict__ cost) {
+  __shared__ WarpFK s_fk[kWarpsPerBlock];
+  __shared__ float s_part[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint64_t traj = blockIdx.x; traj < n_traj; traj += gridDim.x) {
+    float acc = 0.0f;
+    for (uint32_t w = warp; w < n_wp; w += kWarpsPerBlock) {
+      warp_fk(arm, q + (traj * n_wp + w) * arm.n_joints, s_fk[warp]);
+      for (int s = lane; s < arm.n_spheres; s += 32) {
+        float c[3];
+        sphere_centre(arm, s_fk[warp], s, c);
+        const Tri t = trilinear(m, c[0], c[1], c[2]);
+        acc += fmaxf(0.0f, margin - (t.d * m.side - arm.r[s]));
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+    if (lane == 0) s_part[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float sum = 0.0f;
+      for (int i = 0; i < kWarpsPerBlock; ++i) sum += s_part[i];
+      cost[traj] = sum;
+    }
+    __syncthreads();
+  }
+}
+
+// Adjoint of the hinge cost.  For an active sphere s on link j,
+//   d cost / d q_k = -grad d(c_s) . (z_k x (c_s - o_k))   for k <= j,
+// which sums per joint to -z_k . (M_k - o_k x G_k) with suffix sums over links
+// M_k = sum c_s x g_s, G_k = sum g_s.  One warp per waypoint, FK recomputed.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapView m, gvx_arm arm,
+                                                                           const float* __restrict__ q, uint64_t n_traj,
+                                                                           uint32_t n_wp, float margin,
+                                                                           const float* __restrict__ gcost,
+                                                                           float* __restrict__ gq) {
+  __shared__ WarpFK s_fk[kWarpsPerBlock];
+  __shared__ float s_link[kWarpsPerBlock][GVX_MAX_JOINTS][6];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int J = arm.n_joints;
+  const uint64_t n_items = n_traj * n_wp;
+  const uint64_t total_warps = (uint64_t)gridDim.x * kWarpsPerBlock;
+  for (uint64_t item = (uint64_t)blockIdx.x * kWarpsPerBlock + warp; item < n_items; item += total_warps) {
+    const uint64_t traj = item / n_wp;
+    warp_fk(arm, q + item * J, s_fk[warp]);
+    for (int j = 0; j < J; ++j) {
+      // per-link sums of c x g and g over this lane's active spheres
+      float mc[3] = {0.f, 0.f, 0.f}, gg[3] = {0.f, 0.f, 0.f};
+      for (int s = lane; s < arm.n_spheres; s += 32) {
+        if (arm.link[s] != j) continue;
+        float c[3];
+        sphere_centre(arm, s_fk[warp], s, c);
+        const Tri t = trilinear(m, c[0], c[1], c[2]);
+        if (margin - (t.d * m.side - arm.r[s]) > 0.0f) {
+          mc[0] += c[1] * t.gz - c[2] * t.gy;
+          mc[1] += c[2] * t.gx - c[0] * t.gz;
+          mc[2] += c[0] * t.gy - c[1] * t.gx;
+          gg[0] += t.gx; gg[1] += t.gy; gg[2] += t.gz;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          mc[i] += __shfl_xor_sync(kFull, mc[i], o);
+          gg[i] += __shfl_xor_sync(kFull, gg[i], o);
+        }
+      }
+      if (lane == 0) {
+        for (int i = 0; i < 3; ++i) { s_link[warp][j][i] = mc[i]; s_link[warp][j][3 + i] = gg[i]; }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      const float g = __ldg(gcost + traj);
+      float M[3] = {0.f, 0.f, 0.f}, G[3] = {0.f, 0.f, 0.f};
+      for (int k = J - 1; k >= 0; --k) {
+        for (int i = 0; i < 3; ++i) { M[i] += s_link[warp][k][i]; G[i] += s_link[warp][k][3 + i]; }
+        const float* o = s_fk[warp].o[k];
+        const float* z = s_fk[warp].z[k];
+        const float v0 = M[0] - (o[1] * G[2] - o[2] * G[1]);
+        const float v1 = M[1] - (o[2] * G[0] - o[0] * G[2]);
+        const float v2 = M[2] - (o[0] * G[1] - o[1] * G[0]);
+        gq[item * J + k] = -g * (z[0] * v0 + z[1] * v1 + z[2] * v2);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+int g_sms = 0;
+int sms() {
+  if (g_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms;
+}
+
+unsigned blocks_for(uint64_t items, uint64_t per_block, uint64_t cap_per_sm) {
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + per_block - 1) / per_block, (uint64_t)sms() * cap_per_sm));
+}
+
+MapView view(const gvx_dvm* m) { return MapView{m->d_vox, (int)m->dims.x, (int)m->dims.y, (int)m->dims.z, m->side}; }
+
+}  // namespace
+
+cudaError_t launch_trilinear(const gvx_dvm* m, const float* d_xyz, uint64_t n, float* d_dist, float* d_grad, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  trilinear_kernel<<<blocks_for(n, 256, 16), 256, 0, s>>>(view(m), d_xyz, n, d_dist, d_grad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trilinear_bwd(const gvx_dvm* m, const float* d_xyz, uint64_t n, const float* d_gout, float* d_gxyz,
+                                 cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  trilinear_bwd_kernel<<<blocks_for(n, 256, 16), 256, 0, s>>>(view(m), d_xyz, n, d_gout, d_gxyz);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sphere_clearance(const gvx_dvm* m, const gvx_arm& arm, const float* d_q, uint64_t n_cfg, float* d_out,
+                                    cudaStream_t s) {
+  if (n_cfg == 0) return cudaSuccess;
+  sphere_clearance_kernel<<<blocks_for(n_cfg, kWarpsPerBlock, 8), kWarpsPerBlock * 32, 0, s>>>(view(m), arm, d_q, n_cfg,
+                                                                                              d_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_traj_cost(const gvx_dvm* m, const gvx_arm& arm, const float* d_q, uint64_t n_traj, uint32_t n_wp,
+                             float margin, float* d_cost, cudaStream_t s) {
+  if (n_traj == 0) return cudaSuccess;
+  traj_cost_kernel<<<(unsigned)std::min<uint64_t>(n_traj, (uint64_t)sms() * 32), kWarpsPerBlock * 32, 0, s>>>(
+      view(m), arm, d_q, n_traj, n_wp, margin, d_cost);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_traj_cost_bwd(const gvx_dvm* m, const gvx_arm& arm, const float* d_q, uint64_t n_traj, uint32_t n_wp,
+                                 float margin, const float* d_gcost, float* d_gq, cudaStream_t s) {
+  if (n_traj == 0 || n_wp == 0) return cudaSuccess;
+  traj_cost_bwd_kernel<<<blocks_for(n_traj * n_wp, kWarpsPerBlock, 8), kWarpsPerBlock * 32, 0, s>>>(
+      view(m), arm, d_q, n_traj, n_wp, margin, d_gcost, d_gq);
+  return cudaGetLastError();
+}
+
+}  // namespace gvx

@@ -1,0 +1,95 @@
+// Internal definitions shared by the gvx CUDA translation units.
+//
+// Value formats follow gpu-voxels (GV = packages/gpu_voxels/src/gpu_voxels/):
+//   DistanceVoxel  x | y<<10 | z<<20, uninitialised coordinate 1023
+//                  (GV/voxel/DistanceVoxel.hpp:31-65, GV/helpers/common_defines.h:113-131)
+//   BitVoxel<256>  32 bytes, bit k = meaning k (GV/helpers/BitVector.h:349-350)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/gvx.h"
+
+namespace gvx {
+
+constexpr uint32_t kUninit = 1023u;              // PBA_UNINITIALISED_COORD
+constexpr uint32_t kDvUninit = 0x3FFFFFFFu;      // all three coordinates uninitialised
+constexpr int32_t kMaxObstacleDistance = 2147483647;  // MAX_OBSTACLE_DISTANCE
+constexpr uint32_t kBitVoxelBytes = 32;
+constexpr uint32_t kBitVoxelWords = 8;
+constexpr uint32_t kCollisionBit = 2;            // eBVM_COLLISION
+constexpr uint32_t kMaxDim = 1023;
+
+__host__ __device__ __forceinline__ uint32_t dv_pack(uint32_t x, uint32_t y, uint32_t z) {
+  return x | (y << 10) | (z << 20);
+}
+__host__ __device__ __forceinline__ uint32_t dv_x(uint32_t v) { return v & 0x3ffu; }
+__host__ __device__ __forceinline__ uint32_t dv_y(uint32_t v) { return (v >> 10) & 0x3ffu; }
+__host__ __device__ __forceinline__ uint32_t dv_z(uint32_t v) { return v >> 20; }
+
+// mapToVoxels(float, Vector3f) (GV/voxelmap/kernels/VoxelMapOperations.h:121-131):
+// IEEE divide, floor, saturating float->u32 convert (negative and NaN -> 0).
+__device__ __forceinline__ uint32_t coord_to_voxel(float c, float side) {
+  return __float2uint_rz(floorf(__fdiv_rn(c, side)));
+}
+
+}  // namespace gvx
+
+// Opaque handle definitions (C ABI types).
+struct gvx_dvm {
+  gvx_dims dims;
+  float side;
+  uint32_t* d_vox;
+  bool owns;
+};
+
+struct gvx_bvm {
+  gvx_dims dims;
+  float side;
+  uint8_t* d_vox;
+};
+
+struct gvx_blist {
+  gvx_dims ref;
+  float side;
+  uint32_t* d_ids;
+  uint8_t* d_vox;
+  uint64_t n;
+  uint64_t cap;
+};
+
+namespace gvx {
+
+// Error reporting shared by the ABI units.
+void set_error(const std::string& msg);
+gvx_status cuda_status(cudaError_t e, const char* what);
+
+inline uint64_t num_voxels(const gvx_dims& d) { return (uint64_t)d.x * d.y * d.z; }
+inline cudaStream_t as_stream(gvx_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Launchers implemented in the kernel translation units.  They check only
+// what the kernels need; argument validation happens in the ABI layer.
+cudaError_t launch_dvm_clear(uint32_t* d_vox, uint64_t n, cudaStream_t s);
+cudaError_t launch_dvm_insert(uint32_t* d_vox, gvx_dims d, float side, const float* d_xyz, uint64_t n,
+                              uint32_t* d_outside, cudaStream_t s);
+cudaError_t launch_bvm_insert(uint8_t* d_vox, gvx_dims d, float side, const float* d_xyz, uint64_t n, uint32_t meaning,
+                              uint32_t* d_outside, cudaStream_t s);
+cudaError_t launch_edt(uint32_t* d_vox, gvx_dims d, cudaStream_t s);
+cudaError_t launch_edt_pass(uint32_t* d_vox, gvx_dims d, int pass, cudaStream_t s);
+cudaError_t launch_dvm_sqdist(const uint32_t* d_vox, gvx_dims d, const uint32_t* d_ids, uint64_t n, int32_t* d_out,
+                              int mode, cudaStream_t s);
+cudaError_t launch_dvm_sqdist_map(const uint32_t* d_vox, gvx_dims d, int32_t* d_out, cudaStream_t s);
+cudaError_t launch_bvm_collide(uint8_t* d_self, const uint8_t* d_other, uint64_t n, int64_t off, int mark,
+                               unsigned long long* d_count, cudaStream_t s);
+cudaError_t launch_list_collide_map(const uint32_t* d_ids, uint8_t* d_list_vox, uint64_t n, const uint8_t* d_map,
+                                    uint64_t map_n, int64_t off, int mark, unsigned long long* d_count, cudaStream_t s);
+cudaError_t launch_lists_collide_map(const uint32_t* d_ids, uint8_t* d_vox, const uint64_t* d_offsets, uint32_t n_lists,
+                                     uint64_t n_total, const uint8_t* d_map, uint64_t map_n, int mark,
+                                     unsigned long long* d_counts, cudaStream_t s);
+cudaError_t launch_list_collide_list(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
+                                     unsigned long long* d_count, cudaStream_t s);
+
+}  // namespace gvx

@@ -1,0 +1,104 @@
+// Map fill and point-cloud voxelisation kernels.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "gvx_internal.cuh"
+
+namespace gvx {
+namespace {
+
+int g_num_sms = 0;
+int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+// clearMap for DistanceVoxel (GV/voxelmap/TemplateVoxelMap.hpp:244-271):
+// 16-byte stores of the uninitialised value; the map base is 256-B aligned.
+__global__ void dvm_fill_kernel(uint4* __restrict__ v4, uint64_t n4, uint32_t* __restrict__ tail, uint32_t ntail) {
+  const uint4 u = make_uint4(kDvUninit, kDvUninit, kDvUninit, kDvUninit);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) __stcs(v4 + i, u);
+  if (blockIdx.x == 0 && threadIdx.x < ntail) tail[threadIdx.x] = kDvUninit;
+}
+
+// kernelInsertGlobalPointCloud<DistanceVoxel> (GV/voxelmap/kernels/VoxelMapOperations.hpp:266-300):
+// every point in a voxel writes the voxel's own coordinate, so the scatter
+// needs no atomics (DistanceVoxel::insert, GV/voxel/DistanceVoxel.hpp:125-138).
+__global__ void dvm_insert_kernel(uint32_t* __restrict__ map, uint32_t X, uint32_t Y, uint32_t Z, float side,
+                                  const float* __restrict__ xyz, uint64_t n, uint32_t* __restrict__ outside) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  bool out = false;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float px = __ldg(xyz + 3 * i), py = __ldg(xyz + 3 * i + 1), pz = __ldg(xyz + 3 * i + 2);
+    const uint32_t x = coord_to_voxel(px, side), y = coord_to_voxel(py, side), z = coord_to_voxel(pz, side);
+    if (x < X && y < Y && z < Z) {
+      map[z * X * Y + y * X + x] = dv_pack(x, y, z);
+    } else {
+      out = true;
+    }
+  }
+  if (outside != nullptr && __any_sync(0xffffffffu, out) && (threadIdx.x & 31) == 0) *outside = 1u;
+}
+
+// kernelInsertGlobalPointCloud<BitVoxel> (VoxelMapOperations.hpp:241-264).  The
+// reference ORs the byte without an atomic; a 32-bit atomicOr gives the same
+// result and stays correct when different meanings hit one voxel at once.
+__global__ void bvm_insert_kernel(uint32_t* __restrict__ map, uint32_t X, uint32_t Y, uint32_t Z, float side,
+                                  const float* __restrict__ xyz, uint64_t n, uint32_t meaning,
+                                  uint32_t* __restrict__ outside) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t word = meaning >> 5, bit = 1u << (meaning & 31);
+  bool out = false;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float px = __ldg(xyz + 3 * i), py = __ldg(xyz + 3 * i + 1), pz = __ldg(xyz + 3 * i + 2);
+    const uint32_t x = coord_to_voxel(px, side), y = coord_to_voxel(py, side), z = coord_to_voxel(pz, side);
+    if (x < X && y < Y && z < Z) {
+      const uint64_t id = (uint64_t)z * X * Y + (uint64_t)y * X + x;
+      atomicOr(map + id * kBitVoxelWords + word, bit);
+    } else {
+      out = true;
+    }
+  }
+  if (outside != nullptr && __any_sync(0xffffffffu, out) && (threadIdx.x & 31) == 0) *outside = 1u;
+}
+
+unsigned grid_for(uint64_t n, int threads) {
+  const uint64_t want = (n + threads - 1) / threads;
+  const uint64_t cap = (uint64_t)num_sms() * 16;
+  return (unsigned)std::max<uint64_t>(1, std::min(want, cap));
+}
+
+}  // namespace
+
+cudaError_t launch_dvm_clear(uint32_t* d_vox, uint64_t n, cudaStream_t s) {
+  const uint64_t n4 = n / 4;
+  const uint32_t ntail = (uint32_t)(n - n4 * 4);
+  dvm_fill_kernel<<<grid_for(std::max<uint64_t>(n4, 1), 256), 256, 0, s>>>(reinterpret_cast<uint4*>(d_vox), n4,
+                                                                          d_vox + n4 * 4, ntail);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dvm_insert(uint32_t* d_vox, gvx_dims d, float side, const float* d_xyz, uint64_t n,
+                              uint32_t* d_outside, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  dvm_insert_kernel<<<grid_for(n, 256), 256, 0, s>>>(d_vox, d.x, d.y, d.z, side, d_xyz, n, d_outside);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bvm_insert(uint8_t* d_vox, gvx_dims d, float side, const float* d_xyz, uint64_t n, uint32_t meaning,
+                              uint32_t* d_outside, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  bvm_insert_kernel<<<grid_for(n, 256), 256, 0, s>>>(reinterpret_cast<uint32_t*>(d_vox), d.x, d.y, d.z, side, d_xyz, n,
+                                                     meaning, d_outside);
+  return cudaGetLastError();
+}
+
+}  // namespace gvx

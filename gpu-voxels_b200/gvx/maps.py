@@ -1,0 +1,327 @@
+"""Python handles over the C ABI, named after gpu-voxels' map classes.
+
+DistanceVoxelMap, BitVectorVoxelMap and BitVectorVoxelList expose the
+reference's method names (clearMap, insertPointCloud, parallelBanding3D,
+getSquaredDistances, collideWith, ...) with torch CUDA tensors as device
+buffers.  Every call goes to lib/libgvx.so on the current torch stream.
+Methods that the reference makes blocking (the *ToHost queries and the
+collideWith counts) synchronise here too.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, Optional, Sequence
+
+import torch
+
+from . import _abi
+from ._abi import Arm, Dims, call
+
+BIT_VECTOR_LENGTH = 256
+eBVM_FREE = 0
+eBVM_OCCUPIED = 1
+eBVM_COLLISION = 2
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t: Optional[torch.Tensor]) -> ctypes.c_void_p:
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _dev_points(points) -> torch.Tensor:
+    t = points if isinstance(points, torch.Tensor) else torch.as_tensor(points)
+    t = t.to(device="cuda", dtype=torch.float32).reshape(-1, 3).contiguous()
+    return t
+
+
+def _dev_u32(ids) -> torch.Tensor:
+    t = ids if isinstance(ids, torch.Tensor) else torch.as_tensor(ids, dtype=torch.int64)
+    if t.dtype != torch.int32:
+        t = t.to(torch.int64).to(torch.int32)  # same 32 bits
+    return t.to("cuda").contiguous()
+
+
+def _offset(offset: Sequence[int]) -> ctypes.Array:
+    o = (ctypes.c_int32 * 3)(*[int(v) for v in offset])
+    return o
+
+
+class DistanceVoxelMap:
+    """DistanceVoxelMap (GV/voxelmap/DistanceVoxelMap.h): uint32 sites per voxel."""
+
+    def __init__(self, dims: Sequence[int], voxel_side_length: float, voxels: Optional[torch.Tensor] = None):
+        self.dims = tuple(int(d) for d in dims)
+        self.voxel_side_length = float(voxel_side_length)
+        h = ctypes.c_void_p()
+        d = Dims(*self.dims)
+        self._owner = None
+        if voxels is None:
+            call("gvx_dvm_create", ctypes.byref(d), self.voxel_side_length, ctypes.byref(h))
+        else:
+            assert voxels.is_cuda and voxels.dtype == torch.int32 and voxels.numel() == self.size
+            self._owner = voxels
+            call("gvx_dvm_wrap", ctypes.byref(d), self.voxel_side_length, _ptr(voxels), ctypes.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _abi.lib().gvx_dvm_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    @property
+    def size(self) -> int:
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+    def data(self) -> torch.Tensor:
+        """Borrowed int32 CUDA view of the voxel buffer (bit pattern = uint32
+        sites); valid while this map is alive."""
+        if self._owner is not None:
+            return self._owner
+        d, s, p = Dims(), ctypes.c_float(), ctypes.c_void_p()
+        call("gvx_dvm_info", self._h, ctypes.byref(d), ctypes.byref(s), ctypes.byref(p))
+        return _device_view(p.value, self.size)
+
+    def clearMap(self) -> None:
+        call("gvx_dvm_clear", self._h, _stream())
+
+    def insertPointCloud(self, points, meaning: int = eBVM_OCCUPIED, outside: Optional[torch.Tensor] = None) -> None:
+        p = _dev_points(points)
+        call("gvx_dvm_insert_points", self._h, _ptr(p), p.shape[0], _ptr(outside), _stream())
+
+    def parallelBanding3D(self, m1: int = 1, m2: int = 1, m3: int = 1, *unused) -> None:
+        call("gvx_dvm_edt", self._h, m1, m2, m3, _stream())
+
+    def edt_pass(self, pass_index: int) -> None:
+        """One EDT sweep (0: z, 1: y, 2: x)."""
+        call("gvx_dvm_edt_pass", self._h, int(pass_index), _stream())
+
+    def getSquaredDistances(self, ids: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        ids = _dev_u32(ids)
+        out = torch.empty(ids.shape[0], dtype=torch.int32, device="cuda") if out is None else out
+        call("gvx_dvm_sqdist", self._h, _ptr(ids), ids.shape[0], _ptr(out), _stream())
+        return out
+
+    def getSquaredDistancesToHost(self, ids) -> list:
+        return self.getSquaredDistances(ids).cpu().tolist()
+
+    def getDistances(self, ids: torch.Tensor) -> torch.Tensor:
+        ids = _dev_u32(ids)
+        out = torch.empty(ids.shape[0], dtype=torch.int32, device="cuda")
+        call("gvx_dvm_dist", self._h, _ptr(ids), ids.shape[0], _ptr(out), _stream())
+        return out
+
+    def getDistancesToHost(self, ids) -> list:
+        return self.getDistances(ids).cpu().tolist()
+
+    def gatherVoxelsByIndex(self, ids) -> torch.Tensor:
+        ids = _dev_u32(ids)
+        out = torch.empty(ids.shape[0], dtype=torch.int32, device="cuda")
+        call("gvx_dvm_gather", self._h, _ptr(ids), ids.shape[0], _ptr(out), _stream())
+        return out
+
+    def squaredDistanceMap(self) -> torch.Tensor:
+        out = torch.empty(self.size, dtype=torch.int32, device="cuda")
+        call("gvx_dvm_sqdist_map", self._h, _ptr(out), _stream())
+        return out
+
+    def getSquaredObstacleDistance(self, x: int, y: int, z: int) -> int:
+        return self.getSquaredDistancesToHost([(z * self.dims[1] + y) * self.dims[0] + x])[0]
+
+    # continuous queries (new)
+    def trilinear(self, points: torch.Tensor, with_grad: bool = True):
+        p = _dev_points(points)
+        n = p.shape[0]
+        dist = torch.empty(n, dtype=torch.float32, device="cuda")
+        grad = torch.empty(n, 3, dtype=torch.float32, device="cuda") if with_grad else None
+        call("gvx_query_trilinear", self._h, _ptr(p), n, _ptr(dist), _ptr(grad), _stream())
+        return (dist, grad) if with_grad else dist
+
+    def trilinear_backward(self, points: torch.Tensor, grad_dist: torch.Tensor) -> torch.Tensor:
+        p = _dev_points(points)
+        g = grad_dist.to(device="cuda", dtype=torch.float32).contiguous()
+        out = torch.empty(p.shape[0], 3, dtype=torch.float32, device="cuda")
+        call("gvx_query_trilinear_bwd", self._h, _ptr(p), p.shape[0], _ptr(g), _ptr(out), _stream())
+        return out
+
+    def sphere_clearance(self, arm: Arm, q: torch.Tensor) -> torch.Tensor:
+        q = q.to(device="cuda", dtype=torch.float32).contiguous()
+        n = q.shape[0]
+        out = torch.empty(n, dtype=torch.float32, device="cuda")
+        call("gvx_sphere_clearance", self._h, ctypes.byref(arm), _ptr(q), n, _ptr(out), _stream())
+        return out
+
+    def traj_cost(self, arm: Arm, q: torch.Tensor, margin: float) -> torch.Tensor:
+        q = q.to(device="cuda", dtype=torch.float32).contiguous()
+        out = torch.empty(q.shape[0], dtype=torch.float32, device="cuda")
+        call("gvx_traj_cost", self._h, ctypes.byref(arm), _ptr(q), q.shape[0], q.shape[1], float(margin), _ptr(out),
+             _stream())
+        return out
+
+    def traj_cost_backward(self, arm: Arm, q: torch.Tensor, margin: float, grad_cost: torch.Tensor) -> torch.Tensor:
+        q = q.to(device="cuda", dtype=torch.float32).contiguous()
+        g = grad_cost.to(device="cuda", dtype=torch.float32).contiguous()
+        out = torch.empty_like(q)
+        call("gvx_traj_cost_bwd", self._h, ctypes.byref(arm), _ptr(q), q.shape[0], q.shape[1], float(margin), _ptr(g),
+             _ptr(out), _stream())
+        return out
+
+
+def _device_view(ptr: int, n: int) -> torch.Tensor:
+    """A borrowed int32 CUDA tensor over n elements at a raw device pointer."""
+    class _CAI:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_CAI(), device="cuda")
+
+
+def _device_view_u8(ptr: int, n: int) -> torch.Tensor:
+    class _CAI:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_CAI(), device="cuda")
+
+
+class BitVectorVoxelMap:
+    """BitVoxelMap<256> (GV/voxelmap/BitVoxelMap.h): 32-byte bit vectors."""
+
+    def __init__(self, dims: Sequence[int], voxel_side_length: float):
+        self.dims = tuple(int(d) for d in dims)
+        self.voxel_side_length = float(voxel_side_length)
+        h = ctypes.c_void_p()
+        call("gvx_bvm_create", ctypes.byref(Dims(*self.dims)), self.voxel_side_length, ctypes.byref(h))
+        self._h = h
+        self._count = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _abi.lib().gvx_bvm_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    @property
+    def size(self) -> int:
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+    def voxels(self) -> torch.Tensor:
+        """Borrowed uint8 view of the 32-byte voxels (size * 32 bytes)."""
+        d, s, p = Dims(), ctypes.c_float(), ctypes.c_void_p()
+        call("gvx_bvm_info", self._h, ctypes.byref(d), ctypes.byref(s), ctypes.byref(p))
+        return _device_view_u8(p.value, self.size * 32)
+
+    def clearMap(self) -> None:
+        call("gvx_bvm_clear", self._h, _stream())
+
+    def insertPointCloud(self, points, meaning: int = eBVM_OCCUPIED, outside: Optional[torch.Tensor] = None) -> None:
+        p = _dev_points(points)
+        call("gvx_bvm_insert_points", self._h, _ptr(p), p.shape[0], int(meaning), _ptr(outside), _stream())
+
+    def collideWithAsync(self, other: "BitVectorVoxelMap", offset=(0, 0, 0), mark: bool = True,
+                         out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        out = self._count if out is None else out
+        call("gvx_bvm_collide", self._h, other.handle, _offset(offset), 1 if mark else 0, _ptr(out), _stream())
+        return out
+
+    def collideWith(self, other: "BitVectorVoxelMap", coll_threshold: float = 1.0, offset=(0, 0, 0)) -> int:
+        return int(self.collideWithAsync(other, offset).item())
+
+
+class BitVectorVoxelList:
+    """BitVoxelList<256, uint32> (GV/voxellist/BitVoxelList.h): sorted unique
+    voxel ids with 32-byte bit vectors, tied to a reference map's dims."""
+
+    def __init__(self, ref_dims: Sequence[int], voxel_side_length: float):
+        self.dims = tuple(int(d) for d in ref_dims)
+        self.voxel_side_length = float(voxel_side_length)
+        h = ctypes.c_void_p()
+        call("gvx_blist_create", ctypes.byref(Dims(*self.dims)), self.voxel_side_length, ctypes.byref(h))
+        self._h = h
+        self._count = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _abi.lib().gvx_blist_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def getDimensions(self) -> int:
+        n = ctypes.c_uint64()
+        call("gvx_blist_size", self._h, ctypes.byref(n))
+        return n.value
+
+    def ids(self) -> torch.Tensor:
+        n = self.getDimensions()
+        pi, pv = ctypes.c_void_p(), ctypes.c_void_p()
+        call("gvx_blist_data", self._h, ctypes.byref(pi), ctypes.byref(pv))
+        return _device_view(pi.value, n).clone() if n else torch.empty(0, dtype=torch.int32, device="cuda")
+
+    def voxels(self) -> torch.Tensor:
+        n = self.getDimensions()
+        pi, pv = ctypes.c_void_p(), ctypes.c_void_p()
+        call("gvx_blist_data", self._h, ctypes.byref(pi), ctypes.byref(pv))
+        return _device_view_u8(pv.value, n * 32).clone() if n else torch.empty(0, dtype=torch.uint8, device="cuda")
+
+    def clearMap(self) -> None:
+        call("gvx_blist_clear", self._h)
+
+    def insertPointCloud(self, points, meaning: int = eBVM_OCCUPIED) -> None:
+        p = _dev_points(points)
+        call("gvx_blist_insert_points", self._h, _ptr(p), p.shape[0], int(meaning), _stream())
+
+    def set(self, ids: torch.Tensor, voxels: Optional[torch.Tensor] = None, meaning: int = eBVM_OCCUPIED) -> None:
+        ids = _dev_u32(ids)
+        call("gvx_blist_set", self._h, _ptr(ids), _ptr(voxels), ids.shape[0], int(meaning), _stream())
+
+    def collideWith(self, other, coll_threshold: float = 1.0, offset=(0, 0, 0), mark: bool = True) -> int:
+        if isinstance(other, BitVectorVoxelMap):
+            call("gvx_blist_collide_bvm", self._h, other.handle, _offset(offset), 1 if mark else 0, _ptr(self._count),
+                 _stream())
+        elif isinstance(other, BitVectorVoxelList):
+            call("gvx_blist_collide_blist", self._h, other.handle, _offset(offset), _ptr(self._count), _stream())
+        else:
+            raise TypeError("collideWith expects a BitVectorVoxelMap or BitVectorVoxelList")
+        return int(self._count.item())
+
+
+def lists_collide_map(ids: torch.Tensor, voxels: torch.Tensor, offsets: torch.Tensor, bvm: BitVectorVoxelMap,
+                      mark: bool = False, counts: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Batched list-vs-map collision: CSR lists, one launch, per-list counts."""
+    n_lists = offsets.shape[0] - 1
+    counts = torch.empty(n_lists, dtype=torch.int64, device="cuda") if counts is None else counts
+    call("gvx_lists_collide_bvm", _ptr(ids), _ptr(voxels), _ptr(offsets), n_lists, ids.shape[0], bvm.handle,
+         1 if mark else 0, _ptr(counts), _stream())
+    return counts
+
+
+def make_arm(spec: dict) -> Arm:
+    """Pack an arm description (dict of lists) into the C struct."""
+    arm = Arm()
+    arm.n_joints = int(spec["n_joints"])
+    arm.n_spheres = int(len(spec["r"]))
+    for i, v in enumerate(spec["base"]):
+        arm.base[i] = float(v)
+    for j in range(arm.n_joints):
+        arm.theta[j] = float(spec["theta"][j])
+        arm.d[j] = float(spec["d"][j])
+        arm.a[j] = float(spec["a"][j])
+        arm.alpha[j] = float(spec["alpha"][j])
+    for s in range(arm.n_spheres):
+        arm.link[s] = int(spec["link"][s])
+        arm.t[s] = float(spec["t"][s])
+        arm.r[s] = float(spec["r"][s])
+    return arm

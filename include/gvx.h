@@ -1,0 +1,215 @@
+/*
+ * gvx.h -- C ABI of the B200 distance-field collision engine.
+ *
+ * Plain pointers and sizes only.  Every call returns a gvx_status; a
+ * non-zero status leaves a message in gvx_last_error() (per thread).
+ * Device pointers (d_*) are caller-owned device memory; host pointers (h_*)
+ * are caller-owned host memory.  Calls taking a `stream` are stream-ordered
+ * and asynchronous unless their comment says otherwise; pass 0 for the
+ * legacy default stream.
+ *
+ * Each entry point names the reference interface it replaces
+ * (GV = packages/gpu_voxels/src/gpu_voxels/ in gpu-voxels).
+ *
+ * Value formats (identical to the reference):
+ *   DistanceVoxel : uint32  x | y<<10 | z<<20, 0x3FFFFFFF = uninitialised
+ *                   (GV/voxel/DistanceVoxel.hpp:31-65, GV/helpers/common_defines.h:113-131)
+ *   BitVoxel<256> : 32 bytes, bit k = BitVoxelMeaning k (GV/helpers/BitVector.h:349-350)
+ *   linear id     : z*X*Y + y*X + x (GV/voxelmap/kernels/VoxelMapOperations.h:44-49)
+ *   points        : float32 xyz triples in metres (Vector3f, GV/helpers/cuda_vectors.h:192-203)
+ */
+#ifndef GVX_H_
+#define GVX_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GVX_API __attribute__((visibility("default")))
+#else
+#define GVX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gvx_status {
+  GVX_OK = 0,
+  GVX_ERR_INVALID_ARG = 1,  /* null pointer, bad enum, mismatched dims */
+  GVX_ERR_OUT_OF_DOMAIN = 2,/* dims outside [1,1023] per axis, too many voxels */
+  GVX_ERR_OOM = 3,          /* device allocation failed */
+  GVX_ERR_CUDA = 4,         /* a CUDA runtime call failed */
+  GVX_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+  GVX_ERR_NO_DEVICE = 6     /* no CUDA device with compute capability 10.x */
+} gvx_status;
+
+typedef struct gvx_dims { uint32_t x, y, z; } gvx_dims;
+
+/* Opaque handles. */
+typedef struct gvx_dvm gvx_dvm;   /* DistanceVoxelMap */
+typedef struct gvx_bvm gvx_bvm;   /* BitVectorVoxelMap (BitVoxelMap<256>) */
+typedef struct gvx_blist gvx_blist; /* BitVectorVoxelList */
+
+typedef void *gvx_stream; /* cudaStream_t */
+
+/* ---- library ----------------------------------------------------------- */
+GVX_API const char *gvx_last_error(void);
+GVX_API const char *gvx_version(void);
+/* Replaces cuTestAndInitDevice (GV/helpers/cuda_handling.cu:102-130): select
+ * the device, check it is a compute-capability-10 part. */
+GVX_API gvx_status gvx_init_device(int device);
+
+/* ---- DistanceVoxelMap (GV/voxelmap/DistanceVoxelMap.h) ------------------ */
+
+/* Replaces DistanceVoxelMap(dim, side, MT_DISTANCE_VOXELMAP) ->
+ * TemplateVoxelMap ctor (GV/voxelmap/TemplateVoxelMap.hpp:62-144).  The map
+ * is cleared (all voxels uninitialised).  Dims must be in [1,1023] per axis. */
+GVX_API gvx_status gvx_dvm_create(const gvx_dims *dims, float voxel_side, gvx_dvm **out);
+/* Wraps caller-owned device memory, like the non-owning ctor
+ * TemplateVoxelMap(Voxel* dev_data, ...) (TemplateVoxelMap.hpp:145-154). */
+GVX_API gvx_status gvx_dvm_wrap(const gvx_dims *dims, float voxel_side, uint32_t *d_voxels, gvx_dvm **out);
+GVX_API gvx_status gvx_dvm_destroy(gvx_dvm *m);
+GVX_API gvx_status gvx_dvm_info(const gvx_dvm *m, gvx_dims *dims, float *voxel_side, uint32_t **d_voxels);
+
+/* Replaces TemplateVoxelMap<DistanceVoxel>::clearMap (TemplateVoxelMap.hpp:244-271). */
+GVX_API gvx_status gvx_dvm_clear(gvx_dvm *m, gvx_stream stream);
+
+/* Replaces TemplateVoxelMap::insertPointCloud(const Vector3f*, uint32_t, eBVM_OCCUPIED)
+ * (TemplateVoxelMap.hpp:689-709) with kernelInsertGlobalPointCloud<DistanceVoxel>
+ * (GV/voxelmap/kernels/VoxelMapOperations.hpp:266-300).  d_xyz: n float triples
+ * on the device.  d_outside (optional, device uint32): set to 1 when a point
+ * fell outside the map (the reference's points_outside_map flag). */
+GVX_API gvx_status gvx_dvm_insert_points(gvx_dvm *m, const float *d_xyz, uint64_t n, uint32_t *d_outside, gvx_stream stream);
+
+/* Replaces DistanceVoxelMap::parallelBanding3D(m1,m2,m3,...)
+ * (GV/voxelmap/DistanceVoxelMap.hpp:284-645).  Exact EDT in place: every
+ * voxel ends up holding its nearest obstacle site, bit-identical to the
+ * reference with band counts (1,1,1).  The band counts are accepted for
+ * API compatibility; results never depend on them. */
+GVX_API gvx_status gvx_dvm_edt(gvx_dvm *m, uint32_t m1, uint32_t m2, uint32_t m3, gvx_stream stream);
+/* One sweep of the EDT (0: z, 1: y, 2: x), in the order gvx_dvm_edt runs
+ * them; for per-pass timing and tests.  Pass 0 alone equals the reference's
+ * phase 1 (kernelPBAphase1FloodZ, GV/voxelmap/kernels/VoxelMapOperationsPBA.hpp:63-124). */
+GVX_API gvx_status gvx_dvm_edt_pass(gvx_dvm *m, int pass, gvx_stream stream);
+
+/* Replaces DistanceVoxelMap::getSquaredDistances(device_ptr<uint> b, e, device_ptr<int32_t> out)
+ * (DistanceVoxelMap.hpp:741-752): squared voxel distance to the nearest site
+ * at each linear id; INT32_MAX when the map has no site or the id is out of range. */
+GVX_API gvx_status gvx_dvm_sqdist(const gvx_dvm *m, const uint32_t *d_ids, uint64_t n, int32_t *d_out, gvx_stream stream);
+/* Replaces DistanceVoxelMap::getDistances (DistanceVoxelMap.hpp:786-797): int32(sqrtf(sqdist)). */
+GVX_API gvx_status gvx_dvm_dist(const gvx_dvm *m, const uint32_t *d_ids, uint64_t n, int32_t *d_out, gvx_stream stream);
+/* Replaces TemplateVoxelMap::gatherVoxelsByIndex (TemplateVoxelMap.hpp:381-388). */
+GVX_API gvx_status gvx_dvm_gather(const gvx_dvm *m, const uint32_t *d_ids, uint64_t n, uint32_t *d_out, gvx_stream stream);
+/* Whole-map squared distances (the voxel-wise form of SquaredDistanceFunctor). */
+GVX_API gvx_status gvx_dvm_sqdist_map(const gvx_dvm *m, int32_t *d_out, gvx_stream stream);
+
+/* ---- continuous queries (no reference counterpart; new in this library) -- */
+
+/* Trilinear distance (metres) at continuous points (metres) and its spatial
+ * gradient.  Voxel i's centre is (i + 0.5) * side (getVoxelCenter,
+ * GV/voxelmap/kernels/VoxelMapOperations.h:175-182); corner distances are
+ * sqrt(sqdist) * side; points are clamped to the centre lattice.
+ * d_grad (optional): n*3 floats. */
+GVX_API gvx_status gvx_query_trilinear(const gvx_dvm *m, const float *d_xyz, uint64_t n, float *d_dist, float *d_grad,
+                               gvx_stream stream);
+/* Adjoint: d_grad_xyz[i] = d_grad_dist[i] * grad d(x_i); recomputes the gathers. */
+GVX_API gvx_status gvx_query_trilinear_bwd(const gvx_dvm *m, const float *d_xyz, uint64_t n, const float *d_grad_dist,
+                                   float *d_grad_xyz, gvx_stream stream);
+
+/* Serial-chain arm in the reference's DH convention
+ * (KinematicLink::convertDHtoM, GV/robot/dh_robot/KinematicLink.cu:24-79):
+ * T_j = Rz(theta_j + q_j) Tz(d_j) Tx(a_j) Rx(alpha_j).  Spheres sit on links:
+ * sphere s lies on link link[s] at fraction t[s] of the segment from the
+ * link's start frame origin to its end frame origin, radius r[s]. */
+#define GVX_MAX_JOINTS 16
+#define GVX_MAX_SPHERES 256
+typedef struct gvx_arm {
+  int32_t n_joints;
+  int32_t n_spheres;
+  float base[16];                 /* row-major 4x4 base transform */
+  float theta[GVX_MAX_JOINTS], d[GVX_MAX_JOINTS], a[GVX_MAX_JOINTS], alpha[GVX_MAX_JOINTS];
+  int32_t link[GVX_MAX_SPHERES];
+  float t[GVX_MAX_SPHERES], r[GVX_MAX_SPHERES];
+} gvx_arm;
+
+/* Per configuration: min over spheres of (trilinear distance at the centre - radius).
+ * d_q: n_cfg * n_joints floats.  d_out: n_cfg floats. */
+GVX_API gvx_status gvx_sphere_clearance(const gvx_dvm *m, const gvx_arm *arm, const float *d_q, uint64_t n_cfg, float *d_out,
+                                gvx_stream stream);
+/* Hinge cost per trajectory: sum over waypoints and spheres of
+ * max(0, margin - (d(centre) - r)).  d_q: n_traj * n_wp * n_joints.
+ * d_cost: n_traj floats. */
+GVX_API gvx_status gvx_traj_cost(const gvx_dvm *m, const gvx_arm *arm, const float *d_q, uint64_t n_traj, uint32_t n_wp,
+                         float margin, float *d_cost, gvx_stream stream);
+/* Adjoint of gvx_traj_cost: d_grad_q = d_grad_cost[traj] * dcost/dq, with the
+ * forward kinematics recomputed (nothing is stored by the forward). */
+GVX_API gvx_status gvx_traj_cost_bwd(const gvx_dvm *m, const gvx_arm *arm, const float *d_q, uint64_t n_traj, uint32_t n_wp,
+                             float margin, const float *d_grad_cost, float *d_grad_q, gvx_stream stream);
+
+/* ---- BitVectorVoxelMap (GV/voxelmap/BitVoxelMap.h) ---------------------- */
+
+/* Replaces BitVoxelMap<256>(dim, side, MT_BITVECTOR_VOXELMAP).  Unlike the
+ * reference (32-bit byte limit, TemplateVoxelMap.hpp:71-81) a 512^3 map is allowed. */
+GVX_API gvx_status gvx_bvm_create(const gvx_dims *dims, float voxel_side, gvx_bvm **out);
+GVX_API gvx_status gvx_bvm_destroy(gvx_bvm *m);
+GVX_API gvx_status gvx_bvm_info(const gvx_bvm *m, gvx_dims *dims, float *voxel_side, uint8_t **d_voxels);
+/* Replaces TemplateVoxelMap<BitVectorVoxel>::clearMap. */
+GVX_API gvx_status gvx_bvm_clear(gvx_bvm *m, gvx_stream stream);
+/* Replaces insertPointCloud with kernelInsertGlobalPointCloud<BitVoxel>
+ * (VoxelMapOperations.hpp:241-264): sets bit `meaning` (0..255). */
+GVX_API gvx_status gvx_bvm_insert_points(gvx_bvm *m, const float *d_xyz, uint64_t n, uint32_t meaning, uint32_t *d_outside,
+                                 gvx_stream stream);
+/* Replaces BitVoxelMap::collideWith(const BitVectorVoxelMap*, thr, offset)
+ * (GV/voxelmap/BitVoxelMap.hpp:198-203 -> TemplateVoxelMap.hpp:588-621 ->
+ * kernelCollideVoxelMapsDebug, VoxelMapOperations.hpp:129-184, DefaultCollider
+ * GV/voxel/DefaultCollider.hpp:76-81).  Counts voxels i where self[i+off] and
+ * other[i] both hold a meaning other than eBVM_FREE; off is the linear form of
+ * `offset`; pairs whose shifted index leaves the map are skipped.  With
+ * mark != 0 colliding self voxels get eBVM_COLLISION.  *d_count (device
+ * uint64) receives the count. */
+GVX_API gvx_status gvx_bvm_collide(gvx_bvm *self, const gvx_bvm *other, const int32_t offset[3], int mark, uint64_t *d_count,
+                           gvx_stream stream);
+
+/* ---- BitVectorVoxelList (GV/voxellist/BitVoxelList.h) ------------------- */
+
+/* Replaces BitVoxelList<256,uint32>(dim, side, MT_BITVECTOR_VOXELLIST). */
+GVX_API gvx_status gvx_blist_create(const gvx_dims *ref_dims, float voxel_side, gvx_blist **out);
+GVX_API gvx_status gvx_blist_destroy(gvx_blist *l);
+/* Number of (unique) entries; synchronises the list's last update. */
+GVX_API gvx_status gvx_blist_size(const gvx_blist *l, uint64_t *n);
+GVX_API gvx_status gvx_blist_data(const gvx_blist *l, uint32_t **d_ids, uint8_t **d_voxels);
+GVX_API gvx_status gvx_blist_clear(gvx_blist *l);
+/* Replaces TemplateVoxelList::insertPointCloud (GV/voxellist/TemplateVoxelList.hpp:363-393):
+ * voxelise, drop out-of-bounds, sort and merge duplicates (make_unique, :143-212).
+ * Blocking. */
+GVX_API gvx_status gvx_blist_insert_points(gvx_blist *l, const float *d_xyz, uint64_t n, uint32_t meaning, gvx_stream stream);
+/* Set the list to already-sorted unique ids with their voxels (device
+ * arrays, copied).  n_voxels == 0 means every voxel gets bit `meaning`. */
+GVX_API gvx_status gvx_blist_set(gvx_blist *l, const uint32_t *d_ids, const uint8_t *d_voxels, uint64_t n, uint32_t meaning,
+                         gvx_stream stream);
+/* Replaces BitVoxelList::collideWith(const BitVectorVoxelMap*, thr, offset)
+ * (BitVoxelList.hpp:71-77 -> TemplateVoxelList.hpp:1170-1213 ->
+ * kernelCollideWithVoxelMap, GV/voxellist/kernels/VoxelListOperations.hpp:146-197).
+ * Returns GVX_ERR_INVALID_ARG when the map's dims differ from the list's
+ * reference dims (the reference returns SSIZE_MAX). */
+GVX_API gvx_status gvx_blist_collide_bvm(gvx_blist *l, const gvx_bvm *map, const int32_t offset[3], int mark, uint64_t *d_count,
+                                 gvx_stream stream);
+/* Replaces BitVoxelList::collideWith(const BitVectorVoxelList*, thr, offset)
+ * (BitVoxelList.hpp:79-92 -> collideVoxellists, TemplateVoxelList.hpp:231-289):
+ * number of this list's ids present in `other`.  Non-zero offsets are
+ * rejected, as in the reference (:248-251). */
+GVX_API gvx_status gvx_blist_collide_blist(const gvx_blist *l, const gvx_blist *other, const int32_t offset[3],
+                                   uint64_t *d_count, gvx_stream stream);
+
+/* Batched list-vs-map collision (no reference counterpart; the reference
+ * runs one launch per list): n_lists CSR lists over concatenated arrays,
+ * list k = entries [d_offsets[k], d_offsets[k+1]).  Ids must be < the map's
+ * voxel count to be tested.  d_counts: n_lists uint64, overwritten.  One launch. */
+GVX_API gvx_status gvx_lists_collide_bvm(const uint32_t *d_ids, uint8_t *d_voxels, const uint64_t *d_offsets, uint32_t n_lists,
+                                 uint64_t n_total, const gvx_bvm *map, int mark, uint64_t *d_counts, gvx_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GVX_H_ */

@@ -1,0 +1,344 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the CPU oracle (liboracle.so)
+and of the reference-kernel build (_ref/libgvref.so).
+
+Only the test suite, the smoke entry and the benchmark's CPU-baseline leg
+may import this module; the product never does.  Every function restates a
+gpu-voxels routine; see gvx_oracle.c for the file:line each one follows.
+The FP64 restatements of the continuous queries (trilinear distance, DH
+forward kinematics, sphere clearance, hinge cost) live here in numpy.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+DV_UNINIT = 0x3FFFFFFF
+INT_MAX = 2147483647
+
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS")
+
+
+def build():
+    """Compile liboracle.so (gcc, OpenMP) in place."""
+    subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
+
+
+def build_ref():
+    """Compile _ref/libgvref.so from the reference source tree when present."""
+    src = "/root/reference/packages/gpu_voxels/src"
+    if not os.path.isdir(src):
+        return False
+    subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_SRC={src}"], check=True)
+    return True
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.orc_coord_to_voxel.argtypes = [ctypes.c_float, ctypes.c_float]
+        L.orc_coord_to_voxel.restype = ctypes.c_uint32
+        L.orc_dvm_insert.argtypes = [_u32p, _u32p, ctypes.c_float, _f32p, ctypes.c_uint64]
+        L.orc_dvm_insert.restype = ctypes.c_int
+        L.orc_pba.argtypes = [_u32p, _u32p]
+        L.orc_pba.restype = ctypes.c_int
+        L.orc_pba_reference_order.argtypes = [_u32p, _u32p]
+        L.orc_pba_reference_order.restype = ctypes.c_int
+        L.orc_pba_phase1.argtypes = [_u32p, _u32p]
+        L.orc_pba_isect.argtypes = [ctypes.c_int] * 8
+        L.orc_pba_isect.restype = ctypes.c_float
+        L.orc_sqdist.argtypes = [_u32p, _u32p, _u32p, ctypes.c_uint64, _i32p]
+        L.orc_dist.argtypes = [_u32p, _u32p, _u32p, ctypes.c_uint64, _i32p]
+        L.orc_sqdist_map.argtypes = [_u32p, _u32p, _i32p]
+        L.orc_brute_sqdist.argtypes = [_u32p, _u32p, _i32p]
+        L.orc_bvm_insert.argtypes = [_u8p, _u32p, ctypes.c_float, _f32p, ctypes.c_uint64, ctypes.c_uint32]
+        L.orc_bvm_insert.restype = ctypes.c_int
+        L.orc_bvm_collide.argtypes = [_u8p, _u8p, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int]
+        L.orc_bvm_collide.restype = ctypes.c_uint64
+        L.orc_bvm_collide_count_omp.argtypes = [_u8p, _u8p, ctypes.c_uint64]
+        L.orc_bvm_collide_count_omp.restype = ctypes.c_uint64
+        L.orc_list_collide_map.argtypes = [_u32p, _u8p, ctypes.c_uint64, _u8p, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int]
+        L.orc_list_collide_map.restype = ctypes.c_uint64
+        L.orc_lists_collide_map_omp.argtypes = [_u32p, _u8p, _u64p, ctypes.c_uint64, _u8p, ctypes.c_uint64, _u64p]
+        L.orc_list_collide_list.argtypes = [_u32p, ctypes.c_uint64, _u32p, ctypes.c_uint64]
+        L.orc_list_collide_list.restype = ctypes.c_uint64
+        L.orc_list_insert.argtypes = [_u32p, _u8p, ctypes.POINTER(ctypes.c_uint64), _u32p, ctypes.c_float, _f32p,
+                                      ctypes.c_uint64, ctypes.c_uint32]
+        L.orc_num_threads.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def ref_lib():
+    """The reference's own kernels (GPU), or None when not built / no GPU."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(_HERE, "_ref", "libgvref.so")
+        if not os.path.exists(path):
+            return None
+        R = ctypes.CDLL(path)
+        R.ref_available.restype = ctypes.c_int
+        R.ref_pba.argtypes = [_u32p, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+        R.ref_pba.restype = ctypes.c_int
+        R.ref_pba_time.argtypes = [_u32p, _u32p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+        R.ref_pba_time.restype = ctypes.c_int
+        R.ref_dvm_insert.argtypes = [_u32p, _u32p, ctypes.c_float, _f32p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int)]
+        R.ref_dvm_insert.restype = ctypes.c_int
+        R.ref_bvm_collide.argtypes = [_u8p, _u8p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]
+        R.ref_bvm_collide.restype = ctypes.c_int
+        _REF = R
+    return _REF
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()
+
+
+def _dims(dims):
+    return np.ascontiguousarray(np.asarray(dims, dtype=np.uint32))
+
+
+def _pts(xyz):
+    return np.ascontiguousarray(np.asarray(xyz, dtype=np.float32).reshape(-1, 3))
+
+
+# ---- DistanceVoxelMap ------------------------------------------------------
+
+def dvm_empty(dims) -> np.ndarray:
+    """clearMap: every voxel uninitialised (flat uint32, x fastest)."""
+    return np.full(int(np.prod(np.asarray(dims, dtype=np.int64))), DV_UNINIT, dtype=np.uint32)
+
+
+def dvm_insert(vmap: np.ndarray, dims, side: float, xyz) -> bool:
+    """kernelInsertGlobalPointCloud<DistanceVoxel>; returns the outside flag."""
+    p = _pts(xyz)
+    return bool(lib().orc_dvm_insert(vmap, _dims(dims), np.float32(side), p, p.shape[0]))
+
+
+def pba(vmap: np.ndarray, dims) -> np.ndarray:
+    """parallelBanding3D(1,1,1) for any dims, in place; returns vmap."""
+    rc = lib().orc_pba(vmap, _dims(dims))
+    if rc != 0:
+        raise ValueError(f"oracle pba rejected dims {dims}")
+    return vmap
+
+
+def pba_reference_order(vmap: np.ndarray, dims) -> np.ndarray:
+    """Literal launch order of parallelBanding3D (needs dims x == y)."""
+    rc = lib().orc_pba_reference_order(vmap, _dims(dims))
+    if rc != 0:
+        raise ValueError("reference order needs x == y")
+    return vmap
+
+
+def phase1(vmap: np.ndarray, dims) -> np.ndarray:
+    lib().orc_pba_phase1(vmap, _dims(dims))
+    return vmap
+
+
+def sqdist(vmap, dims, ids) -> np.ndarray:
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    out = np.empty(ids.shape[0], dtype=np.int32)
+    lib().orc_sqdist(vmap, _dims(dims), ids, ids.shape[0], out)
+    return out
+
+
+def dist(vmap, dims, ids) -> np.ndarray:
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    out = np.empty(ids.shape[0], dtype=np.int32)
+    lib().orc_dist(vmap, _dims(dims), ids, ids.shape[0], out)
+    return out
+
+
+def sqdist_map(vmap, dims) -> np.ndarray:
+    out = np.empty(vmap.shape[0], dtype=np.int32)
+    lib().orc_sqdist_map(vmap, _dims(dims), out)
+    return out
+
+
+def brute_sqdist(inserted, dims) -> np.ndarray:
+    out = np.empty(inserted.shape[0], dtype=np.int32)
+    lib().orc_brute_sqdist(np.ascontiguousarray(inserted, dtype=np.uint32), _dims(dims), out)
+    return out
+
+
+def coord_to_voxel(c: float, side: float) -> int:
+    return int(lib().orc_coord_to_voxel(float(c), float(side)))
+
+
+def isect(*args) -> float:
+    return float(lib().orc_pba_isect(*[int(a) for a in args]))
+
+
+# ---- BitVoxel maps and lists ----------------------------------------------
+
+def bvm_empty(dims) -> np.ndarray:
+    return np.zeros(int(np.prod(np.asarray(dims, dtype=np.int64))) * 32, dtype=np.uint8)
+
+
+def bvm_insert(bmap: np.ndarray, dims, side: float, xyz, meaning: int) -> bool:
+    p = _pts(xyz)
+    return bool(lib().orc_bvm_insert(bmap, _dims(dims), np.float32(side), p, p.shape[0], int(meaning)))
+
+
+def bvm_collide(self_map: np.ndarray, other: np.ndarray, offset_linear: int = 0, mark: bool = True) -> int:
+    n = self_map.shape[0] // 32
+    return int(lib().orc_bvm_collide(self_map, other, n, int(offset_linear), 1 if mark else 0))
+
+
+def bvm_collide_count_omp(self_map: np.ndarray, other: np.ndarray) -> int:
+    return int(lib().orc_bvm_collide_count_omp(self_map, other, self_map.shape[0] // 32))
+
+
+def list_collide_map(ids, list_vox: np.ndarray, bmap: np.ndarray, offset_linear: int = 0, mark: bool = True) -> int:
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    return int(lib().orc_list_collide_map(ids, list_vox, ids.shape[0], bmap, bmap.shape[0] // 32, int(offset_linear),
+                                          1 if mark else 0))
+
+
+def lists_collide_map_omp(ids, list_vox, offsets, bmap) -> np.ndarray:
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    counts = np.zeros(offsets.shape[0] - 1, dtype=np.uint64)
+    lib().orc_lists_collide_map_omp(np.ascontiguousarray(ids, dtype=np.uint32), list_vox, offsets, counts.shape[0], bmap,
+                                    bmap.shape[0] // 32, counts)
+    return counts
+
+
+def list_collide_list(a, b) -> int:
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    b = np.ascontiguousarray(b, dtype=np.uint32)
+    return int(lib().orc_list_collide_list(a, a.shape[0], b, b.shape[0]))
+
+
+def list_insert(ids, vox, dims, side, xyz, meaning):
+    """TemplateVoxelList::insertPointCloud; returns new (ids, voxels)."""
+    p = _pts(xyz)
+    n0 = 0 if ids is None else int(ids.shape[0])
+    cap = n0 + p.shape[0] + 1
+    ids_io = np.zeros(cap, dtype=np.uint32)
+    vox_io = np.zeros(cap * 32, dtype=np.uint8)
+    if n0:
+        ids_io[:n0] = ids
+        vox_io[: n0 * 32] = vox
+    n = ctypes.c_uint64(n0)
+    lib().orc_list_insert(ids_io, vox_io, ctypes.byref(n), _dims(dims), np.float32(side), p, p.shape[0], int(meaning))
+    return ids_io[: n.value].copy(), vox_io[: n.value * 32].copy()
+
+
+# ---- FP64 continuous queries ------------------------------------------------
+
+def decode_sites(vmap: np.ndarray):
+    v = vmap.astype(np.int64)
+    return v & 0x3FF, (v >> 10) & 0x3FF, v >> 20
+
+
+def corner_dist64(vmap: np.ndarray, dims, i, j, k) -> np.ndarray:
+    """sqrt(squaredObstacleDistance) at lattice points, float64, voxel units."""
+    X, Y, _ = (int(d) for d in dims)
+    v = vmap[(k.astype(np.int64) * Y + j) * X + i].astype(np.int64)
+    ox, oy, oz = v & 0x3FF, (v >> 10) & 0x3FF, v >> 20
+    sq = (i - ox) ** 2 + (j - oy) ** 2 + (k - oz) ** 2
+    bad = (ox == 1023) | (oy == 1023) | (oz == 1023)
+    sq = np.where(bad, INT_MAX, sq)
+    return np.sqrt(sq.astype(np.float64))
+
+
+def trilinear64(vmap: np.ndarray, dims, side: float, xyz):
+    """FP64 trilinear distance (metres) and gradient at float points, with the
+    same lattice, clamping and corner convention as the CUDA queries."""
+    p = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
+    side = float(np.float32(side))
+    idx, frac, free = [], [], []
+    for a in range(3):
+        n = int(dims[a])
+        u = p[:, a] / side - 0.5
+        fr = (u >= 0) & (u <= n - 1)
+        uc = np.clip(np.nan_to_num(u, nan=0.0), 0, n - 1)
+        i0 = np.minimum(np.floor(uc).astype(np.int64), max(n - 2, 0))
+        i1 = np.minimum(i0 + 1, n - 1)
+        idx.append((i0, i1))
+        frac.append(uc - i0)
+        free.append(fr)
+    (i0, i1), (j0, j1), (k0, k1) = idx
+    fx, fy, fz = frac
+    D = {}
+    for a, ii in (("0", i0), ("1", i1)):
+        for b, jj in (("0", j0), ("1", j1)):
+            for c, kk in (("0", k0), ("1", k1)):
+                D[a + b + c] = corner_dist64(vmap, dims, ii, jj, kk)
+    e00 = D["000"] + fx * (D["100"] - D["000"])
+    e10 = D["010"] + fx * (D["110"] - D["010"])
+    e01 = D["001"] + fx * (D["101"] - D["001"])
+    e11 = D["011"] + fx * (D["111"] - D["011"])
+    g0 = e00 + fy * (e10 - e00)
+    g1 = e01 + fy * (e11 - e01)
+    d = g0 + fz * (g1 - g0)
+    sx0 = (D["100"] - D["000"]) + fy * ((D["110"] - D["010"]) - (D["100"] - D["000"]))
+    sx1 = (D["101"] - D["001"]) + fy * ((D["111"] - D["011"]) - (D["101"] - D["001"]))
+    gx = np.where(free[0], sx0 + fz * (sx1 - sx0), 0.0)
+    gy = np.where(free[1], (e10 - e00) + fz * ((e11 - e01) - (e10 - e00)), 0.0)
+    gz = np.where(free[2], g1 - g0, 0.0)
+    return d * side, np.stack([gx, gy, gz], axis=1)
+
+
+def dh_matrix64(theta, d, a, alpha, q):
+    """DHParameters::convertDHtoM (GV/robot/dh_robot/KinematicLink.cu:24-79),
+    revolute joint, float64: Rz(theta+q) Tz(d) Tx(a) Rx(alpha)."""
+    ct, st = np.cos(theta + q), np.sin(theta + q)
+    ca, sa = np.cos(alpha), np.sin(alpha)
+    m = np.zeros(q.shape + (4, 4))
+    m[..., 0, 0], m[..., 0, 1], m[..., 0, 2], m[..., 0, 3] = ct, -st * ca, st * sa, a * ct
+    m[..., 1, 0], m[..., 1, 1], m[..., 1, 2], m[..., 1, 3] = st, ct * ca, -ct * sa, a * st
+    m[..., 2, 1], m[..., 2, 2], m[..., 2, 3] = sa, ca, d
+    m[..., 3, 3] = 1.0
+    return m
+
+
+def sphere_centres64(arm: dict, q: np.ndarray) -> np.ndarray:
+    """Chain as KinematicChain::setConfiguration (KinematicChain.cu:104-124):
+    link j spans the origins of F_j = base*A_0*...*A_{j-1} and F_{j+1}."""
+    q = np.asarray(q, dtype=np.float64)
+    J = arm["n_joints"]
+    F = np.broadcast_to(np.asarray(arm["base"], dtype=np.float64).reshape(4, 4), q.shape[:-1] + (4, 4)).copy()
+    origins = [F[..., :3, 3].copy()]
+    for j in range(J):
+        A = dh_matrix64(float(np.float32(arm["theta"][j])), float(np.float32(arm["d"][j])),
+                        float(np.float32(arm["a"][j])), float(np.float32(arm["alpha"][j])), q[..., j])
+        F = F @ A
+        origins.append(F[..., :3, 3].copy())
+    O = np.stack(origins, axis=-2)  # [..., J+1, 3]
+    link = np.asarray(arm["link"], dtype=np.int64)
+    t = np.asarray(arm["t"], dtype=np.float32).astype(np.float64)[:, None]
+    return O[..., link, :] + t * (O[..., link + 1, :] - O[..., link, :])
+
+
+def sphere_clearance64(vmap, dims, side, arm, q) -> np.ndarray:
+    c = sphere_centres64(arm, q)
+    shp = c.shape
+    d, _ = trilinear64(vmap, dims, side, c.reshape(-1, 3))
+    r = np.asarray(arm["r"], dtype=np.float32).astype(np.float64)
+    return (d.reshape(shp[:-1]) - r).min(axis=-1)
+
+
+def traj_cost64(vmap, dims, side, arm, q, margin) -> np.ndarray:
+    """q: [n_traj, n_wp, J] -> cost per trajectory (FP64)."""
+    c = sphere_centres64(arm, q)
+    shp = c.shape
+    d, _ = trilinear64(vmap, dims, side, c.reshape(-1, 3))
+    r = np.asarray(arm["r"], dtype=np.float32).astype(np.float64)
+    clear = d.reshape(shp[:-1]) - r
+    return np.maximum(0.0, float(np.float32(margin)) - clear).sum(axis=(-1, -2))

@@ -1,0 +1,120 @@
+"""GPU parity of voxelisation + EDT + discrete queries against the oracle
+(bit-exact sites, so squared distances and tie-breaking match)."""
+import numpy as np
+import pytest
+import torch
+
+import gvx
+import oracle
+import refgeom
+from gpu_helpers import first_mismatch, gpu_edt, oracle_edt, to_u32
+from gvx import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(dims, side, pts):
+    ins_o, edt_o = oracle_edt(dims, side, pts)
+    ins_g, edt_g, dvm = gpu_edt(dims, side, pts)
+    assert np.array_equal(ins_g, ins_o), first_mismatch(ins_g, ins_o, dims)
+    assert np.array_equal(edt_g, edt_o), first_mismatch(edt_g, edt_o, dims)
+    return dvm, edt_o
+
+
+@pytest.mark.parametrize("dims,seed,npts", [
+    ((64, 64, 64), 0, 300),
+    ((128, 128, 131), 1, 5000),
+    ((32, 32, 32), 2, 1),
+    ((17, 33, 9), 3, 40),
+    ((96, 40, 70), 4, 500),
+    ((1, 50, 50), 5, 20),
+    ((50, 1, 50), 6, 20),
+    ((50, 50, 1), 7, 20),
+    ((33, 65, 129), 8, 2000),
+    ((255, 3, 7), 9, 30),
+    ((200, 200, 20), 10, 20000),
+])
+def test_edt_random_scenes(dims, seed, npts):
+    rng = np.random.default_rng(seed)
+    pts = (rng.random((npts, 3)) * np.asarray(dims)).astype(np.float32)
+    _check(dims, 1.0, pts)
+
+
+def test_edt_tie_rich_lattice():
+    dims = (128, 128, 131)
+    _check(dims, 1.0, refgeom.equidistant_points_fast(10_000, dims, 1.0))
+
+
+def test_edt_special_maps():
+    dims = (64, 64, 40)
+    for pts in [np.zeros((0, 3), np.float32),
+                np.array([[10.5, 20.5, 30.5]], np.float32),
+                np.array([[10.5, 32.5, 20.5], [53.5, 32.5, 20.5]], np.float32),
+                np.array([[5.5, 5.5, 5.5], [25.5, 25.5, 25.5], [45.5, 45.5, 35.5]], np.float32),
+                refgeom.box_of_points((0, 0, 0), (63.5, 63.5, 39.5), 1.0) + np.float32(0.25)]:
+        _check(dims, 1.0, pts)
+
+
+def test_edt_negative_nan_and_outside_points():
+    dims = (40, 40, 40)
+    rng = np.random.default_rng(3)
+    pts = (rng.random((500, 3)) * 50 - 5).astype(np.float32)  # some negative, some beyond the map
+    pts[:7] = np.nan
+    dvm, _ = _check(dims, 1.0, pts)
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    dvm.clearMap()
+    dvm.insertPointCloud(torch.as_tensor(pts), outside=flag)
+    assert int(flag.item()) == 1
+
+
+def test_edt_c1_config():
+    sc = workloads.c1_scene()
+    dvm, edt_o = _check(sc.dims, sc.side, sc.points)
+    ids = workloads.c1_queries()
+    got = dvm.getSquaredDistances(torch.as_tensor(ids.astype(np.int64))).cpu().numpy()
+    assert np.array_equal(got, oracle.sqdist(edt_o, sc.dims, ids))
+    got = dvm.getDistances(torch.as_tensor(ids.astype(np.int64))).cpu().numpy()
+    assert np.array_equal(got, oracle.dist(edt_o, sc.dims, ids))
+    got = to_u32(dvm.gatherVoxelsByIndex(torch.as_tensor(ids.astype(np.int64))))
+    assert np.array_equal(got, edt_o[ids])
+    assert np.array_equal(dvm.squaredDistanceMap().cpu().numpy(), oracle.sqdist_map(edt_o, sc.dims))
+
+
+def test_edt_256_scene_and_repeat_is_deterministic():
+    sc = workloads.c3_scene()
+    dvm, edt_o = _check(sc.dims, sc.side, sc.points)
+    dvm.clearMap()
+    dvm.insertPointCloud(torch.as_tensor(sc.points))
+    dvm.parallelBanding3D()
+    assert np.array_equal(to_u32(dvm.data()), edt_o)
+
+
+def test_edt_twice_matches_oracle_on_already_transformed_map():
+    """Running the EDT on an EDT'd map (a legal reference call sequence)."""
+    dims = (48, 48, 48)
+    rng = np.random.default_rng(11)
+    pts = (rng.random((300, 3)) * 48).astype(np.float32)
+    _, edt_o = oracle_edt(dims, 1.0, pts)
+    again_o = edt_o.copy()
+    oracle.pba(again_o, dims)
+    _, _, dvm = gpu_edt(dims, 1.0, pts)
+    dvm.parallelBanding3D()
+    assert np.array_equal(to_u32(dvm.data()), again_o)
+
+
+def test_edt_c2_512_sqdist_matches_exact_property():
+    """512^3 C2 scene: full bit-exact comparison with the oracle."""
+    pts = workloads.c2_points()
+    dims, side = (512, 512, 512), 0.005
+    ins_o, edt_o = oracle_edt(dims, side, pts)
+    ins_g, edt_g, dvm = gpu_edt(dims, side, pts)
+    assert np.array_equal(ins_g, ins_o), first_mismatch(ins_g, ins_o, dims)
+    assert np.array_equal(edt_g, edt_o), first_mismatch(edt_g, edt_o, dims)
+
+
+def test_sqdist_out_of_range_ids_are_guarded():
+    dims = (16, 16, 16)
+    _, _, dvm = gpu_edt(dims, 1.0, np.array([[1.5, 1.5, 1.5]], np.float32))
+    ids = torch.tensor([0, 16 ** 3 - 1, 16 ** 3, 2 ** 31], dtype=torch.int64)
+    out = dvm.getSquaredDistances(ids).cpu().numpy()
+    assert out[0] == 3 and out[2] == 2147483647 and out[3] == 2147483647

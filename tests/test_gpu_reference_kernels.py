@@ -1,0 +1,93 @@
+"""Three-way check on the GPU: gpu-voxels' own kernels (oracle/_ref, built
+from the reference sources for sm_100a) == CPU oracle == this library, inside
+the reference's PBA domain (x == y, x % 64 == 0)."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import gvx
+import oracle
+import refgeom
+from gpu_helpers import first_mismatch, gpu_edt, oracle_edt, to_u32
+from gvx import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref():
+    R = oracle.ref_lib()
+    if R is None:
+        pytest.skip("oracle/_ref/libgvref.so not built (needs the reference source tree at build time)")
+    return R
+
+
+def _ref_edt(R, ins, dims, m=(1, 1, 1)):
+    out = ins.copy()
+    rc = R.ref_pba(out, np.asarray(dims, dtype=np.uint32), *m)
+    assert rc == 0
+    return out
+
+
+CASES = [
+    ("random64", (64, 64, 64), lambda: (np.random.default_rng(0).random((400, 3)) * 64).astype(np.float32), 1.0),
+    ("random128x131", (128, 128, 131), lambda: (np.random.default_rng(1).random((6000, 3)) * [128, 128, 131]).astype(np.float32), 1.0),
+    ("lattice", (128, 128, 131), lambda: refgeom.equidistant_points_fast(10_000, (128, 128, 131), 1.0), 1.0),
+    ("c1", (128, 128, 128), lambda: workloads.c1_scene().points, 0.01),
+    ("sparse192", (192, 192, 64), lambda: (np.random.default_rng(2).random((50, 3)) * [192, 192, 64]).astype(np.float32), 1.0),
+]
+
+
+@pytest.mark.parametrize("name,dims,gen,side", CASES, ids=[c[0] for c in CASES])
+def test_reference_kernels_equal_oracle_and_library(ref, name, dims, gen, side):
+    pts = gen()
+    ins_o, edt_o = oracle_edt(dims, side, pts)
+    # the reference's own insert kernel
+    ins_r = oracle.dvm_empty(dims)
+    flag = ctypes.c_int(0)
+    assert ref.ref_dvm_insert(ins_r, np.asarray(dims, np.uint32), np.float32(side), np.ascontiguousarray(pts, np.float32),
+                              pts.shape[0], ctypes.byref(flag)) == 0
+    assert np.array_equal(ins_r, ins_o)
+    edt_r = _ref_edt(ref, ins_o, dims)
+    assert np.array_equal(edt_r, edt_o), first_mismatch(edt_r, edt_o, dims)
+    _, edt_g, _ = gpu_edt(dims, side, pts)
+    assert np.array_equal(edt_g, edt_r), first_mismatch(edt_g, edt_r, dims)
+
+
+def test_reference_banded_settings_keep_distances(ref):
+    """Band counts change the reference's tie-breaking (sites) but never the
+    squared distances; the library always returns the (1,1,1) sites."""
+    dims = (128, 128, 128)
+    pts = (np.random.default_rng(5).random((3000, 3)) * 128).astype(np.float32)
+    ins_o, edt_o = oracle_edt(dims, 1.0, pts)
+    sq_o = oracle.sqdist_map(edt_o, dims)
+    for m in [(2, 2, 2), (4, 1, 1), (1, 4, 2), (8, 8, 4)]:
+        edt_r = _ref_edt(ref, ins_o, dims, m)
+        assert np.array_equal(oracle.sqdist_map(edt_r, dims), sq_o), m
+    _, _, dvm = gpu_edt(dims, 1.0, pts, m=4)
+    assert np.array_equal(to_u32(dvm.data()), edt_o)
+
+
+def test_reference_collide_kernel(ref):
+    dims = (64, 64, 64)
+    rng = np.random.default_rng(7)
+    a_pts = (rng.random((20000, 3)) * 64).astype(np.float32)
+    b_pts = (rng.random((20000, 3)) * 64).astype(np.float32)
+    a = oracle.bvm_empty(dims)
+    b = oracle.bvm_empty(dims)
+    oracle.bvm_insert(a, dims, 1.0, a_pts, 1)
+    oracle.bvm_insert(b, dims, 1.0, b_pts, 5)
+    a_ref = a.copy()
+    cnt = ctypes.c_uint64(0)
+    assert ref.ref_bvm_collide(a_ref, b, a.shape[0] // 32, ctypes.byref(cnt)) == 0
+    a_orc = a.copy()
+    assert oracle.bvm_collide(a_orc, b) == cnt.value
+    assert np.array_equal(a_orc, a_ref)
+    ga = gvx.BitVectorVoxelMap(dims, 1.0)
+    gb = gvx.BitVectorVoxelMap(dims, 1.0)
+    ga.insertPointCloud(torch.as_tensor(a_pts), 1)
+    gb.insertPointCloud(torch.as_tensor(b_pts), 5)
+    assert ga.collideWith(gb) == cnt.value
+    assert np.array_equal(ga.voxels().cpu().numpy(), a_ref)
