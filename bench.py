@@ -150,6 +150,192 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# secondary sections (rank 0, after the headline)
+# ---------------------------------------------------------------------------
+
+def _time(fn, reps, warm=2):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps  # ms
+
+
+def section_c1(hbm_peak):
+    import torch
+    import gvx
+    from gvx import workloads
+    sc = workloads.c1_scene()
+    dvm = gvx.DistanceVoxelMap(sc.dims, sc.side)
+    pts = torch.as_tensor(sc.points).cuda()
+    ids = torch.as_tensor(workloads.c1_queries().astype(np.int32)).cuda()
+    out = torch.empty_like(ids)
+    nvox = int(np.prod(sc.dims))
+
+    def edt():
+        dvm.clearMap()
+        dvm.insertPointCloud(pts)
+        dvm.parallelBanding3D()
+
+    ms_edt = _time(edt, 20)
+    ms_q = _time(lambda: dvm.getSquaredDistances(ids, out=out), 50)
+    return {"workload": "128^3 @ 1 cm, 50k box-scene points, 100k squared-distance queries",
+            "voxelise_edt_ms": round(ms_edt, 4), "edt_gvoxel_per_s": round(nvox / ms_edt / 1e6, 3),
+            "queries_per_s": round(ids.numel() / ms_q * 1e3, 1), "query_ms": round(ms_q, 4)}
+
+
+def section_c2_collide(hbm_peak, pts_host):
+    import torch
+    import gvx
+    from gvx import workloads
+    dims = C2_DIMS
+    nvox = int(np.prod(dims))
+    scene = gvx.BitVectorVoxelMap(dims, C2_SIDE)
+    caps = gvx.BitVectorVoxelMap(dims, C2_SIDE)
+    scene.insertPointCloud(torch.as_tensor(pts_host).cuda(), 1)
+    caps.insertPointCloud(torch.as_tensor(workloads.capsule_points()).cuda(), 4)
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ms = _time(lambda: scene.collideWithAsync(caps, (0, 0, 0), True, cnt), 10)
+    achieved = 64.0 * nvox / (ms / 1e3) / 1e9
+    count = int(cnt.item())
+    del scene, caps
+    torch.cuda.empty_cache()
+    return {"workload": "BitVectorVoxelMap 512^3 (depth scene) collideWith 512^3 (64 capsules)",
+            "ms": round(ms, 4), "count": count, "achieved_gbs": round(achieved, 1),
+            "frac_of_hbm": round(achieved / hbm_peak, 4), "algorithmic_bytes": 64 * nvox,
+            "note": "the reference cannot allocate a 512^3 BitVoxelMap (32-bit byte limit)"}
+
+
+def section_c3(hbm_peak):
+    import torch
+    import gvx
+    from gvx import workloads
+    sc = workloads.c3_scene()
+    dvm = gvx.DistanceVoxelMap(sc.dims, sc.side)
+    dvm.insertPointCloud(torch.as_tensor(sc.points).cuda())
+    dvm.parallelBanding3D()
+    arm = gvx.make_arm(workloads.arm_spec())
+    q = torch.as_tensor(workloads.c3_configs()).cuda()
+    n_cfg = q.shape[0]
+    ms_batched = _time(lambda: dvm.sphere_clearance(arm, q), 20)
+    cfg_views = [q[i:i + 1] for i in range(n_cfg)]
+    ms_loop = _time(lambda: [dvm.sphere_clearance(arm, v) for v in cfg_views], 2, warm=1)
+    n_sph = arm.n_spheres
+    res = {"workload": "256^3 @ 1 cm scene; 4096 configs x 56 spheres; 4096 lists of 2k..200k ids",
+           "sphere_queries_per_s": round(n_cfg * n_sph / ms_batched * 1e3, 1),
+           "clearance_batched_ms": round(ms_batched, 4), "clearance_per_config_loop_ms": round(ms_loop, 3),
+           "clearance_speedup_vs_loop": round(ms_loop / ms_batched, 1)}
+    # lists vs the scene BitVoxelMap
+    bmap = gvx.BitVectorVoxelMap(sc.dims, sc.side)
+    bmap.insertPointCloud(torch.as_tensor(sc.points).cuda(), 1)
+    lengths = workloads.list_lengths()
+    ids, offs = workloads.c3_lists_device(lengths, int(np.prod(sc.dims)))
+    n_ids = ids.numel()
+    vox = torch.zeros(n_ids, 32, dtype=torch.uint8, device="cuda")
+    owner = torch.repeat_interleave(torch.arange(len(lengths), device="cuda"), offs[1:] - offs[:-1])
+    meaning = 4 + owner % 200
+    vox.scatter_(1, (meaning // 8).unsqueeze(1), (1 << (meaning % 8)).to(torch.uint8).unsqueeze(1))
+    vox = vox.reshape(-1)
+    counts = torch.empty(len(lengths), dtype=torch.int64, device="cuda")
+    ms_lb = _time(lambda: gvx.lists_collide_map(ids, vox, offs, bmap, counts=counts), 5)
+    offs_h = offs.cpu().numpy()
+    one = torch.empty(1, dtype=torch.int64, device="cuda")
+    lens = offs[1:] - offs[:-1]
+    local_offs = torch.stack([torch.zeros_like(lens), lens], 1).contiguous()  # [n_lists, 2]
+
+    def per_list():
+        for k in range(len(lengths)):
+            a, b = int(offs_h[k]), int(offs_h[k + 1])
+            gvx.lists_collide_map(ids[a:b], vox[a * 32:b * 32], local_offs[k], bmap, counts=one)
+            _ = int(one.item())  # the reference returns each count to the host
+
+    ms_ll = _time(per_list, 1, warm=1)
+    ach = 68.0 * n_ids / (ms_lb / 1e3) / 1e9
+    res.update({"list_ids": int(n_ids), "lists_batched_ms": round(ms_lb, 4),
+                "list_ids_per_s": round(n_ids / ms_lb * 1e3, 1), "lists_achieved_gbs": round(ach, 1),
+                "lists_frac_of_hbm": round(ach / hbm_peak, 4),
+                "lists_per_list_loop_ms": round(ms_ll, 2), "lists_speedup_vs_loop": round(ms_ll / ms_lb, 1),
+                "list_hits_total": int(counts.sum().item())})
+    return res
+
+
+def section_c4(hbm_peak):
+    import torch
+    import gvx
+    from gvx import autograd, workloads
+    sc = workloads.c3_scene()
+    dvm = gvx.DistanceVoxelMap(sc.dims, sc.side)
+    dvm.insertPointCloud(torch.as_tensor(sc.points).cuda())
+    dvm.parallelBanding3D()
+    pts = torch.as_tensor(workloads.c4_points()).cuda()
+    n = pts.shape[0]
+    gout = torch.ones(n, device="cuda")
+
+    def fwd_bwd():
+        d = dvm.trilinear(pts, with_grad=False)
+        return dvm.trilinear_backward(pts, gout)
+
+    ms_fb = _time(fwd_bwd, 20)
+    p = pts.clone().requires_grad_(True)
+
+    def autograd_step():
+        p.grad = None
+        autograd.trilinear_distance(p, dvm).sum().backward()
+
+    ms_ag = _time(autograd_step, 20)
+    arm = gvx.make_arm(workloads.arm_spec())
+    q = torch.as_tensor(workloads.c4_trajectories()).cuda()
+    B, T = q.shape[0], q.shape[1]
+    gc = torch.ones(B, device="cuda")
+
+    def traj():
+        dvm.traj_cost(arm, q, 0.05)
+        dvm.traj_cost_backward(arm, q, 0.05, gc)
+
+    ms_tr = _time(traj, 10)
+    views = [q[i:i + 1] for i in range(B)]
+    gcv = gc[:1]
+
+    def traj_loop():
+        for v in views:
+            dvm.traj_cost(arm, v, 0.05)
+            dvm.traj_cost_backward(arm, v, 0.05, gcv)
+
+    ms_trl = _time(traj_loop, 1, warm=1)
+    bytes_fb = 48 + 60
+    return {"workload": "256^3 map; 1M points trilinear fwd+bwd; 512 x 64 waypoints x 56 spheres hinge cost + adjoint",
+            "trilinear_fwd_bwd_ms": round(ms_fb, 4), "trilinear_queries_with_grad_per_s": round(n / ms_fb * 1e3, 1),
+            "trilinear_achieved_gbs": round(bytes_fb * n / (ms_fb / 1e3) / 1e9, 1),
+            "autograd_step_ms": round(ms_ag, 4),
+            "traj_fwd_bwd_ms": round(ms_tr, 4),
+            "traj_sphere_evals_with_grad_per_s": round(B * T * arm.n_spheres / ms_tr * 1e3, 1),
+            "traj_per_trajectory_loop_ms": round(ms_trl, 2), "traj_speedup_vs_loop": round(ms_trl / ms_tr, 1)}
+
+
+def run_sections(args, hbm_peak, pts_host):
+    import torch
+    out = {}
+    for name, fn in (("c1_128", lambda: section_c1(hbm_peak)),
+                     ("c2_collide_512", lambda: section_c2_collide(hbm_peak, pts_host)),
+                     ("c3_spheres_lists", lambda: section_c3(hbm_peak)),
+                     ("c4_gradients", lambda: section_c4(hbm_peak))):
+        if args.sections not in ("all", "") and name not in args.sections.split(","):
+            continue
+        try:
+            out[name] = fn()
+        except Exception as exc:  # a failing section is reported, not fatal
+            out[name] = {"error": repr(exc)[:300]}
+        torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 
@@ -160,6 +346,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sections", default="all", help="comma list of extra sections or 'none'")
+    ap.add_argument("--map", default="c2", choices=["c2", "c3"],
+                    help="headline map: c2 = 512^3 depth scene (default), c3 = 256^3 box scene")
+    ap.add_argument("--no-baselines", action="store_true", help="skip the CPU and reference-kernel baselines")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -194,8 +383,13 @@ def main():
     stream = torch.cuda.current_stream()
     hbm_peak, peak_kind = _peaks()
 
-    # ---- C2 workload, resident in HBM ------------------------------------
-    pts_host = workloads.c2_points()
+    # ---- headline workload, resident in HBM ------------------------------
+    global C2_DIMS, C2_SIDE
+    if args.map == "c3":  # the 256^3 @ 1 cm box scene (used for small profiling captures)
+        sc = workloads.c3_scene()
+        C2_DIMS, C2_SIDE, pts_host = sc.dims, sc.side, sc.points
+    else:
+        pts_host = workloads.c2_points()
     pts = torch.as_tensor(pts_host).cuda()
     dvm = gvx.DistanceVoxelMap(C2_DIMS, C2_SIDE)
     nvox = int(np.prod(C2_DIMS))
@@ -303,7 +497,7 @@ def main():
         "clocks": clocks.summary(),
     }
 
-    if rank == 0:
+    if rank == 0 and not args.no_baselines:
         # ---- gpu-voxels' own kernels on this GPU (oracle/_ref), same map ----
         try:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -332,12 +526,11 @@ def main():
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
 
+    if rank == 0:
         if args.sections != "none":
-            try:
-                import bench_sections
-                line["sections"] = bench_sections.run_all(args, dvm, pts, hbm_peak)
-            except Exception as exc:
-                line["sections"] = {"error": repr(exc)[:300]}
+            del dvm
+            torch.cuda.empty_cache()
+            line["sections"] = run_sections(args, hbm_peak, pts_host)
         print(json.dumps(line), flush=True)
 
     if dist is not None:

@@ -93,11 +93,13 @@ gvx_status gvx_dvm_create(const gvx_dims* dims, float voxel_side, gvx_dvm** out)
   gvx_status st = check_dims(dims);
   if (st != GVX_OK) return st;
   if (!(voxel_side > 0.0f)) return fail(GVX_ERR_INVALID_ARG, "voxel side must be > 0");
-  gvx_dvm* m = new (std::nothrow) gvx_dvm{*dims, voxel_side, nullptr, true};
+  gvx_dvm* m = new (std::nothrow) gvx_dvm{*dims, voxel_side, nullptr, true, nullptr};
   if (m == nullptr) return fail(GVX_ERR_OOM, "host allocation failed");
   const uint64_t n = num_voxels(*dims);
   cudaError_t e = cudaMalloc(&m->d_vox, n * sizeof(uint32_t) + 16);
+  if (e == cudaSuccess) e = cudaMalloc(&m->d_scratch, edt_scratch_words(*dims) * sizeof(uint32_t));
   if (e != cudaSuccess) {
+    if (m->d_vox) cudaFree(m->d_vox);
     delete m;
     return cuda_status(e, "cudaMalloc(DistanceVoxelMap)");
   }
@@ -105,6 +107,7 @@ gvx_status gvx_dvm_create(const gvx_dims* dims, float voxel_side, gvx_dvm** out)
   if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   if (e != cudaSuccess) {
     cudaFree(m->d_vox);
+    cudaFree(m->d_scratch);
     delete m;
     return cuda_status(e, "clear new DistanceVoxelMap");
   }
@@ -119,8 +122,13 @@ gvx_status gvx_dvm_wrap(const gvx_dims* dims, float voxel_side, uint32_t* d_voxe
   if (st != GVX_OK) return st;
   if (!(voxel_side > 0.0f)) return fail(GVX_ERR_INVALID_ARG, "voxel side must be > 0");
   if (reinterpret_cast<uintptr_t>(d_voxels) % 16 != 0) return fail(GVX_ERR_INVALID_ARG, "voxel buffer must be 16-byte aligned");
-  gvx_dvm* m = new (std::nothrow) gvx_dvm{*dims, voxel_side, d_voxels, false};
+  gvx_dvm* m = new (std::nothrow) gvx_dvm{*dims, voxel_side, d_voxels, false, nullptr};
   if (m == nullptr) return fail(GVX_ERR_OOM, "host allocation failed");
+  cudaError_t e = cudaMalloc(&m->d_scratch, edt_scratch_words(*dims) * sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    delete m;
+    return cuda_status(e, "cudaMalloc(EDT workspace)");
+  }
   *out = m;
   return GVX_OK;
 }
@@ -129,6 +137,10 @@ gvx_status gvx_dvm_destroy(gvx_dvm* m) {
   if (m == nullptr) return GVX_OK;
   cudaError_t e = cudaSuccess;
   if (m->owns && m->d_vox) e = cudaFree(m->d_vox);
+  if (m->d_scratch) {
+    cudaError_t e2 = cudaFree(m->d_scratch);
+    if (e == cudaSuccess) e = e2;
+  }
   delete m;
   return cuda_status(e, "cudaFree(DistanceVoxelMap)");
 }
@@ -155,12 +167,12 @@ gvx_status gvx_dvm_insert_points(gvx_dvm* m, const float* d_xyz, uint64_t n, uin
 gvx_status gvx_dvm_edt(gvx_dvm* m, uint32_t m1, uint32_t m2, uint32_t m3, gvx_stream stream) {
   (void)m1; (void)m2; (void)m3;
   if (m == nullptr) return fail(GVX_ERR_INVALID_ARG, "map is null");
-  return cuda_status(launch_edt(m->d_vox, m->dims, as_stream(stream)), "parallelBanding3D");
+  return cuda_status(launch_edt(m->d_vox, m->d_scratch, m->dims, as_stream(stream)), "parallelBanding3D");
 }
 
 gvx_status gvx_dvm_edt_pass(gvx_dvm* m, int pass, gvx_stream stream) {
   if (m == nullptr || pass < 0 || pass > 2) return fail(GVX_ERR_INVALID_ARG, "map is null or pass not in {0,1,2}");
-  return cuda_status(launch_edt_pass(m->d_vox, m->dims, pass, as_stream(stream)), "EDT pass");
+  return cuda_status(launch_edt_pass(m->d_vox, m->d_scratch, m->dims, pass, as_stream(stream)), "EDT pass");
 }
 
 gvx_status gvx_dvm_sqdist(const gvx_dvm* m, const uint32_t* d_ids, uint64_t n, int32_t* d_out, gvx_stream stream) {

@@ -48,7 +48,13 @@ __device__ __forceinline__ void axis_setup(float p, float side, int n, int& i0, 
   const float hi = (float)(n - 1);
   free_axis = (u >= 0.0f) && (u <= hi);
   const float uc = fminf(fmaxf(u, 0.0f), hi);  // NaN -> 0
-  i0 = min((int)floorf(uc), max(n - 2, 0));
+  i0 = (int)floorf(uc);
+  if (free_axis) {
+    // choose the cell by the sign of the exact residual, not the rounded u
+    if (i0 > 0 && fmaf(-((float)i0 + 0.5f), side, p) < 0.0f) --i0;
+    else if (i0 < n - 1 && fmaf(-((float)i0 + 1.5f), side, p) >= 0.0f) ++i0;
+  }
+  i0 = min(i0, max(n - 2, 0));
   i1 = min(i0 + 1, n - 1);
   if (free_axis) {
     f = __fdiv_rn(fmaf(-((float)i0 + 0.5f), side, p), side);

@@ -5,7 +5,7 @@
 // nearest site, including the reference's tie-breaking -- for any dims in
 // [1,1023]^3 (the reference itself needs x == y and x % 64 == 0).
 //
-// Three sweeps, each one kernel that reads and writes every voxel once:
+// Three sweeps, one kernel each:
 //   pass Z : phase 1 (kernelPBAphase1FloodZ, VoxelMapOperationsPBA.hpp:63-124)
 //            per (x,y) column.
 //   pass Y : phase 2 + 3 (kernelPBAphase2ProximateBackpointers :289-379,
@@ -15,12 +15,15 @@
 //            again; sweeping x directly in the original frame is the same
 //            computation with the roles of the site's x and y fields swapped.
 //
-// Layout: one warp owns 32 adjacent columns and stages them in shared memory
-// (cp.async), so the column walk and the positional proximate-site stack of
-// phases 2/3 live on chip.  Column element (row r, lane l) sits at
-// tile[r * pitch + l]; with pitch % 32 == 0 (passes Z, Y) or pitch == 33
-// (pass X, transposed on load) the sequential walk is bank-conflict free.
-// Each voxel costs 4 B of HBM read + 4 B of write per pass (24 B per EDT).
+// Passes Y and X: one thread per column, a warp owns 32 adjacent columns.
+// The columns stream through shared memory in 32-row chunks (cp.async,
+// double buffered; pass X transposes each 32x32 chunk on the way in), the
+// proximate-site stack of phases 2/3 is the reference's positional stack,
+// kept in a per-map scratch buffer laid out [slice][block][row][lane] so the
+// lanes of a warp push and pop the same row with one 128-byte access, and
+// phase 3 writes each row of the warp's 32 columns with one coalesced store
+// (pass X through a 32x33 staging tile).  The sweep is a chain of dependent
+// steps per column, so the design goal is many columns in flight per SM.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -31,6 +34,10 @@
 namespace gvx {
 namespace {
 
+constexpr int kChunk = 32;        // rows staged per step
+constexpr int kSweepWarps = 8;    // warps per CTA in passes Y and X
+constexpr int kTileWords = 32 * 33;
+
 __device__ __forceinline__ void cp_async4(uint32_t* smem_dst, const uint32_t* gmem_src) {
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem_src) : "memory");
@@ -39,16 +46,19 @@ __device__ __forceinline__ void cp_async16(uint32_t* smem_dst, const uint32_t* g
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // devicePBAintersection3DY (VoxelMapOperationsPBA.hpp:265-276) in a column
-// frame: sites (a, row, c), column at (a0, c0).  Same operation order; the
-// products and sums are exact for coordinates below 1024, so only the IEEE
-// divide and the final add round.  Explicit _rn intrinsics forbid contraction.
+// frame: sites (a, row, c), column at (a0, c0).  Halving is exact, so the
+// reference's "/ 2.0f" is a multiply by 0.5; the products and sums are exact
+// for coordinates below 1024, so only the IEEE divide and the final add
+// round.  The _rn intrinsics forbid any contraction.
 __device__ __forceinline__ float pba_isect(int a1, int r1, int c1, int a2, int r2, int c2, int a0, int c0) {
-  const float aM = __fdiv_rn((float)(a1 + a2), 2.0f);
-  const float rM = __fdiv_rn((float)(r1 + r2), 2.0f);
-  const float cM = __fdiv_rn((float)(c1 + c2), 2.0f);
+  const float aM = __fmul_rn((float)(a1 + a2), 0.5f);
+  const float rM = __fmul_rn((float)(r1 + r2), 0.5f);
+  const float cM = __fmul_rn((float)(c1 + c2), 0.5f);
   const float na = (float)(a2 - a1);
   const float nr = (float)(r2 - r1);
   const float nc = (float)(c2 - c1);
@@ -56,108 +66,14 @@ __device__ __forceinline__ float pba_isect(int a1, int r1, int c1, int a2, int r
   return __fadd_rn(rM, __fdiv_rn(num, nr));
 }
 
-// Stack entry (internal): a | backptr<<10 | c<<20, the reference's packing.
+// Stack entry: a | backptr<<10 | c<<20, the reference's packing.
 struct Site {
-  uint32_t a, b, c;  // a-field, back-pointer (or row for the input), c-field
+  uint32_t a, b, c;
 };
 __device__ __forceinline__ Site unpack(uint32_t e) { return Site{e & 0x3ffu, (e >> 10) & 0x3ffu, e >> 20}; }
 
-// The a-field of an input value: x for pass Y, y for pass X (the transposed frame).
-template <bool kXPass>
-__device__ __forceinline__ uint32_t field_a(uint32_t v) {
-  return kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
-}
-
-// Phase 2 for one column held in shared memory (element r at col[r * pitch]).
-// In place: each row is read before its stack entry overwrites it and
-// back-pointers only reach rows already overwritten, exactly the reference's
-// positional stack (there held in a separate initial_map buffer).
-template <bool kXPass>
-__device__ __forceinline__ void column_phase2(uint32_t* col, int pitch, int L, int a0, int c0) {
-  int last_y = (int)kUninit;  // row of the stack top, UNINIT when empty
-  Site top{kUninit, kUninit, kUninit}, second{kUninit, kUninit, kUninit};
-  float i_top = 0.0f;  // intersection of (second, top); valid when top.b != UNINIT
-  uint32_t cur_a = kUninit;
-  for (int ty = 0; ty < L; ++ty) {
-    const uint32_t v = col[ty * pitch];
-    cur_a = field_a<kXPass>(v);
-    if (cur_a != kUninit) {
-      const uint32_t cur_c = v >> 20;
-      float i2 = 0.0f;
-      bool have_i2 = false;
-      while (top.b != kUninit) {
-        i2 = pba_isect((int)top.a, last_y, (int)top.c, (int)cur_a, ty, (int)cur_c, a0, c0);
-        have_i2 = true;
-        if (i_top < i2) break;
-        last_y = (int)top.b;  // pop: top <- second, second <- *(second.backpointer)
-        top = second;
-        have_i2 = false;
-        if (top.b != kUninit) {
-          second = unpack(col[(int)top.b * pitch]);
-          i_top = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
-        }
-      }
-      if (last_y != (int)kUninit) {  // the new pair (old top, current) gets its intersection
-        i_top = have_i2 ? i2 : pba_isect((int)top.a, last_y, (int)top.c, (int)cur_a, ty, (int)cur_c, a0, c0);
-      }
-      second = top;
-      top = Site{cur_a, (uint32_t)last_y, cur_c};
-      last_y = ty;
-      col[ty * pitch] = dv_pack(top.a, top.b, top.c);
-    }
-  }
-  if (cur_a == kUninit) col[(L - 1) * pitch] = dv_pack(kUninit, (uint32_t)last_y, kUninit);  // tail pointer
-}
-
-// Phase 3 walk: calls emit(ty, site_a, site_row, site_c) for ty = L-1 .. 0.
-template <class Emit>
-__device__ __forceinline__ void column_phase3(const uint32_t* col, int pitch, int L, int a0, int c0, Emit&& emit) {
-  int last_y = L - 1;
-  Site top = unpack(col[last_y * pitch]);
-  Site second{kUninit, kUninit, kUninit};
-  float inter = 0.0f;
-  if (top.a == kUninit) {  // tail pointer
-    last_y = (int)top.b;
-    if (last_y != (int)kUninit) top = unpack(col[last_y * pitch]);
-  }
-  if (top.b != kUninit) {
-    second = unpack(col[(int)top.b * pitch]);
-    inter = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
-  }
-  for (int ty = L - 1; ty >= 0; --ty) {
-    while (top.b != kUninit) {
-      if ((float)ty > inter) break;
-      last_y = (int)top.b;
-      top = second;
-      if (top.b != kUninit) {
-        second = unpack(col[(int)top.b * pitch]);
-        inter = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
-      }
-    }
-    emit(ty, top.a, (uint32_t)last_y, top.c);
-  }
-}
-
-// Stage 32 adjacent columns (x0 .. x0+31) of `rows` rows into tile[r*32 + lane].
-// Row r starts at src + r * stride.  Lanes past the map edge get UNINIT.
-__device__ __forceinline__ void stage_rows32(uint32_t* tile, const uint32_t* src, uint64_t stride, int rows,
-                                             int valid_cols, bool vec16) {
-  const int lane = threadIdx.x & 31;
-  if (vec16) {
-    // 8 chunks of 16 B per row; lane covers chunk (lane & 7) of rows (lane >> 3) + 4k.
-    const int part = lane & 7;
-    for (int r = lane >> 3; r < rows; r += 4) cp_async16(tile + r * 32 + part * 4, src + (uint64_t)r * stride + part * 4);
-  } else if (lane < valid_cols) {
-    for (int r = 0; r < rows; ++r) cp_async4(tile + r * 32 + lane, src + (uint64_t)r * stride + lane);
-  } else {
-    for (int r = 0; r < rows; ++r) tile[r * 32 + lane] = kDvUninit;
-  }
-  cp_async_wait_all();
-  __syncwarp();
-}
-
 // ---------------------------------------------------------------------------
-// pass Z: phase 1 per (x, y) column, m1 = 1.
+// pass Z: phase 1 per (x, y) column, m1 = 1; the whole column in shared memory.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) edt_pass_z(uint32_t* __restrict__ map, int X, int Y, int Z, int warps_per_cta) {
   extern __shared__ __align__(16) uint32_t smem[];
@@ -170,8 +86,16 @@ __global__ void __launch_bounds__(256) edt_pass_z(uint32_t* __restrict__ map, in
   const uint64_t layer = (uint64_t)X * Y;
   uint32_t* tile = smem + (size_t)warp * Z * 32;
   const uint32_t* src = map + (uint64_t)y * X + x0;
-  const bool vec16 = (valid_cols == 32) && ((X & 3) == 0);
-  stage_rows32(tile, src, layer, Z, valid_cols, vec16);
+  if (valid_cols == 32 && (X & 3) == 0) {
+    const int part = lane & 7;
+    for (int r = lane >> 3; r < Z; r += 4) cp_async16(tile + r * 32 + part * 4, src + (uint64_t)r * layer + part * 4);
+  } else if (lane < valid_cols) {
+    for (int r = 0; r < Z; ++r) cp_async4(tile + r * 32 + lane, src + (uint64_t)r * layer + lane);
+  } else {
+    for (int r = 0; r < Z; ++r) tile[r * 32 + lane] = kDvUninit;
+  }
+  cp_async_wait_all();
+  __syncwarp();
 
   // flood forward (in shared memory)
   uint32_t obstacle = kDvUninit;
@@ -196,75 +120,167 @@ __global__ void __launch_bounds__(256) edt_pass_z(uint32_t* __restrict__ map, in
 }
 
 // ---------------------------------------------------------------------------
-// pass Y: phases 2 + 3 per (x, z) column along y.
+// passes Y and X
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) edt_pass_y(uint32_t* __restrict__ map, int X, int Y, int Z, int warps_per_cta) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nxb = (X + 31) >> 5;
-  const long long item = (long long)blockIdx.x * warps_per_cta + warp;
-  if (item >= (long long)nxb * Z) return;
-  const int xb = (int)(item % nxb), z = (int)(item / nxb);
-  const int x0 = xb * 32, valid_cols = min(32, X - x0);
-  const uint64_t layer = (uint64_t)X * Y;
-  uint32_t* tile = smem + (size_t)warp * Y * 32;
-  uint32_t* slice = map + (uint64_t)z * layer + x0;
-  const bool vec16 = (valid_cols == 32) && ((X & 3) == 0);
-  stage_rows32(tile, slice, (uint64_t)X, Y, valid_cols, vec16);
 
-  const int tx = x0 + lane;
-  uint32_t* col = tile + lane;
-  column_phase2<false>(col, 32, Y, tx, z);
-  const bool store = lane < valid_cols;
-  column_phase3(col, 32, Y, tx, z, [&](int ty, uint32_t a, uint32_t row, uint32_t c) {
-    if (store) slice[(uint64_t)ty * X + lane] = dv_pack(a, row, c);
-  });
-}
+// Geometry of one warp's work item.
+struct Sweep {
+  int L;             // column length (rows)
+  int a0_base;       // column coordinate of lane 0 (x0 for pass Y, y0 for pass X)
+  int c0;            // slice (z)
+  int valid;         // valid lanes
+  uint32_t* slice;   // map + z * layer
+  int X;             // map row length
+};
 
-// ---------------------------------------------------------------------------
-// pass X: phases 2 + 3 per (y, z) row along x, in the original frame.
-// Lane l owns row y0 + l; the rows are staged transposed (tile[x*33 + l]) and
-// the results leave through a 32x33 per-warp buffer so stores stay coalesced.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) edt_pass_x(uint32_t* __restrict__ map, int X, int Y, int Z, int warps_per_cta) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nyb = (Y + 31) >> 5;
-  const long long item = (long long)blockIdx.x * warps_per_cta + warp;
-  if (item >= (long long)nyb * Z) return;
-  const int yb = (int)(item % nyb), z = (int)(item / nyb);
-  const int y0 = yb * 32, valid_rows = min(32, Y - y0);
-  const uint64_t layer = (uint64_t)X * Y;
-  const int per_warp = X * 33 + 32 * 33;
-  uint32_t* tile = smem + (size_t)warp * per_warp;
-  uint32_t* stage = tile + X * 33;
-  uint32_t* slice = map + (uint64_t)z * layer + (uint64_t)y0 * X;
-
-  for (int r = 0; r < 32; ++r) {
-    if (r < valid_rows) {
-      for (int x = lane; x < X; x += 32) cp_async4(tile + x * 33 + r, slice + (uint64_t)r * X + x);
+// Issue the cp.async copies of chunk `c` into `tile`.
+template <bool kXPass>
+__device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int c, bool vec16) {
+  const int lane = threadIdx.x & 31;
+  const int r0 = c * kChunk;
+  const int rows = min(kChunk, s.L - r0);
+  if (!kXPass) {
+    // rows r0.. of columns a0_base..a0_base+31: tile[r*32 + lane]
+    const uint32_t* src = s.slice + (uint64_t)r0 * s.X + s.a0_base;
+    if (vec16) {
+      const int part = lane & 7;
+      for (int r = lane >> 3; r < rows; r += 4) cp_async16(tile + r * 32 + part * 4, src + (uint64_t)r * s.X + part * 4);
+    } else if (lane < s.valid) {
+      for (int r = 0; r < rows; ++r) cp_async4(tile + r * 32 + lane, src + (uint64_t)r * s.X + lane);
     } else {
-      for (int x = lane; x < X; x += 32) tile[x * 33 + r] = kDvUninit;
+      for (int r = 0; r < rows; ++r) tile[r * 32 + lane] = kDvUninit;
+    }
+  } else {
+    // x positions r0+lane of rows a0_base+t, transposed: tile[(x - r0) * 33 + t]
+    const uint32_t* src = s.slice + (uint64_t)s.a0_base * s.X + r0 + lane;
+    const bool in_row = lane < rows;
+    for (int t = 0; t < 32; ++t) {
+      if (!in_row) continue;
+      if (t < s.valid) cp_async4(tile + lane * 33 + t, src + (uint64_t)t * s.X);
+      else tile[lane * 33 + t] = kDvUninit;
     }
   }
-  cp_async_wait_all();
-  __syncwarp();
+}
 
-  const int ty0 = y0 + lane;
-  uint32_t* col = tile + lane;
-  column_phase2<true>(col, 33, X, ty0, z);
-  column_phase3(col, 33, X, ty0, z, [&](int tx, uint32_t a, uint32_t row, uint32_t c) {
-    // output in the original frame: x-field = row of the site, y-field = a
-    stage[(tx & 31) * 33 + lane] = dv_pack(row, a, c);
-    if ((tx & 31) == 0) {
-      __syncwarp();
-      const int xb = tx;  // chunk [xb, xb + 31]
-      if (xb + lane < X) {
-        for (int r = 0; r < valid_rows; ++r) slice[(uint64_t)r * X + xb + lane] = stage[lane * 33 + r];
+template <bool kXPass>
+__device__ __forceinline__ uint32_t tile_at(const uint32_t* tile, int r) {
+  const int lane = threadIdx.x & 31;
+  return kXPass ? tile[r * 33 + lane] : tile[r * 32 + lane];
+}
+
+template <bool kXPass>
+__global__ void __launch_bounds__(kSweepWarps * 32, 3) edt_sweep(uint32_t* __restrict__ map, uint32_t* __restrict__ scratch,
+                                                                 int X, int Y, int Z) {
+  extern __shared__ __align__(16) uint32_t s_tiles[];  // [kSweepWarps][2][kTileWords]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cols = kXPass ? Y : X;  // columns per slice
+  const int L = kXPass ? X : Y;
+  const int nblk = (cols + 31) >> 5;
+  const long long item = (long long)blockIdx.x * kSweepWarps + warp;
+  if (item >= (long long)nblk * Z) return;
+  const int blk = (int)(item % nblk), z = (int)(item / nblk);
+  Sweep s;
+  s.L = L;
+  s.a0_base = blk * 32;
+  s.c0 = z;
+  s.valid = min(32, cols - s.a0_base);
+  s.slice = map + (uint64_t)z * X * Y;
+  s.X = X;
+  const bool vec16 = !kXPass && s.valid == 32 && (X & 3) == 0;
+  uint32_t* tiles[2] = {s_tiles + (2 * warp) * kTileWords, s_tiles + (2 * warp + 1) * kTileWords};
+  uint32_t* stk = scratch + ((uint64_t)item * L) * 32 + lane;  // entry of row p: stk[p * 32]
+  const int a0 = s.a0_base + lane;
+  const int c0 = z;
+  const int nchunks = (L + kChunk - 1) / kChunk;
+
+  // ---- phase 2: proximate sites, positional stack with back-pointers ----
+  stage_chunk<kXPass>(tiles[0], s, 0, vec16);
+  cp_async_commit();
+  if (nchunks > 1) stage_chunk<kXPass>(tiles[1], s, 1, vec16);
+  cp_async_commit();
+
+  int last_y = (int)kUninit;  // row of the stack top, UNINIT when empty
+  Site top{kUninit, kUninit, kUninit}, second{kUninit, kUninit, kUninit};
+  float i_top = 0.0f;  // intersection of (second, top); valid when top.b != UNINIT
+  uint32_t cur_a = kUninit;
+  for (int c = 0; c < nchunks; ++c) {
+    cp_async_wait1();
+    __syncwarp();
+    const uint32_t* tile = tiles[c & 1];
+    const int r0 = c * kChunk;
+    const int rows = min(kChunk, L - r0);
+    for (int r = 0; r < rows; ++r) {
+      const int ty = r0 + r;
+      const uint32_t v = tile_at<kXPass>(tile, r);
+      cur_a = kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
+      if (cur_a != kUninit) {
+        const uint32_t cur_c = v >> 20;
+        float i2 = 0.0f;
+        bool have_i2 = false;
+        while (top.b != kUninit) {
+          i2 = pba_isect((int)top.a, last_y, (int)top.c, (int)cur_a, ty, (int)cur_c, a0, c0);
+          have_i2 = true;
+          if (i_top < i2) break;
+          last_y = (int)top.b;  // pop
+          top = second;
+          have_i2 = false;
+          if (top.b != kUninit) {
+            second = unpack(stk[(int)top.b * 32]);
+            i_top = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
+          }
+        }
+        if (last_y != (int)kUninit)
+          i_top = have_i2 ? i2 : pba_isect((int)top.a, last_y, (int)top.c, (int)cur_a, ty, (int)cur_c, a0, c0);
+        second = top;
+        top = Site{cur_a, (uint32_t)last_y, cur_c};
+        last_y = ty;
+        stk[ty * 32] = dv_pack(top.a, top.b, top.c);
       }
-      __syncwarp();
     }
-  });
+    __syncwarp();
+    if (c + 2 < nchunks) stage_chunk<kXPass>(tiles[c & 1], s, c + 2, vec16);
+    cp_async_commit();
+  }
+  cp_async_wait_all();
+  if (cur_a == kUninit) stk[(L - 1) * 32] = dv_pack(kUninit, (uint32_t)last_y, kUninit);  // tail pointer
+
+  // ---- phase 3: walk rows downward, popping sites that fall behind ----
+  float inter = 0.0f;
+  last_y = L - 1;
+  top = unpack(stk[last_y * 32]);
+  if (top.a == kUninit) {
+    last_y = (int)top.b;
+    if (last_y != (int)kUninit) top = unpack(stk[last_y * 32]);
+  }
+  if (top.b != kUninit) {
+    second = unpack(stk[(int)top.b * 32]);
+    inter = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
+  }
+  uint32_t* stage = tiles[0];
+  for (int ty = L - 1; ty >= 0; --ty) {
+    while (top.b != kUninit) {
+      if ((float)ty > inter) break;
+      last_y = (int)top.b;
+      top = second;
+      if (top.b != kUninit) {
+        second = unpack(stk[(int)top.b * 32]);
+        inter = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
+      }
+    }
+    if (!kXPass) {
+      if (lane < s.valid) s.slice[(uint64_t)ty * X + s.a0_base + lane] = dv_pack(top.a, (uint32_t)last_y, top.c);
+    } else {
+      // original frame: x-field = row of the site, y-field = a
+      stage[(ty & 31) * 33 + lane] = dv_pack((uint32_t)last_y, top.a, top.c);
+      if ((ty & 31) == 0) {
+        __syncwarp();
+        if (ty + lane < X) {
+          for (int r = 0; r < s.valid; ++r) s.slice[(uint64_t)(s.a0_base + r) * X + ty + lane] = stage[lane * 33 + r];
+        }
+        __syncwarp();
+      }
+    }
+  }
 }
 
 int g_smem_optin = -1;
@@ -279,39 +295,55 @@ int max_smem_optin() {
   return g_smem_optin;
 }
 
-// Warps per CTA: as many as fit a ~96 KB CTA budget, at most 8.
-int pick_warps(size_t bytes_per_warp) {
-  int w = (int)(98304 / bytes_per_warp);
-  return std::max(1, std::min(8, w));
+cudaError_t launch_pass_z(uint32_t* map, gvx_dims d, cudaStream_t s) {
+  const size_t per_warp = (size_t)d.z * 32 * 4;
+  int w = (int)std::max<size_t>(1, std::min<size_t>(8, 98304 / per_warp));
+  const size_t smem = per_warp * w;
+  if ((int)smem > max_smem_optin()) return cudaErrorInvalidConfiguration;
+  cudaError_t e = cudaFuncSetAttribute(edt_pass_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(edt_pass_z, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  const long long items = (long long)((d.x + 31) / 32) * d.y;
+  edt_pass_z<<<(unsigned)((items + w - 1) / w), 32 * w, smem, s>>>(map, (int)d.x, (int)d.y, (int)d.z, w);
+  return cudaGetLastError();
 }
 
-template <typename K>
-cudaError_t launch_pass(K kernel, uint32_t* map, gvx_dims d, long long items, size_t bytes_per_warp, cudaStream_t s) {
-  const int w = pick_warps(bytes_per_warp);
-  const size_t smem = bytes_per_warp * w;
-  if ((int)smem > max_smem_optin()) return cudaErrorInvalidConfiguration;
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <bool kXPass>
+cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStream_t s) {
+  const long long cols = kXPass ? d.y : d.x;
+  const long long items = ((cols + 31) / 32) * d.z;
+  const int smem = kSweepWarps * 2 * kTileWords * 4;
+  cudaError_t e = cudaFuncSetAttribute(edt_sweep<kXPass>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(edt_sweep<kXPass>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  const long long blocks = (items + w - 1) / w;
-  kernel<<<(unsigned)blocks, 32 * w, smem, s>>>(map, (int)d.x, (int)d.y, (int)d.z, w);
+  edt_sweep<kXPass><<<(unsigned)((items + kSweepWarps - 1) / kSweepWarps), kSweepWarps * 32, smem, s>>>(
+      map, scratch, (int)d.x, (int)d.y, (int)d.z);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_edt_pass(uint32_t* d_vox, gvx_dims d, int pass, cudaStream_t s) {
-  const long long nxb = (d.x + 31) / 32, nyb = (d.y + 31) / 32;
+uint64_t edt_scratch_words(gvx_dims d) {
+  const uint64_t y_pass = (uint64_t)((d.x + 31) / 32) * 32 * d.y * d.z;
+  const uint64_t x_pass = (uint64_t)((d.y + 31) / 32) * 32 * d.x * d.z;
+  return std::max(y_pass, x_pass);
+}
+
+cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s) {
   switch (pass) {
-    case 0: return launch_pass(edt_pass_z, d_vox, d, nxb * d.y, (size_t)d.z * 32 * 4, s);
-    case 1: return launch_pass(edt_pass_y, d_vox, d, nxb * d.z, (size_t)d.y * 32 * 4, s);
-    case 2: return launch_pass(edt_pass_x, d_vox, d, nyb * d.z, ((size_t)d.x * 33 + 32 * 33) * 4, s);
+    case 0: return launch_pass_z(d_vox, d, s);
+    case 1: return launch_sweep<false>(d_vox, d_scratch, d, s);
+    case 2: return launch_sweep<true>(d_vox, d_scratch, d, s);
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_edt(uint32_t* d_vox, gvx_dims d, cudaStream_t s) {
+cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s) {
   for (int pass = 0; pass < 3; ++pass) {
-    cudaError_t e = launch_edt_pass(d_vox, d, pass, s);
+    cudaError_t e = launch_edt_pass(d_vox, d_scratch, d, pass, s);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -44,6 +44,7 @@ struct gvx_dvm {
   float side;
   uint32_t* d_vox;
   bool owns;
+  uint32_t* d_scratch;  // EDT workspace (positional proximate-site stacks), owned
 };
 
 struct gvx_bvm {
@@ -77,8 +78,9 @@ cudaError_t launch_dvm_insert(uint32_t* d_vox, gvx_dims d, float side, const flo
                               uint32_t* d_outside, cudaStream_t s);
 cudaError_t launch_bvm_insert(uint8_t* d_vox, gvx_dims d, float side, const float* d_xyz, uint64_t n, uint32_t meaning,
                               uint32_t* d_outside, cudaStream_t s);
-cudaError_t launch_edt(uint32_t* d_vox, gvx_dims d, cudaStream_t s);
-cudaError_t launch_edt_pass(uint32_t* d_vox, gvx_dims d, int pass, cudaStream_t s);
+uint64_t edt_scratch_words(gvx_dims d);
+cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s);
+cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s);
 cudaError_t launch_dvm_sqdist(const uint32_t* d_vox, gvx_dims d, const uint32_t* d_ids, uint64_t n, int32_t* d_out,
                               int mode, cudaStream_t s);
 cudaError_t launch_dvm_sqdist_map(const uint32_t* d_vox, gvx_dims d, int32_t* d_out, cudaStream_t s);

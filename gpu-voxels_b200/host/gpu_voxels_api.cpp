@@ -1,0 +1,437 @@
+// Implementation of the gpu_voxels C++ API (include/gpu_voxels/*.h) over the
+// gvx C ABI (include/gvx.h).  Every map operation takes the map's recursive
+// timed mutex, like the reference (GV/GpuVoxelsMap.h:289); calls the
+// reference makes blocking (host-vector queries, collideWith counts) block
+// here too, the rest are stream-ordered on the default stream.  Errors are
+// reported as the reference does: a message on stderr and a neutral return
+// value (SSIZE_MAX for a dimension mismatch in list collisions).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <climits>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/gpu_voxels/GpuVoxels.h"
+#include "../../include/gvx.h"
+
+namespace gpu_voxels {
+namespace {
+
+void report(const char* what) { std::fprintf(stderr, "gpu_voxels: %s: %s\n", what, gvx_last_error()); }
+
+bool ok(gvx_status st, const char* what) {
+  if (st == GVX_OK) return true;
+  report(what);
+  return false;
+}
+
+void require(gvx_status st, const char* what) {
+  if (st != GVX_OK) throw std::runtime_error(std::string("gpu_voxels: ") + what + ": " + gvx_last_error());
+}
+
+gvx_dims to_dims(const Vector3ui& d) { return gvx_dims{d.x, d.y, d.z}; }
+
+// Temporary device copy of a host point cloud.
+struct DevicePoints {
+  float* p = nullptr;
+  explicit DevicePoints(const std::vector<Vector3f>& pts) {
+    if (pts.empty()) return;
+    if (cudaMalloc(&p, pts.size() * sizeof(Vector3f)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+    cudaMemcpy(p, pts.data(), pts.size() * sizeof(Vector3f), cudaMemcpyHostToDevice);
+  }
+  ~DevicePoints() { if (p) cudaFree(p); }
+};
+
+template <class T>
+struct DeviceArray {
+  T* p = nullptr;
+  size_t n = 0;
+  explicit DeviceArray(size_t count) : n(count) {
+    if (count && cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+  }
+  ~DeviceArray() { if (p) cudaFree(p); }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// DistanceVoxelMap
+// ---------------------------------------------------------------------------
+namespace voxelmap {
+
+DistanceVoxelMap::DistanceVoxelMap(const Vector3ui dim, const float voxel_side_length, const MapType map_type)
+    : GpuVoxelsMap(map_type, dim, voxel_side_length) {
+  gvx_dims d = to_dims(dim);
+  require(gvx_dvm_create(&d, voxel_side_length, &m_handle), "DistanceVoxelMap");
+}
+
+DistanceVoxelMap::DistanceVoxelMap(Voxel* dev_data, const Vector3ui dim, const float voxel_side_length,
+                                   const MapType map_type)
+    : GpuVoxelsMap(map_type, dim, voxel_side_length) {
+  gvx_dims d = to_dims(dim);
+  require(gvx_dvm_wrap(&d, voxel_side_length, reinterpret_cast<uint32_t*>(dev_data), &m_handle), "DistanceVoxelMap");
+}
+
+DistanceVoxelMap::~DistanceVoxelMap() { gvx_dvm_destroy(m_handle); }
+
+void DistanceVoxelMap::clearMap() {
+  lock_guard g(m_mutex);
+  ok(gvx_dvm_clear(m_handle, nullptr), "clearMap");
+}
+
+void DistanceVoxelMap::insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  DevicePoints d(points);
+  insertPointCloud(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size(), voxel_meaning);
+  cudaDeviceSynchronize();
+}
+
+void DistanceVoxelMap::insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  if (voxel_meaning != eBVM_OCCUPIED) {
+    // DistanceVoxel::insert only knows eBVM_OCCUPIED (GV/voxel/DistanceVoxel.hpp:125-138)
+    std::fprintf(stderr, "gpu_voxels: DistanceVoxelMap only supports eBVM_OCCUPIED; use clearMap to free voxels\n");
+    return;
+  }
+  ok(gvx_dvm_insert_points(m_handle, reinterpret_cast<const float*>(d_points), size, nullptr, nullptr), "insertPointCloud");
+}
+
+size_t DistanceVoxelMap::getMemoryUsage() const { return getVoxelMapSize() * sizeof(Voxel); }
+
+void DistanceVoxelMap::parallelBanding3D(uint32_t m1, uint32_t m2, uint32_t m3, uint32_t, uint32_t, uint32_t, bool) {
+  lock_guard g(m_mutex);
+  ok(gvx_dvm_edt(m_handle, m1, m2, m3, nullptr), "parallelBanding3D");
+  cudaDeviceSynchronize();  // the reference returns with the EDT complete
+}
+
+void DistanceVoxelMap::getSquaredDistances(const uint32_t* b, const uint32_t* e, int32_t* out) {
+  lock_guard g(m_mutex);
+  ok(gvx_dvm_sqdist(m_handle, b, (uint64_t)(e - b), out, nullptr), "getSquaredDistances");
+}
+
+void DistanceVoxelMap::getDistances(const uint32_t* b, const uint32_t* e, int32_t* out) {
+  lock_guard g(m_mutex);
+  ok(gvx_dvm_dist(m_handle, b, (uint64_t)(e - b), out, nullptr), "getDistances");
+}
+
+void DistanceVoxelMap::gatherVoxelsByIndex(const uint32_t* b, const uint32_t* e, Voxel* out) {
+  lock_guard g(m_mutex);
+  ok(gvx_dvm_gather(m_handle, b, (uint64_t)(e - b), reinterpret_cast<uint32_t*>(out), nullptr), "gatherVoxelsByIndex");
+}
+
+static void host_query(gvx_dvm* h, std::vector<uint32_t>& idx, std::vector<int32_t>& out, bool squared) {
+  out.resize(idx.size());
+  if (idx.empty()) return;
+  DeviceArray<uint32_t> di(idx.size());
+  DeviceArray<int32_t> dout(idx.size());
+  cudaMemcpy(di.p, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice);
+  gvx_status st = squared ? gvx_dvm_sqdist(h, di.p, idx.size(), dout.p, nullptr) : gvx_dvm_dist(h, di.p, idx.size(), dout.p, nullptr);
+  if (ok(st, squared ? "getSquaredDistancesToHost" : "getDistancesToHost"))
+    cudaMemcpy(out.data(), dout.p, idx.size() * 4, cudaMemcpyDeviceToHost);
+}
+
+void DistanceVoxelMap::getSquaredDistancesToHost(std::vector<uint32_t>& indices, std::vector<int32_t>& output) {
+  lock_guard g(m_mutex);
+  host_query(m_handle, indices, output, true);
+}
+
+void DistanceVoxelMap::getDistancesToHost(std::vector<uint32_t>& indices, std::vector<int32_t>& output) {
+  lock_guard g(m_mutex);
+  host_query(m_handle, indices, output, false);
+}
+
+DistanceVoxel::pba_dist_t DistanceVoxelMap::getSquaredObstacleDistance(uint32_t x, uint32_t y, uint32_t z) {
+  std::vector<uint32_t> idx(1, (z * m_dim.y + y) * m_dim.x + x);
+  std::vector<int32_t> out;
+  getSquaredDistancesToHost(idx, out);
+  return out.empty() ? MAX_OBSTACLE_DISTANCE : out[0];
+}
+
+DistanceVoxel::pba_dist_t DistanceVoxelMap::getSquaredObstacleDistance(const Vector3ui& p) {
+  return getSquaredObstacleDistance(p.x, p.y, p.z);
+}
+
+DistanceVoxel::pba_dist_t DistanceVoxelMap::getObstacleDistance(uint32_t x, uint32_t y, uint32_t z) {
+  std::vector<uint32_t> idx(1, (z * m_dim.y + y) * m_dim.x + x);
+  std::vector<int32_t> out;
+  getDistancesToHost(idx, out);
+  return out.empty() ? MAX_OBSTACLE_DISTANCE : out[0];
+}
+
+DistanceVoxel::pba_dist_t DistanceVoxelMap::getObstacleDistance(const Vector3ui& p) { return getObstacleDistance(p.x, p.y, p.z); }
+
+DistanceVoxel* DistanceVoxelMap::getDeviceDataPtr() {
+  uint32_t* p = nullptr;
+  gvx_dvm_info(m_handle, nullptr, nullptr, &p);
+  return reinterpret_cast<DistanceVoxel*>(p);
+}
+
+const DistanceVoxel* DistanceVoxelMap::getConstDeviceDataPtr() const {
+  uint32_t* p = nullptr;
+  gvx_dvm_info(m_handle, nullptr, nullptr, &p);
+  return reinterpret_cast<const DistanceVoxel*>(p);
+}
+
+// ---------------------------------------------------------------------------
+// BitVoxelMap<256>
+// ---------------------------------------------------------------------------
+
+template <size_t length>
+BitVoxelMap<length>::BitVoxelMap(const Vector3ui dim, const float voxel_side_length, const MapType map_type)
+    : GpuVoxelsMap(map_type, dim, voxel_side_length) {
+  gvx_dims d = to_dims(dim);
+  require(gvx_bvm_create(&d, voxel_side_length, &m_handle), "BitVoxelMap");
+  if (cudaMalloc(&m_dev_count, sizeof(uint64_t)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+}
+
+template <size_t length>
+BitVoxelMap<length>::~BitVoxelMap() {
+  gvx_bvm_destroy(m_handle);
+  if (m_dev_count) cudaFree(m_dev_count);
+}
+
+template <size_t length>
+void BitVoxelMap<length>::clearMap() {
+  lock_guard g(m_mutex);
+  ok(gvx_bvm_clear(m_handle, nullptr), "clearMap");
+}
+
+template <size_t length>
+void BitVoxelMap<length>::insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  DevicePoints d(points);
+  insertPointCloud(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size(), voxel_meaning);
+  cudaDeviceSynchronize();
+}
+
+template <size_t length>
+void BitVoxelMap<length>::insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  ok(gvx_bvm_insert_points(m_handle, reinterpret_cast<const float*>(d_points), size, (uint32_t)voxel_meaning, nullptr,
+                           nullptr),
+     "insertPointCloud");
+}
+
+template <size_t length>
+size_t BitVoxelMap<length>::getMemoryUsage() const {
+  return getVoxelMapSize() * (length / 8);
+}
+
+template <size_t length>
+size_t BitVoxelMap<length>::collideWith(const BitVoxelMap<length>* map, float, const Vector3i& offset) {
+  std::lock(m_mutex, map->m_mutex);
+  std::lock_guard<std::recursive_timed_mutex> g1(m_mutex, std::adopt_lock);
+  std::lock_guard<std::recursive_timed_mutex> g2(map->m_mutex, std::adopt_lock);
+  const int32_t off[3] = {offset.x, offset.y, offset.z};
+  if (!ok(gvx_bvm_collide(m_handle, map->m_handle, off, 1, m_dev_count, nullptr), "collideWith")) return 0;
+  uint64_t count = 0;
+  cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
+  return (size_t)count;
+}
+
+template <size_t length>
+uint8_t* BitVoxelMap<length>::getDeviceDataPtr() {
+  uint8_t* p = nullptr;
+  gvx_bvm_info(m_handle, nullptr, nullptr, &p);
+  return p;
+}
+
+template class BitVoxelMap<BIT_VECTOR_LENGTH>;
+
+}  // namespace voxelmap
+
+// ---------------------------------------------------------------------------
+// BitVoxelList<256, uint32>
+// ---------------------------------------------------------------------------
+namespace voxellist {
+
+template <size_t length, class ID>
+BitVoxelList<length, ID>::BitVoxelList(const Vector3ui ref_map_dim, const float voxel_side_length, const MapType map_type)
+    : GpuVoxelsMap(map_type, ref_map_dim, voxel_side_length) {
+  gvx_dims d = to_dims(ref_map_dim);
+  require(gvx_blist_create(&d, voxel_side_length, &m_handle), "BitVoxelList");
+  if (cudaMalloc(&m_dev_count, sizeof(uint64_t)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+}
+
+template <size_t length, class ID>
+BitVoxelList<length, ID>::~BitVoxelList() {
+  gvx_blist_destroy(m_handle);
+  if (m_dev_count) cudaFree(m_dev_count);
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::clearMap() {
+  lock_guard g(m_mutex);
+  ok(gvx_blist_clear(m_handle), "clearMap");
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  DevicePoints d(points);
+  insertPointCloud(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size(), voxel_meaning);
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  ok(gvx_blist_insert_points(m_handle, reinterpret_cast<const float*>(d_points), size, (uint32_t)voxel_meaning, nullptr),
+     "insertPointCloud");
+}
+
+template <size_t length, class ID>
+size_t BitVoxelList<length, ID>::getMemoryUsage() const {
+  uint64_t n = 0;
+  gvx_blist_size(m_handle, &n);
+  return (size_t)n * (sizeof(ID) + length / 8);
+}
+
+template <size_t length, class ID>
+Vector3ui BitVoxelList<length, ID>::getDimensions() const {
+  uint64_t n = 0;
+  gvx_blist_size(m_handle, &n);
+  return Vector3ui((uint32_t)n, 1, 1);
+}
+
+template <size_t length, class ID>
+size_t BitVoxelList<length, ID>::collideWith(const voxelmap::BitVoxelMap<length>* map, float, const Vector3i& offset) {
+  if (map->getDimensions() != m_dim) {
+    std::fprintf(stderr, "gpu_voxels: list reference dims differ from the map's; not checking collisions\n");
+    return SSIZE_MAX;
+  }
+  lock_guard g(m_mutex);
+  const int32_t off[3] = {offset.x, offset.y, offset.z};
+  if (!ok(gvx_blist_collide_bvm(m_handle, map->handle(), off, 1, m_dev_count, nullptr), "collideWith")) return 0;
+  uint64_t count = 0;
+  cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
+  return (size_t)count;
+}
+
+template <size_t length, class ID>
+size_t BitVoxelList<length, ID>::collideWith(const BitVoxelList<length, ID>* other, float, const Vector3i& offset) {
+  if (offset != Vector3i()) {
+    std::fprintf(stderr, "gpu_voxels: offset for voxel-list collision not supported\n");
+    return 0;
+  }
+  lock_guard g(m_mutex);
+  const int32_t off[3] = {0, 0, 0};
+  if (!ok(gvx_blist_collide_blist(m_handle, other->m_handle, off, m_dev_count, nullptr), "collideWith")) return 0;
+  uint64_t count = 0;
+  cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
+  return (size_t)count;
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::copyIdsToHost(std::vector<ID>& ids) const {
+  uint64_t n = 0;
+  uint32_t* d = nullptr;
+  gvx_blist_size(m_handle, &n);
+  gvx_blist_data(m_handle, &d, nullptr);
+  ids.resize(n);
+  if (n) cudaMemcpy(ids.data(), d, n * sizeof(ID), cudaMemcpyDeviceToHost);
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::copyVoxelsToHost(std::vector<uint8_t>& voxels) const {
+  uint64_t n = 0;
+  uint8_t* d = nullptr;
+  gvx_blist_size(m_handle, &n);
+  gvx_blist_data(m_handle, nullptr, &d);
+  voxels.resize(n * (length / 8));
+  if (n) cudaMemcpy(voxels.data(), d, voxels.size(), cudaMemcpyDeviceToHost);
+}
+
+template class BitVoxelList<BIT_VECTOR_LENGTH, MapVoxelID>;
+
+}  // namespace voxellist
+
+// ---------------------------------------------------------------------------
+// GpuVoxels facade
+// ---------------------------------------------------------------------------
+
+std::mutex GpuVoxels::s_instance_mutex;
+GpuVoxelsSharedPtr GpuVoxels::s_instance;
+
+GpuVoxels::GpuVoxels() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (gvx_init_device(dev) != GVX_OK) {
+    // the reference exits with code 123 when no suitable GPU is found (GV/GpuVoxels.cpp:33-42)
+    std::fprintf(stderr, "gpu_voxels: %s\n", gvx_last_error());
+  }
+}
+
+GpuVoxels::~GpuVoxels() { m_managed_maps.clear(); }
+
+GpuVoxelsSharedPtr GpuVoxels::getInstance() {
+  std::lock_guard<std::mutex> g(s_instance_mutex);
+  if (!s_instance) s_instance.reset(new GpuVoxels());
+  return s_instance;
+}
+
+void GpuVoxels::initialize(uint32_t dim_x, uint32_t dim_y, uint32_t dim_z, float voxel_side_length) {
+  std::lock_guard<std::recursive_mutex> g(m_mutex);
+  m_dim = Vector3ui(dim_x, dim_y, dim_z);
+  m_voxel_side_length = voxel_side_length;
+}
+
+bool GpuVoxels::addMap(const MapType map_type, const std::string& map_name) {
+  std::lock_guard<std::recursive_mutex> g(m_mutex);
+  if (m_managed_maps.count(map_name)) return false;
+  GpuVoxelsMapSharedPtr map;
+  try {
+    switch (map_type) {
+      case MT_DISTANCE_VOXELMAP: map.reset(new voxelmap::DistanceVoxelMap(m_dim, m_voxel_side_length, map_type)); break;
+      case MT_BITVECTOR_VOXELMAP: map.reset(new BitVectorVoxelMap(m_dim, m_voxel_side_length, map_type)); break;
+      case MT_BITVECTOR_VOXELLIST: map.reset(new BitVectorVoxelList(m_dim, m_voxel_side_length, map_type)); break;
+      default:
+        std::fprintf(stderr, "gpu_voxels: map type %d is outside the distance-field collision path\n", (int)map_type);
+        return false;
+    }
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return false;
+  }
+  m_managed_maps[map_name] = map;
+  return true;
+}
+
+bool GpuVoxels::delMap(const std::string& map_name) {
+  std::lock_guard<std::recursive_mutex> g(m_mutex);
+  return m_managed_maps.erase(map_name) > 0;
+}
+
+GpuVoxelsMapSharedPtr GpuVoxels::getMap(const std::string& map_name) {
+  std::lock_guard<std::recursive_mutex> g(m_mutex);
+  auto it = m_managed_maps.find(map_name);
+  return it == m_managed_maps.end() ? GpuVoxelsMapSharedPtr() : it->second;
+}
+
+bool GpuVoxels::clearMap(const std::string& map_name) {
+  GpuVoxelsMapSharedPtr m = getMap(map_name);
+  if (!m) return false;
+  m->clearMap();
+  return true;
+}
+
+bool GpuVoxels::insertPointCloudIntoMap(const std::vector<Vector3f>& point_cloud, std::string map_name,
+                                        const BitVoxelMeaning voxel_meaning) {
+  GpuVoxelsMapSharedPtr m = getMap(map_name);
+  if (!m) return false;
+  m->insertPointCloud(point_cloud, voxel_meaning);
+  return true;
+}
+
+void GpuVoxels::getDimensions(uint32_t& dim_x, uint32_t& dim_y, uint32_t& dim_z) const {
+  dim_x = m_dim.x;
+  dim_y = m_dim.y;
+  dim_z = m_dim.z;
+}
+
+void GpuVoxels::getDimensions(Vector3ui& dim) const { dim = m_dim; }
+
+void GpuVoxels::getVoxelSideLength(float& voxel_side_length) const { voxel_side_length = m_voxel_side_length; }
+
+}  // namespace gpu_voxels

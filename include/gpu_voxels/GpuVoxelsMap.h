@@ -1,0 +1,53 @@
+// Abstract map of the gpu_voxels C++ API (gpu-voxels GV/GpuVoxelsMap.h:49-290):
+// every map has a type, dimensions, a voxel side length and a recursive timed
+// mutex that each operation takes, like the reference's
+// boost::recursive_timed_mutex (std:: in place of boost::).
+#pragma once
+
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "helpers/common_defines.h"
+#include "helpers/cuda_datatypes.h"
+
+namespace gpu_voxels {
+
+class GpuVoxelsMap {
+ public:
+  GpuVoxelsMap(MapType type, const Vector3ui& dims, float voxel_side_length)
+      : m_map_type(type), m_dim(dims), m_voxel_side_length(voxel_side_length) {}
+  virtual ~GpuVoxelsMap() {}
+
+  GpuVoxelsMap(const GpuVoxelsMap&) = delete;
+  GpuVoxelsMap& operator=(const GpuVoxelsMap&) = delete;
+
+  // Down-cast, as GpuVoxelsMap::as<T>() (GV/GpuVoxelsMap.h:70-87).
+  template <class T>
+  T* as() { return dynamic_cast<T*>(this); }
+  template <class T>
+  const T* as() const { return dynamic_cast<const T*>(this); }
+
+  MapType getMapType() const { return m_map_type; }
+  virtual Vector3ui getDimensions() const { return m_dim; }
+  float getVoxelSideLength() const { return m_voxel_side_length; }
+
+  virtual void clearMap() = 0;
+  virtual void insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) = 0;
+  // Device-resident points (n packed Vector3f on the current device).
+  virtual void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) = 0;
+  // Number of bytes of device memory held by the map.
+  virtual size_t getMemoryUsage() const = 0;
+
+ protected:
+  typedef std::lock_guard<std::recursive_timed_mutex> lock_guard;
+  MapType m_map_type;
+  Vector3ui m_dim;
+  float m_voxel_side_length;
+  mutable std::recursive_timed_mutex m_mutex;
+};
+
+typedef std::shared_ptr<GpuVoxelsMap> GpuVoxelsMapSharedPtr;
+
+}  // namespace gpu_voxels

@@ -1,0 +1,55 @@
+// BitVoxelList<256, MapVoxelID> of the gpu_voxels C++ API (gpu-voxels
+// GV/voxellist/BitVoxelList.h:40-170) over the gvx C ABI: a sorted list of
+// unique voxel ids with 32-byte bit vectors, tied to a reference map's dims.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "../GpuVoxelsMap.h"
+#include "../voxelmap/BitVoxelMap.h"
+
+struct gvx_blist;
+
+namespace gpu_voxels {
+namespace voxellist {
+
+template <size_t length, class VoxelIDType>
+class BitVoxelList : public GpuVoxelsMap {
+  static_assert(length == BIT_VECTOR_LENGTH, "only BitVoxelList<256, uint32> is provided");
+
+ public:
+  BitVoxelList(const Vector3ui ref_map_dim, const float voxel_side_length, const MapType map_type = MT_BITVECTOR_VOXELLIST);
+  ~BitVoxelList() override;
+
+  void clearMap() override;
+  void insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) override;
+  void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) override;
+  size_t getMemoryUsage() const override;
+  // As in the reference, a list's "dimensions" are its length in x.
+  Vector3ui getDimensions() const override;
+
+  // collideWith(const BitVectorVoxelMap*) (GV/voxellist/BitVoxelList.hpp:71-77).
+  // Returns SSIZE_MAX when the map's dims differ from the list's reference dims.
+  size_t collideWith(const voxelmap::BitVoxelMap<length>* map, float coll_threshold = 1.0,
+                     const Vector3i& offset = Vector3i());
+  // collideWith(const BitVectorVoxelList*) (GV/voxellist/BitVoxelList.hpp:79-92):
+  // number of this list's ids present in `other`; offsets are not supported (returns 0).
+  size_t collideWith(const BitVoxelList<length, VoxelIDType>* other, float coll_threshold = 1.0,
+                     const Vector3i& offset = Vector3i());
+
+  // Host copies of the ids and the 32-byte voxels.
+  void copyIdsToHost(std::vector<VoxelIDType>& ids) const;
+  void copyVoxelsToHost(std::vector<uint8_t>& voxels) const;
+  gvx_blist* handle() const { return m_handle; }
+
+ private:
+  gvx_blist* m_handle = nullptr;
+  uint64_t* m_dev_count = nullptr;
+};
+
+extern template class BitVoxelList<BIT_VECTOR_LENGTH, MapVoxelID>;
+
+}  // namespace voxellist
+}  // namespace gpu_voxels

@@ -1,0 +1,48 @@
+// BitVoxelMap<256> of the gpu_voxels C++ API (gpu-voxels
+// GV/voxelmap/BitVoxelMap.h:40-120) over the gvx C ABI: 32-byte bit-vector
+// voxels, point insertion with a meaning, and the collideWith counts.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "../GpuVoxelsMap.h"
+
+struct gvx_bvm;
+
+namespace gpu_voxels {
+namespace voxelmap {
+
+template <size_t length>
+class BitVoxelMap : public GpuVoxelsMap {
+  static_assert(length == BIT_VECTOR_LENGTH, "only BitVoxelMap<256> is provided");
+
+ public:
+  BitVoxelMap(const Vector3ui dim, const float voxel_side_length, const MapType map_type = MT_BITVECTOR_VOXELMAP);
+  ~BitVoxelMap() override;
+
+  void clearMap() override;
+  void insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) override;
+  void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) override;
+  size_t getMemoryUsage() const override;
+
+  // collideWith(const BitVectorVoxelMap*, float, const Vector3i&) (GV/voxelmap/BitVoxelMap.hpp:198-203):
+  // voxels where both maps hold a meaning other than eBVM_FREE, this map
+  // shifted by `offset`; colliding voxels of this map get eBVM_COLLISION.
+  size_t collideWith(const BitVoxelMap<length>* map, float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
+
+  // Raw 32-byte voxels on the device.
+  uint8_t* getDeviceDataPtr();
+  size_t getVoxelMapSize() const { return (size_t)m_dim.x * m_dim.y * m_dim.z; }
+  gvx_bvm* handle() const { return m_handle; }
+
+ private:
+  gvx_bvm* m_handle = nullptr;
+  uint64_t* m_dev_count = nullptr;
+};
+
+extern template class BitVoxelMap<BIT_VECTOR_LENGTH>;
+
+}  // namespace voxelmap
+}  // namespace gpu_voxels

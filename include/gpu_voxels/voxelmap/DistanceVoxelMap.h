@@ -1,0 +1,93 @@
+// DistanceVoxelMap of the gpu_voxels C++ API (gpu-voxels
+// GV/voxelmap/DistanceVoxelMap.h:55-140) over the gvx C ABI.  Voxels are
+// uint32 DistanceVoxels (x | y<<10 | z<<20); parallelBanding3D computes the
+// exact EDT in place with the results of the reference's (1,1,1) banding.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "../GpuVoxelsMap.h"
+
+struct gvx_dvm;
+
+namespace gpu_voxels {
+
+// Host-side view of one DistanceVoxel (GV/voxel/DistanceVoxel.h:51-120).
+class DistanceVoxel {
+ public:
+  typedef int32_t pba_dist_t;
+  typedef uint32_t pba_voxel_t;
+  DistanceVoxel() : m_obstacle(0x3FFFFFFFu) {}
+  explicit DistanceVoxel(pba_voxel_t v) : m_obstacle(v) {}
+  DistanceVoxel(uint32_t x, uint32_t y, uint32_t z) : m_obstacle(x | (y << 10) | (z << 20)) {}
+  Vector3ui getObstacle() const { return Vector3ui(m_obstacle & 0x3ffu, (m_obstacle >> 10) & 0x3ffu, m_obstacle >> 20); }
+  // squaredObstacleDistance (GV/voxel/DistanceVoxel.hpp:40-55)
+  pba_dist_t squaredObstacleDistance(const Vector3i& p) const {
+    const Vector3ui o = getObstacle();
+    if (p.x == PBA_UNINITIALISED_COORD || p.y == PBA_UNINITIALISED_COORD || p.z == PBA_UNINITIALISED_COORD ||
+        (int32_t)o.x == PBA_UNINITIALISED_COORD || (int32_t)o.y == PBA_UNINITIALISED_COORD ||
+        (int32_t)o.z == PBA_UNINITIALISED_COORD)
+      return MAX_OBSTACLE_DISTANCE;
+    const int32_t dx = p.x - (int32_t)o.x, dy = p.y - (int32_t)o.y, dz = p.z - (int32_t)o.z;
+    return dx * dx + dy * dy + dz * dz;
+  }
+  pba_voxel_t raw() const { return m_obstacle; }
+
+ private:
+  pba_voxel_t m_obstacle;
+};
+static_assert(sizeof(DistanceVoxel) == 4, "DistanceVoxel is 4 bytes");
+
+namespace voxelmap {
+
+class DistanceVoxelMap : public GpuVoxelsMap {
+ public:
+  typedef DistanceVoxel Voxel;
+
+  DistanceVoxelMap(const Vector3ui dim, const float voxel_side_length, const MapType map_type = MT_DISTANCE_VOXELMAP);
+  // Non-owning: wraps caller-owned device memory of dim.x*dim.y*dim.z voxels.
+  DistanceVoxelMap(Voxel* dev_data, const Vector3ui dim, const float voxel_side_length,
+                   const MapType map_type = MT_DISTANCE_VOXELMAP);
+  ~DistanceVoxelMap() override;
+
+  void clearMap() override;
+  void insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) override;
+  void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) override;
+  size_t getMemoryUsage() const override;
+
+  // Exact EDT (GV/voxelmap/DistanceVoxelMap.hpp:284-645).  Band counts and
+  // block sizes are accepted for source compatibility; the result is always
+  // the reference's (1,1,1) result.
+  void parallelBanding3D(uint32_t m1 = 1, uint32_t m2 = 1, uint32_t m3 = 1,
+                         uint32_t m1_blocksize = PBA_DEFAULT_M1_BLOCK_SIZE,
+                         uint32_t m2_blocksize = PBA_DEFAULT_M2_BLOCK_SIZE,
+                         uint32_t m3_blocksize = PBA_DEFAULT_M3_BLOCK_SIZE, bool detailtimer = false);
+
+  // Queries at linear voxel ids (device pointers; [begin, end) ids -> out).
+  void getSquaredDistances(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, int32_t* dev_output);
+  void getDistances(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, int32_t* dev_output);
+  void gatherVoxelsByIndex(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, Voxel* dev_output);
+  // Host vectors; blocking (GV/voxelmap/DistanceVoxelMap.hpp:726-739,771-784).
+  void getSquaredDistancesToHost(std::vector<uint32_t>& indices, std::vector<int32_t>& output);
+  void getDistancesToHost(std::vector<uint32_t>& indices, std::vector<int32_t>& output);
+  DistanceVoxel::pba_dist_t getSquaredObstacleDistance(const Vector3ui& pos);
+  DistanceVoxel::pba_dist_t getSquaredObstacleDistance(uint32_t x, uint32_t y, uint32_t z);
+  DistanceVoxel::pba_dist_t getObstacleDistance(const Vector3ui& pos);
+  DistanceVoxel::pba_dist_t getObstacleDistance(uint32_t x, uint32_t y, uint32_t z);
+
+  Voxel* getDeviceDataPtr();
+  const Voxel* getConstDeviceDataPtr() const;
+  size_t getVoxelMapSize() const { return (size_t)m_dim.x * m_dim.y * m_dim.z; }
+  gvx_dvm* handle() const { return m_handle; }
+
+ private:
+  gvx_dvm* m_handle = nullptr;
+};
+
+}  // namespace voxelmap
+
+typedef std::shared_ptr<voxelmap::DistanceVoxelMap> DistanceVoxelMapSharedPtr;
+
+}  // namespace gpu_voxels

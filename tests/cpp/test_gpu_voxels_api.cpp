@@ -1,0 +1,166 @@
+// The reference's own test scenarios, written against the gpu_voxels C++ API
+// of this library (include/gpu_voxels/*.h) the way gpu-voxels' Boost tests
+// are written (GV/test/testing_distance.cu, testing_voxelmap.cu,
+// testing_voxellist.cu).  Prints one line per case; exit code = failures.
+#include <cuda_runtime.h>
+#include <limits.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <vector>
+
+#include "../../include/gpu_voxels/GpuVoxels.h"
+
+using namespace gpu_voxels;
+
+static int g_failures = 0;
+#define CHECK(cond, name)                                            \
+  do {                                                               \
+    const bool _ok = (cond);                                         \
+    std::printf("%s %s\n", _ok ? "PASS" : "FAIL", name);             \
+    if (!_ok) ++g_failures;                                          \
+  } while (0)
+
+// createBoxOfPoints (GV/helpers/GeometryGeneration.cpp:90-107), float accumulation.
+static std::vector<Vector3f> box_of_points(Vector3f lo, Vector3f hi, float delta) {
+  std::vector<Vector3f> out;
+  for (float x = lo.x; x <= hi.x; x += delta)
+    for (float y = lo.y; y <= hi.y; y += delta)
+      for (float z = lo.z; z <= hi.z; z += delta) out.push_back(Vector3f(x, y, z));
+  return out;
+}
+
+// createEquidistantPointsInBox (GV/helpers/GeometryGeneration.cpp:237-264).
+static std::vector<Vector3f> equidistant(size_t max_points, Vector3ui dims, float s) {
+  std::vector<Vector3f> out;
+  for (uint32_t i = 0; i < (dims.x - 1) / 2; i++)
+    for (uint32_t j = 0; j < (dims.y - 1) / 2; j++)
+      for (uint32_t k = 0; k < (dims.z - 1) / 2; k++) {
+        if (out.size() >= max_points) return out;
+        out.push_back(Vector3f(i * 2 * s + s / 2.0, j * 2 * s + s / 2.0, k * 2 * s + s / 2.0));
+      }
+  return out;
+}
+
+static void distance_extraction() {
+  // GV/test/testing_distance.cu:129-220
+  const Vector3ui dims(64, 64, 64);
+  voxelmap::DistanceVoxelMap map(dims, 1.f);
+  std::vector<uint32_t> idx = {0, 10, 100, 1000, 10000};
+  std::vector<Vector3f> obstacles;
+  for (uint32_t id : idx)
+    obstacles.push_back(Vector3f((float)(id % 64), (float)((id / 64) % 64), (float)(id / 4096)));
+  map.clearMap();
+  map.insertPointCloud(obstacles, eBVM_OCCUPIED);
+  std::vector<DistanceVoxel> gathered(idx.size());
+  {
+    uint32_t* d_idx = nullptr;
+    DistanceVoxel* d_out = nullptr;
+    cudaMalloc(&d_idx, idx.size() * 4);
+    cudaMalloc(&d_out, idx.size() * 4);
+    cudaMemcpy(d_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice);
+    map.gatherVoxelsByIndex(d_idx, d_idx + idx.size(), d_out);
+    cudaMemcpy(gathered.data(), d_out, idx.size() * 4, cudaMemcpyDeviceToHost);
+    cudaFree(d_idx);
+    cudaFree(d_out);
+  }
+  bool own = true;
+  for (size_t i = 0; i < idx.size(); ++i)
+    own &= gathered[i].getObstacle() == Vector3ui(idx[i] % 64, (idx[i] / 64) % 64, idx[i] / 4096);
+  CHECK(own, "distance_extraction: gatherVoxelsByIndex returns own coordinates");
+  std::vector<int32_t> sq, d, dn;
+  map.getSquaredDistancesToHost(idx, sq);
+  map.getDistancesToHost(idx, d);
+  std::vector<uint32_t> nb(idx);
+  for (auto& v : nb) ++v;
+  map.parallelBanding3D(1, 1, 1);
+  map.getDistancesToHost(nb, dn);
+  bool zero = true, differ = true;
+  for (size_t i = 0; i < idx.size(); ++i) {
+    zero &= sq[i] == 0 && d[i] == 0;
+    differ &= d[i] != dn[i];
+  }
+  CHECK(zero, "distance_extraction: zero distance at obstacles");
+  CHECK(differ, "distance_extraction: neighbour distance differs");
+}
+
+static void distance_correctness() {
+  // GV/test/testing_distance.cu:39-127, PBA against brute force on the lattice
+  const Vector3ui dims(128, 128, 131);
+  voxelmap::DistanceVoxelMap map(dims, 1.f);
+  std::vector<Vector3f> pts = equidistant(10000, dims, 1.f);
+  map.insertPointCloud(pts, eBVM_OCCUPIED);
+  map.parallelBanding3D();
+  // brute force on a sample of voxels
+  std::vector<uint32_t> idx;
+  for (uint32_t i = 0; i < dims.x * dims.y * dims.z; i += 997) idx.push_back(i);
+  std::vector<int32_t> sq;
+  map.getSquaredDistancesToHost(idx, sq);
+  double maxerr = 0;
+  for (size_t k = 0; k < idx.size(); ++k) {
+    const int x = idx[k] % dims.x, y = (idx[k] / dims.x) % dims.y, z = idx[k] / (dims.x * dims.y);
+    int64_t best = INT64_MAX;
+    for (const Vector3f& p : pts) {
+      const int64_t dx = x - (int)p.x, dy = y - (int)p.y, dz = z - (int)p.z;
+      best = std::min(best, dx * dx + dy * dy + dz * dz);
+    }
+    maxerr = std::max(maxerr, std::fabs(std::sqrt((double)best) - std::sqrt((double)sq[k])));
+  }
+  CHECK(maxerr < 0.01, "distance_correctness: PBA vs brute force maxerr < 0.01");
+}
+
+static void collisions() {
+  // GV/test/testing_voxelmap.cu:96-168 with BitVectorVoxelMaps, default dims 89x123x74
+  GpuVoxels::getInstance()->initialize(89, 123, 74, 1.f);
+  GpuVoxelsSharedPtr gvl = GpuVoxels::getInstance();
+  gvl->addMap(MT_BITVECTOR_VOXELMAP, "a");
+  gvl->addMap(MT_BITVECTOR_VOXELMAP, "b");
+  BitVectorVoxelMap* a = gvl->getMap("a")->as<BitVectorVoxelMap>();
+  BitVectorVoxelMap* b = gvl->getMap("b")->as<BitVectorVoxelMap>();
+  std::vector<Vector3f> pts = equidistant(10000, Vector3ui(89, 123, 74), 1.f);
+  gvl->insertPointCloudIntoMap(pts, "a", eBVM_OCCUPIED);
+  gvl->insertPointCloudIntoMap(pts, "b", eBVM_OCCUPIED);
+  CHECK(a->collideWith(b, 0.1f) == 10000, "collision: all points collide");
+  a->clearMap();
+  b->clearMap();
+  a->insertPointCloud(box_of_points(Vector3f(2.1f, 2.1f, 2.1f), Vector3f(4.1f, 4.1f, 4.1f), 0.5f), eBVM_OCCUPIED);
+  b->insertPointCloud(box_of_points(Vector3f(3.1f, 3.1f, 3.1f), Vector3f(5.1f, 5.1f, 5.1f), 0.5f), eBVM_OCCUPIED);
+  CHECK(a->collideWith(b, 0.1f) == 8, "collision_with_offset: 8 without offset");
+  CHECK(a->collideWith(b, 0.1f, Vector3i(-1, 0, -1)) == 18, "collision_with_offset: 18 with negative offset");
+  CHECK(b->collideWith(a, 0.1f, Vector3i(1, 0, 1)) == 18, "collision_with_offset: 18 with positive offset");
+
+  BitVectorVoxelList list(Vector3ui(89, 123, 74), 1.f);
+  list.insertPointCloud(box_of_points(Vector3f(1.1f, 1.1f, 1.1f), Vector3f(3.9f, 3.9f, 3.9f), 0.1f), BitVoxelMeaning(11));
+  list.insertPointCloud(box_of_points(Vector3f(2.1f, 2.1f, 2.1f), Vector3f(4.9f, 4.9f, 4.9f), 0.1f), BitVoxelMeaning(12));
+  CHECK(list.getDimensions().x == 46, "bitvoxellist: 46 unique voxels");
+  BitVectorVoxelMap m(Vector3ui(89, 123, 74), 1.f);
+  m.insertPointCloud(box_of_points(Vector3f(1.1f, 1.1f, 1.1f), Vector3f(3.9f, 3.9f, 3.9f), 0.1f), eBVM_OCCUPIED);
+  m.insertPointCloud(box_of_points(Vector3f(2.1f, 2.1f, 2.1f), Vector3f(4.9f, 4.9f, 4.9f), 0.1f), eBVM_OCCUPIED);
+  CHECK(list.collideWith(&m, 1.0f) == 46, "collide_bitvoxellist_with_bitvoxelmap: 46");
+  CHECK(list.collideWith(&list, 1.0f) == 46, "bitvoxellist vs bitvoxellist: 46");
+  BitVectorVoxelList one(Vector3ui(89, 123, 74), 1.f);
+  std::vector<Vector3f> box = box_of_points(Vector3f(1.1f, 1.1f, 1.1f), Vector3f(3.9f, 3.9f, 3.9f), 0.1f);
+  one.insertPointCloud(box, eBVM_OCCUPIED);
+  BitVectorVoxelMap m2(Vector3ui(89, 123, 74), 1.f);
+  m2.insertPointCloud(box, eBVM_OCCUPIED);
+  const size_t want[] = {27, 27, 18, 18, 9, 9, 0, 0};
+  bool shift_ok = true;
+  int k = 0;
+  for (float shift = 0.0f; shift < 4.0f; shift += 0.5f) shift_ok &= one.collideWith(&m2, 1.0f, Vector3i(shift, 0, 0)) == want[k++];
+  CHECK(shift_ok, "collide_bitvoxellist_with_voxelmap_shifting: 27/18/9/0");
+  BitVectorVoxelMap wrong(Vector3ui(10, 10, 10), 1.f);
+  CHECK(one.collideWith(&wrong, 1.0f) == (size_t)SSIZE_MAX, "list vs map with other dims: SSIZE_MAX");
+  gvl->delMap("a");
+  gvl->delMap("b");
+}
+
+int main() {
+  GpuVoxels::getInstance();
+  distance_extraction();
+  distance_correctness();
+  collisions();
+  std::printf("%d failure(s)\n", g_failures);
+  return g_failures;
+}

@@ -1,0 +1,53 @@
+"""CPU: the oracle reproduces gpu-voxels' own kernel outputs bit for bit
+(fixtures produced on a B200 by tests/golden/make_ref_fixtures.py)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from golden_cases import CASES, points_for
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "ref_*.npz")))
+
+
+def test_fixtures_present():
+    assert any("ref_random64" in f for f in FIXTURES), "golden fixtures missing"
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_matches_reference_kernels(name):
+    path = os.path.join(HERE, f"ref_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip("fixture not generated")
+    f = np.load(path)
+    spec = CASES[name]
+    dims = tuple(int(v) for v in f["dims"])
+    pts = points_for(spec)
+    m = oracle.dvm_empty(dims)
+    outside = oracle.dvm_insert(m, dims, float(f["side"]), pts)
+    assert np.array_equal(m, f["inserted"]), "voxelisation differs from the reference kernel"
+    assert int(outside) == int(f["outside"])
+    oracle.pba(m, dims)
+    assert np.array_equal(m, f["edt"]), f"EDT differs at {int(np.count_nonzero(m != f['edt']))} voxels"
+    lit = f["inserted"].copy()
+    oracle.pba_reference_order(lit, dims)
+    assert np.array_equal(lit, f["edt"])
+
+
+def test_oracle_collision_matches_reference_kernel():
+    path = os.path.join(HERE, "ref_bvm_collide.npz")
+    if not os.path.exists(path):
+        pytest.skip("fixture not generated")
+    f = np.load(path)
+    dims = (64, 64, 64)
+    rng = np.random.default_rng(77)
+    pa = (rng.random((30000, 3)) * 64).astype(np.float32)
+    pb = (rng.random((30000, 3)) * 64).astype(np.float32)
+    a, b = oracle.bvm_empty(dims), oracle.bvm_empty(dims)
+    oracle.bvm_insert(a, dims, 1.0, pa, 1)
+    oracle.bvm_insert(b, dims, 1.0, pb, 33)
+    assert oracle.bvm_collide(a, b) == int(f["count"])
+    assert np.array_equal(a, f["marked"])

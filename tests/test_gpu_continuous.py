@@ -34,9 +34,13 @@ def test_trilinear_matches_fp64(scene):
     d32, g32 = dvm.trilinear(torch.as_tensor(pts))
     d64, g64 = oracle.trilinear64(edt, sc.dims, sc.side, pts)
     err_vox = np.abs(d32.cpu().numpy().astype(np.float64) - d64) / sc.side
-    gerr = np.abs(g32.cpu().numpy().astype(np.float64) - g64)
+    # the gradient jumps across cell faces: compare away from them (where the
+    # FP64 cell choice itself is decided by the last bit)
+    u = pts.astype(np.float64) / np.float64(np.float32(sc.side)) - 0.5
+    on_face = _near_face(u - np.floor(u), 1e-6)
+    gerr = np.abs(g32.cpu().numpy().astype(np.float64) - g64)[~on_face]
     print(f"\ntrilinear FP32 vs FP64: max {err_vox.max():.3e} vox, rms {np.sqrt((err_vox**2).mean()):.3e} vox; "
-          f"grad max {gerr.max():.3e}")
+          f"grad max {gerr.max():.3e} rms {np.sqrt((gerr**2).mean()):.3e} ({int(on_face.sum())} pts on faces skipped)")
     assert err_vox.max() <= DIST_MAX_ERR_VOX
     assert gerr.max() <= GRAD_MAX_ERR
 
@@ -120,3 +124,29 @@ def test_traj_cost_and_adjoint(scene):
     print(f"\ntrajectory adjoint vs FP64 central differences: median rel err {np.median(errs):.2e}, "
           f"90th pct {np.percentile(errs, 90):.2e}")
     assert np.median(errs) < 1e-2
+
+
+def test_torch_autograd_functions(scene):
+    """libtorch torch::autograd::Function wrappers: backward = the adjoint kernels."""
+    from gvx import autograd
+
+    sc, edt, dvm = scene
+    pts = torch.as_tensor(workloads.c4_points(10_000, sc.dims, sc.side)).cuda().requires_grad_(True)
+    d = autograd.trilinear_distance(pts, dvm)
+    w = torch.linspace(0.5, 2.0, d.shape[0], device="cuda")
+    (d * w).sum().backward()
+    _, g = dvm.trilinear(pts.detach())
+    assert torch.allclose(pts.grad, g * w[:, None], atol=0, rtol=0)
+    assert torch.equal(d.detach(), dvm.trilinear(pts.detach(), with_grad=False))
+
+    spec = workloads.arm_spec()
+    arm = gvx.make_arm(spec)
+    q0 = torch.as_tensor(workloads.c3_configs(8)).cuda().requires_grad_(True)
+    q1 = torch.as_tensor(workloads.c3_configs(16)[8:]).cuda()
+    t = torch.linspace(0, 1, 32, device="cuda")[None, :, None]
+    q = q0[:, None, :] + (q1 - q0)[:, None, :] * t          # [8, 32, 7] waypoints
+    cost = autograd.trajectory_cost(q, dvm, arm, 0.05)
+    cost.sum().backward()
+    gq = dvm.traj_cost_backward(arm, q.detach(), 0.05, torch.ones(8, device="cuda"))
+    want = (gq * (1 - t)).sum(1)                               # chain rule through the interpolation
+    assert torch.allclose(q0.grad, want, rtol=1e-5, atol=1e-6)
