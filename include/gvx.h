@@ -93,6 +93,23 @@ GVX_API gvx_status gvx_dvm_edt(gvx_dvm *m, uint32_t m1, uint32_t m2, uint32_t m3
  * phase 1 (kernelPBAphase1FloodZ, GV/voxelmap/kernels/VoxelMapOperationsPBA.hpp:63-124). */
 GVX_API gvx_status gvx_dvm_edt_pass(gvx_dvm *m, int pass, gvx_stream stream);
 
+/* No counterpart in the reference.  The same EDT as gvx_dvm_edt, in place on
+ * caller-owned device voxels (uint32 DistanceVoxels, x fastest, 16-byte
+ * aligned), for callers that may not allocate device memory once running
+ * (real-time control loops, plugins inside a host that owns all device
+ * memory).  It calls no cudaMalloc/cudaFree and no allocating library
+ * routine: its workspace is a 64 MiB array built into the library, held on
+ * every GPU that loads the library's kernels until the process exits.
+ * Limit: the map must need at most 16,777,216 workspace words, i.e. at most
+ * 16,777,216 voxels with x and y rounded up to multiples of 32 (256^3 fits);
+ * larger maps return GVX_ERR_OUT_OF_DOMAIN and are left untouched.
+ * The first call on each device looks up the workspace's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one workspace and no part of it has to start at zero,
+ * but calls that overlap on the GPU (other streams, other threads) race on
+ * it: order them on one stream or synchronise between them. */
+GVX_API gvx_status gvx_dvm_edt_static_workspace(uint32_t *d_voxels, const gvx_dims *dims, gvx_stream stream);
+
 /* Replaces DistanceVoxelMap::getSquaredDistances(device_ptr<uint> b, e, device_ptr<int32_t> out)
  * (DistanceVoxelMap.hpp:741-752): squared voxel distance to the nearest site
  * at each linear id; INT32_MAX when the map has no site or the id is out of range. */
