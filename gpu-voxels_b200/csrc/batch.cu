@@ -1,0 +1,232 @@
+// Batched processing of many DistanceVoxelMaps of uneven dims (no
+// counterpart in gpu-voxels, which handles one map per call with a device
+// synchronisation after every step).
+//
+// A gvx_batch holds a device table of map descriptors.  Clear, voxelisation
+// and trilinear queries run as one launch each over all maps; the EDT runs
+// its three passes over all maps; the whole step (clear -> insert -> EDT ->
+// queries) can be recorded once as a CUDA graph and replayed with a single
+// launch call.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "gvx_internal.cuh"
+#include "trilinear.cuh"
+
+namespace gvx {
+namespace {
+
+// clearMap for every map: CTA row y clears map y.
+__global__ void batch_clear_kernel(const BatchMap* __restrict__ maps) {
+  const BatchMap m = maps[blockIdx.y];
+  const uint64_t n4 = m.nvox / 4;
+  const uint4 u = make_uint4(kDvUninit, kDvUninit, kDvUninit, kDvUninit);
+  uint4* v4 = reinterpret_cast<uint4*>(m.vox);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) __stcs(v4 + i, u);
+  if (blockIdx.x == 0 && threadIdx.x < (m.nvox & 3)) m.vox[n4 * 4 + threadIdx.x] = kDvUninit;
+}
+
+// Map owning item i of a CSR layout: last k with offsets[k] <= i.
+__device__ __forceinline__ uint32_t owner(const uint64_t* __restrict__ offsets, uint32_t n, uint64_t i) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(offsets + mid) <= i) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// kernelInsertGlobalPointCloud<DistanceVoxel> for every map at once: point i
+// belongs to map owner(offsets, i).
+__global__ void batch_insert_kernel(const BatchMap* __restrict__ maps, uint32_t n_maps, const float* __restrict__ xyz,
+                                    const uint64_t* __restrict__ offsets, uint64_t n) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const BatchMap m = maps[owner(offsets, n_maps, i)];
+    const uint32_t x = coord_to_voxel(__ldg(xyz + 3 * i), m.side), y = coord_to_voxel(__ldg(xyz + 3 * i + 1), m.side),
+                   z = coord_to_voxel(__ldg(xyz + 3 * i + 2), m.side);
+    if (x < (uint32_t)m.X && y < (uint32_t)m.Y && z < (uint32_t)m.Z)
+      m.vox[((uint64_t)z * m.Y + y) * m.X + x] = dv_pack(x, y, z);
+  }
+}
+
+// Trilinear distance (+ gradient) for queries of many maps: query i reads map map_of[i].
+__global__ void batch_trilinear_kernel(const BatchMap* __restrict__ maps, const float* __restrict__ xyz,
+                                       const uint32_t* __restrict__ map_of, uint64_t n, float* __restrict__ dist,
+                                       float* __restrict__ grad) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const BatchMap bm = maps[__ldg(map_of + i)];
+    const MapView m{bm.vox, bm.X, bm.Y, bm.Z, bm.side};
+    const Tri t = trilinear(m, __ldg(xyz + 3 * i), __ldg(xyz + 3 * i + 1), __ldg(xyz + 3 * i + 2));
+    dist[i] = t.d * m.side;
+    if (grad != nullptr) {
+      grad[3 * i] = t.gx;
+      grad[3 * i + 1] = t.gy;
+      grad[3 * i + 2] = t.gz;
+    }
+  }
+}
+
+int g_sms = 0;
+int sms() {
+  if (g_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms;
+}
+
+gvx_status fail(gvx_status st, const char* msg) {
+  set_error(msg);
+  return st;
+}
+
+}  // namespace
+}  // namespace gvx
+
+struct gvx_batch {
+  std::vector<gvx_dvm*> maps;
+  gvx::BatchMap* d_table = nullptr;
+  gvx::BatchItems items{};
+  long long* d_prefix = nullptr;  // 3 x (n_maps + 1)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+using namespace gvx;
+
+extern "C" {
+
+gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** out) {
+  if (out == nullptr || maps == nullptr || n_maps == 0) return fail(GVX_ERR_INVALID_ARG, "need at least one map");
+  *out = nullptr;
+  std::vector<BatchMap> table(n_maps);
+  for (uint32_t k = 0; k < n_maps; ++k) {
+    if (maps[k] == nullptr) return fail(GVX_ERR_INVALID_ARG, "null map in batch");
+    const gvx_dvm* m = maps[k];
+    table[k] = BatchMap{m->d_vox, m->d_scratch, (int)m->dims.x, (int)m->dims.y, (int)m->dims.z, m->side, num_voxels(m->dims)};
+  }
+  gvx_batch* b = new (std::nothrow) gvx_batch();
+  if (b == nullptr) return fail(GVX_ERR_OOM, "host allocation failed");
+  b->maps.assign(maps, maps + n_maps);
+  std::vector<long long> prefix(3 * (size_t)(n_maps + 1), 0);
+  for (int p = 0; p < 3; ++p) {
+    for (uint32_t k = 0; k < n_maps; ++k)
+      prefix[p * (n_maps + 1) + k + 1] = prefix[p * (n_maps + 1) + k] + edt_pass_items(maps[k]->dims, p);
+    b->items.total[p] = prefix[p * (n_maps + 1) + n_maps];
+  }
+  b->items.n_maps = n_maps;
+  cudaError_t e = cudaMalloc(&b->d_table, n_maps * sizeof(BatchMap));
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_table, table.data(), n_maps * sizeof(BatchMap), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_prefix, prefix.size() * sizeof(long long));
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_prefix, prefix.data(), prefix.size() * sizeof(long long), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    if (b->d_table) cudaFree(b->d_table);
+    if (b->d_prefix) cudaFree(b->d_prefix);
+    delete b;
+    return cuda_status(e, "batch table");
+  }
+  for (int p = 0; p < 3; ++p) b->items.d_prefix[p] = b->d_prefix + p * (size_t)(n_maps + 1);
+  *out = b;
+  return GVX_OK;
+}
+
+gvx_status gvx_batch_destroy(gvx_batch* b) {
+  if (b == nullptr) return GVX_OK;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->d_table) cudaFree(b->d_table);
+  if (b->d_prefix) cudaFree(b->d_prefix);
+  delete b;
+  return GVX_OK;
+}
+
+gvx_status gvx_batch_clear(gvx_batch* b, gvx_stream stream) {
+  if (b == nullptr) return fail(GVX_ERR_INVALID_ARG, "batch is null");
+  dim3 grid((unsigned)std::max(1, sms() * 4 / (int)std::min<size_t>(b->maps.size(), 64)), (unsigned)b->maps.size());
+  batch_clear_kernel<<<grid, 256, 0, as_stream(stream)>>>(b->d_table);
+  return cuda_status(cudaGetLastError(), "batch clear");
+}
+
+gvx_status gvx_batch_insert_points(gvx_batch* b, const float* d_xyz, const uint64_t* d_offsets, uint64_t n_total,
+                                   gvx_stream stream) {
+  if (b == nullptr || d_offsets == nullptr || (n_total > 0 && d_xyz == nullptr)) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (n_total == 0) return GVX_OK;
+  const unsigned blocks = (unsigned)std::min<uint64_t>((n_total + 255) / 256, (uint64_t)sms() * 16);
+  batch_insert_kernel<<<blocks, 256, 0, as_stream(stream)>>>(b->d_table, (uint32_t)b->maps.size(), d_xyz, d_offsets,
+                                                             n_total);
+  return cuda_status(cudaGetLastError(), "batch insert");
+}
+
+gvx_status gvx_batch_edt(gvx_batch* b, gvx_stream stream) {
+  if (b == nullptr) return fail(GVX_ERR_INVALID_ARG, "batch is null");
+  return cuda_status(launch_edt_batch(b->d_table, b->items, as_stream(stream)), "batch EDT");
+}
+
+gvx_status gvx_batch_query_trilinear(gvx_batch* b, const float* d_xyz, const uint32_t* d_map, uint64_t n, float* d_dist,
+                                     float* d_grad, gvx_stream stream) {
+  if (b == nullptr || (n > 0 && (d_xyz == nullptr || d_map == nullptr || d_dist == nullptr)))
+    return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (n == 0) return GVX_OK;
+  const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms() * 16);
+  batch_trilinear_kernel<<<blocks, 256, 0, as_stream(stream)>>>(b->d_table, d_xyz, d_map, n, d_dist, d_grad);
+  return cuda_status(cudaGetLastError(), "batch trilinear");
+}
+
+gvx_status gvx_batch_graph_capture(gvx_batch* b, const float* d_xyz, const uint64_t* d_offsets, uint64_t n_total,
+                                   const float* d_qxyz, const uint32_t* d_qmap, uint64_t n_q, float* d_dist, float* d_grad,
+                                   gvx_stream stream) {
+  if (b == nullptr) return fail(GVX_ERR_INVALID_ARG, "batch is null");
+  cudaStream_t s = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_status(e, "capture stream");
+  // one plain run first: it sets every kernel attribute outside the capture
+  gvx_status st = gvx_batch_clear(b, s);
+  if (st == GVX_OK) st = gvx_batch_insert_points(b, d_xyz, d_offsets, n_total, s);
+  if (st == GVX_OK) st = gvx_batch_edt(b, s);
+  if (st == GVX_OK) st = gvx_batch_query_trilinear(b, d_qxyz, d_qmap, n_q, d_dist, d_grad, s);
+  if (st == GVX_OK) st = cuda_status(cudaStreamSynchronize(s), "batch warm-up");
+  if (st != GVX_OK) {
+    cudaStreamDestroy(s);
+    return st;
+  }
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    st = gvx_batch_clear(b, s);
+    if (st == GVX_OK) st = gvx_batch_insert_points(b, d_xyz, d_offsets, n_total, s);
+    if (st == GVX_OK) st = gvx_batch_edt(b, s);
+    if (st == GVX_OK) st = gvx_batch_query_trilinear(b, d_qxyz, d_qmap, n_q, d_dist, d_grad, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (st == GVX_OK && e2 == cudaSuccess) {
+      b->graph = g;
+      e2 = cudaGraphInstantiate(&b->exec, g, 0);
+      if (e2 != cudaSuccess) st = cuda_status(e2, "graph instantiate");
+    } else if (st == GVX_OK) {
+      st = cuda_status(e2, "end capture");
+    }
+  } else {
+    st = cuda_status(e, "begin capture");
+  }
+  cudaStreamDestroy(s);
+  (void)stream;
+  return st;
+}
+
+gvx_status gvx_batch_graph_launch(gvx_batch* b, gvx_stream stream) {
+  if (b == nullptr || b->exec == nullptr) return fail(GVX_ERR_INVALID_ARG, "no captured graph");
+  return cuda_status(cudaGraphLaunch(b->exec, as_stream(stream)), "graph launch");
+}
+
+}  // extern "C"

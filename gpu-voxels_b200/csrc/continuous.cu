@@ -19,82 +19,12 @@
 #include <algorithm>
 
 #include "gvx_internal.cuh"
+#include "trilinear.cuh"
 
 namespace gvx {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-
-struct MapView {
-  const uint32_t* vox;
-  int X, Y, Z;
-  float side;
-};
-
-__device__ __forceinline__ float corner_dist(const MapView& m, int i, int j, int k) {
-  const uint32_t v = __ldg(m.vox + ((uint64_t)k * m.Y + j) * m.X + i);
-  const int ox = (int)dv_x(v), oy = (int)dv_y(v), oz = (int)dv_z(v);
-  if (ox == (int)kUninit || oy == (int)kUninit || oz == (int)kUninit) return sqrtf((float)kMaxObstacleDistance);
-  const int dx = i - ox, dy = j - oy, dz = k - oz;
-  return sqrtf((float)(dx * dx + dy * dy + dz * dz));
-}
-
-// Lattice coordinate along one axis: u = p/side - 0.5 clamped to [0, n-1];
-// returns the lower corner, the fraction and whether the axis is free.  The
-// fraction is taken from the residual p - (i0 + 0.5) * side (one fused
-// rounding) rather than from u, which keeps it accurate far from the origin.
-__device__ __forceinline__ void axis_setup(float p, float side, int n, int& i0, int& i1, float& f, bool& free_axis) {
-  const float u = __fsub_rn(__fdiv_rn(p, side), 0.5f);
-  const float hi = (float)(n - 1);
-  free_axis = (u >= 0.0f) && (u <= hi);
-  const float uc = fminf(fmaxf(u, 0.0f), hi);  // NaN -> 0
-  i0 = (int)floorf(uc);
-  if (free_axis) {
-    // choose the cell by the sign of the exact residual, not the rounded u
-    if (i0 > 0 && fmaf(-((float)i0 + 0.5f), side, p) < 0.0f) --i0;
-    else if (i0 < n - 1 && fmaf(-((float)i0 + 1.5f), side, p) >= 0.0f) ++i0;
-  }
-  i0 = min(i0, max(n - 2, 0));
-  i1 = min(i0 + 1, n - 1);
-  if (free_axis) {
-    f = __fdiv_rn(fmaf(-((float)i0 + 0.5f), side, p), side);
-    f = fminf(fmaxf(f, 0.0f), 1.0f);
-  } else {
-    f = uc - (float)i0;
-  }
-}
-
-struct Tri {
-  float d;           // voxel units
-  float gx, gy, gz;  // d(distance)/d(position), dimensionless
-};
-
-__device__ __forceinline__ Tri trilinear(const MapView& m, float px, float py, float pz) {
-  int i0, i1, j0, j1, k0, k1;
-  float fx, fy, fz;
-  bool ax, ay, az;
-  axis_setup(px, m.side, m.X, i0, i1, fx, ax);
-  axis_setup(py, m.side, m.Y, j0, j1, fy, ay);
-  axis_setup(pz, m.side, m.Z, k0, k1, fz, az);
-  const float d000 = corner_dist(m, i0, j0, k0), d100 = corner_dist(m, i1, j0, k0);
-  const float d010 = corner_dist(m, i0, j1, k0), d110 = corner_dist(m, i1, j1, k0);
-  const float d001 = corner_dist(m, i0, j0, k1), d101 = corner_dist(m, i1, j0, k1);
-  const float d011 = corner_dist(m, i0, j1, k1), d111 = corner_dist(m, i1, j1, k1);
-  // interpolate along x, then y, then z
-  const float e00 = fmaf(fx, d100 - d000, d000), e10 = fmaf(fx, d110 - d010, d010);
-  const float e01 = fmaf(fx, d101 - d001, d001), e11 = fmaf(fx, d111 - d011, d011);
-  const float g0 = fmaf(fy, e10 - e00, e00), g1 = fmaf(fy, e11 - e01, e01);
-  Tri t;
-  t.d = fmaf(fz, g1 - g0, g0);
-  // partial derivatives of the interpolant in lattice units
-  const float sx0 = fmaf(fy, (d110 - d010) - (d100 - d000), d100 - d000);
-  const float sx1 = fmaf(fy, (d111 - d011) - (d101 - d001), d101 - d001);
-  t.gx = ax ? fmaf(fz, sx1 - sx0, sx0) : 0.0f;
-  const float sy0 = e10 - e00, sy1 = e11 - e01;
-  t.gy = ay ? fmaf(fz, sy1 - sy0, sy0) : 0.0f;
-  t.gz = az ? (g1 - g0) : 0.0f;
-  return t;
-}
 
 __global__ void trilinear_kernel(MapView m, const float* __restrict__ xyz, uint64_t n, float* __restrict__ dist,
                                  float* __restrict__ grad) {

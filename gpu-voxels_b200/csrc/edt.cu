@@ -15,28 +15,25 @@
 //            again; sweeping x directly in the original frame is the same
 //            computation with the roles of the site's x and y fields swapped.
 //
-// Passes Y and X: one thread per column, a warp owns 32 adjacent columns.
-// The columns stream through shared memory in 32-row chunks (cp.async,
-// double buffered; pass X transposes each 32x32 chunk on the way in), the
-// proximate-site stack of phases 2/3 is the reference's positional stack,
-// kept in a per-map scratch buffer laid out [slice][block][row][lane] so the
-// lanes of a warp push and pop the same row with one 128-byte access, and
-// phase 3 writes each row of the warp's 32 columns with one coalesced store
-// (pass X through a 32x33 staging tile).  The sweep is a chain of dependent
-// steps per column, so the design goal is many columns in flight per SM.
+// Passes Y and X: one thread per column, a warp owns 32 adjacent columns and
+// streams them through shared memory in chunks of rows (cp.async, double
+// buffered; pass X transposes each chunk on the way in and out).  Within a
+// chunk the rows advance in lockstep and only the stack pops a row triggers
+// run divergently.  The proximate-site stack is compact (depth-indexed, each
+// entry carries its row): its top lives in an on-chip ring per lane together
+// with each entry's bisector, every push is written through to the map's
+// workspace, and phase 3 streams the stack back top-down in prefetched
+// blocks.  Stack order, tests and tie rules are the reference's.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "gvx_internal.cuh"
 
 namespace gvx {
 namespace {
-
-constexpr int kChunk = 32;        // rows staged per step
-constexpr int kSweepWarps = 8;    // warps per CTA in passes Y and X
-constexpr int kTileWords = 32 * 33;
 
 __device__ __forceinline__ void cp_async4(uint32_t* smem_dst, const uint32_t* gmem_src) {
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
@@ -50,72 +47,115 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// devicePBAintersection3DY (VoxelMapOperationsPBA.hpp:265-276) in a column
-// frame: sites (a, row, c), column at (a0, c0).  Halving is exact, so the
-// reference's "/ 2.0f" is a multiply by 0.5; the products and sums are exact
-// for coordinates below 1024, so only the IEEE divide and the final add
-// round.  The _rn intrinsics forbid any contraction.
-__device__ __forceinline__ float pba_isect(int a1, int r1, int c1, int a2, int r2, int c2, int a0, int c0) {
-  const float aM = __fmul_rn((float)(a1 + a2), 0.5f);
-  const float rM = __fmul_rn((float)(r1 + r2), 0.5f);
-  const float cM = __fmul_rn((float)(c1 + c2), 0.5f);
-  const float na = (float)(a2 - a1);
-  const float nr = (float)(r2 - r1);
-  const float nc = (float)(c2 - c1);
-  const float num = __fadd_rn(__fmul_rn(na, __fsub_rn(aM, (float)a0)), __fmul_rn(nc, __fsub_rn(cM, (float)c0)));
-  return __fadd_rn(rM, __fdiv_rn(num, nr));
-}
-
-// Stack entry: a | backptr<<10 | c<<20, the reference's packing.
-struct Site {
-  uint32_t a, b, c;
-};
-__device__ __forceinline__ Site unpack(uint32_t e) { return Site{e & 0x3ffu, (e >> 10) & 0x3ffu, e >> 20}; }
-
 // ---------------------------------------------------------------------------
-// pass Z: phase 1 per (x, y) column, m1 = 1; the whole column in shared memory.
+// pass Z: phase 1 per (x, y) column, m1 = 1.
+// The forward flood only changes value at rows whose input holds a site, so
+// the forward scan records those (value, row) pairs -- the column's site list
+// -- in an on-chip ring, and the backward flood walks the list downward.  A
+// column with more sites than the ring holds finds the older ones again by
+// scanning its (still unmodified) input below the current row.  Reads and
+// writes stream once; each row is a fixed, lockstep step.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) edt_pass_z(uint32_t* __restrict__ map, int X, int Y, int Z, int warps_per_cta) {
-  extern __shared__ __align__(16) uint32_t smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+constexpr int kZChunk = 16;
+constexpr int kZRing = 16;
+constexpr int kZWarps = 8;
+constexpr int kZWarpWords = 2 * kZChunk * 32 + 2 * kZRing * 32;
+
+// One warp item of pass Z: 32 adjacent (x, y) columns; wbase = the warp's
+// kZWarpWords of shared memory.
+__device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, int Y, int Z, long long item,
+                                            uint32_t* wbase) {
+  const int lane = threadIdx.x & 31;
   const int nxb = (X + 31) >> 5;
-  const long long item = (long long)blockIdx.x * warps_per_cta + warp;
-  if (item >= (long long)nxb * Y) return;
   const int xb = (int)(item % nxb), y = (int)(item / nxb);
   const int x0 = xb * 32, valid_cols = min(32, X - x0);
   const uint64_t layer = (uint64_t)X * Y;
-  uint32_t* tile = smem + (size_t)warp * Z * 32;
+  uint32_t* const tile0 = wbase;
+  uint32_t* const tile1 = wbase + kZChunk * 32;
+  uint32_t* ringV = wbase + 2 * kZChunk * 32 + lane;  // slot k: ringV[k * 32]
+  uint32_t* ringR = ringV + kZRing * 32;
   const uint32_t* src = map + (uint64_t)y * X + x0;
-  if (valid_cols == 32 && (X & 3) == 0) {
-    const int part = lane & 7;
-    for (int r = lane >> 3; r < Z; r += 4) cp_async16(tile + r * 32 + part * 4, src + (uint64_t)r * layer + part * 4);
-  } else if (lane < valid_cols) {
-    for (int r = 0; r < Z; ++r) cp_async4(tile + r * 32 + lane, src + (uint64_t)r * layer + lane);
-  } else {
-    for (int r = 0; r < Z; ++r) tile[r * 32 + lane] = kDvUninit;
+  const bool vec16 = valid_cols == 32 && (X & 3) == 0;
+  const int nchunks = (Z + kZChunk - 1) / kZChunk;
+  auto stage = [&](uint32_t* tile, int c) {
+    const int r0 = c * kZChunk, rows = min(kZChunk, Z - r0);
+    const uint32_t* s0 = src + (uint64_t)r0 * layer;
+    if (vec16) {
+      const int part = lane & 7;
+      for (int r = lane >> 3; r < rows; r += 4) cp_async16(tile + r * 32 + part * 4, s0 + (uint64_t)r * layer + part * 4);
+    } else if (lane < valid_cols) {
+      for (int r = 0; r < rows; ++r) cp_async4(tile + r * 32 + lane, s0 + (uint64_t)r * layer + lane);
+    } else {
+      for (int r = 0; r < rows; ++r) tile[r * 32 + lane] = kDvUninit;
+    }
+  };
+
+  // forward: record the sites of the column
+  stage(tile0, 0);
+  cp_async_commit();
+  if (nchunks > 1) stage(tile1, 1);
+  cp_async_commit();
+  int m = 0;  // sites seen
+  for (int c = 0; c < nchunks; ++c) {
+    cp_async_wait1();
+    __syncwarp();
+    const uint32_t* tile = (c & 1) ? tile1 : tile0;
+    const int r0 = c * kZChunk, rows = min(kZChunk, Z - r0);
+    for (int r = 0; r < rows; ++r) {
+      const uint32_t v = tile[r * 32 + lane];
+      if ((v >> 20) != kUninit) {
+        ringV[(m % kZRing) * 32] = v;
+        ringR[(m % kZRing) * 32] = (uint32_t)(r0 + r);
+        ++m;
+      }
+    }
+    __syncwarp();
+    if (c + 2 < nchunks) stage((c & 1) ? tile1 : tile0, c + 2);
+    cp_async_commit();
   }
   cp_async_wait_all();
-  __syncwarp();
 
-  // flood forward (in shared memory)
-  uint32_t obstacle = kDvUninit;
-#pragma unroll 8
-  for (int z = 0; z < Z; ++z) {
-    const uint32_t cur = tile[z * 32 + lane];
-    if ((cur >> 20) != kUninit) obstacle = cur;
-    tile[z * 32 + lane] = obstacle;
+  // backward: obstacle(z) from the forward value fwd(z) = last site at or below z;
+  // ties keep the lower z (<=, VoxelMapOperationsPBA.hpp:112-122)
+  const uint32_t* col = src + lane;  // this lane's column (input rows <= z are still unmodified)
+  int j = m - 1;                     // index of the site fwd(z)
+  uint32_t fwdV = kDvUninit;
+  int fwdRow = -1;
+  if (j >= 0) {
+    fwdV = ringV[(j % kZRing) * 32];
+    fwdRow = (int)ringR[(j % kZRing) * 32];
   }
-  // flood backward; ties keep the lower z (<=, VoxelMapOperationsPBA.hpp:118)
-  obstacle = kDvUninit;
+  uint32_t obstacle = kDvUninit;
   uint32_t* dst = map + (uint64_t)y * X + x0 + lane;
-  const bool store = lane < valid_cols;
-#pragma unroll 8
+  const bool live = lane < valid_cols;
   for (int z = Z - 1; z >= 0; --z) {
+    while (fwdRow > z) {  // step to the previous site
+      --j;
+      if (j < 0) {
+        fwdV = kDvUninit;
+        fwdRow = -1;
+      } else if (j >= m - kZRing) {
+        fwdV = ringV[(j % kZRing) * 32];
+        fwdRow = (int)ringR[(j % kZRing) * 32];
+      } else if (live) {  // older than the ring: scan the input downward
+        int rr = z;
+        uint32_t v = kDvUninit;
+        for (; rr >= 0; --rr) {
+          v = col[(uint64_t)rr * layer];
+          if ((v >> 20) != kUninit) break;
+        }
+        fwdRow = rr;
+        fwdV = rr >= 0 ? v : kDvUninit;
+        if (rr < 0) j = -1;
+      } else {
+        fwdV = kDvUninit;
+        fwdRow = -1;
+      }
+    }
     const int dist_prev = abs((int)(obstacle >> 20) - z);
-    const uint32_t next = tile[z * 32 + lane];
-    const int dist_next = abs(z - (int)(next >> 20));
-    if (dist_next <= dist_prev) obstacle = next;
-    if (store) dst[(uint64_t)z * layer] = obstacle;
+    const int dist_next = abs(z - (int)(fwdV >> 20));
+    if (dist_next <= dist_prev) obstacle = fwdV;
+    if (live) dst[(uint64_t)z * layer] = obstacle;
   }
 }
 
@@ -123,24 +163,69 @@ __global__ void __launch_bounds__(256) edt_pass_z(uint32_t* __restrict__ map, in
 // passes Y and X
 // ---------------------------------------------------------------------------
 
+// Exact small-integer -> float conversions on the FMA/ALU pipes (the
+// converter sits on the narrow XU pipe, which the reciprocal also needs):
+// for 0 <= v < 2^22 the bit pattern 0x4B400000 + v is the float 2^23 + 2^22 + v.
+__device__ __forceinline__ float small_to_float(int v) { return __int_as_float(0x4B400000 + v) - 12582912.0f; }
+
+// A site in the column frame: packed entry (a | row << 10 | c << 20) plus its
+// row and squared offset from the column as exact floats (offset < 2^21).
+struct Col {
+  uint32_t e;
+  float r, d;
+};
+
+__device__ __forceinline__ Col make_col(uint32_t e, float a0f, float c0f) {
+  Col s;
+  s.e = e;
+  s.r = small_to_float((int)((e >> 10) & 0x3ffu));
+  const float da = small_to_float((int)(e & 0x3ffu)) - a0f;
+  const float dc = small_to_float((int)(e >> 20)) - c0f;
+  s.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));  // exact: integers below 2^21
+  return s;
+}
+
+// devicePBAintersection3DY (VoxelMapOperationsPBA.hpp:265-276) is
+//   yM + (nx*(xM-x0) + nz*(zM-z0)) / ny.
+// For integer coordinates below 1024 its numerator is exact in float and
+// equals (d2 - d1) / 2, d = squared offset of a site from the column, so the
+// value is fl(0.5*(r1 + r2) + fl((d2 - d1) / (2*(r2 - r1)))) with every operand
+// exact: bit for bit the reference's float.  Equal offsets give exactly the
+// midpoint; the divide is skipped when no lane of the warp needs it.
+__device__ __forceinline__ float bisect(const Col& s1, const Col& s2) {
+  const float num = __fsub_rn(s2.d, s1.d);
+  float q = 0.0f;
+  if (__any_sync(__activemask(), num != 0.0f)) q = __fdiv_rn(num, __fmul_rn(__fsub_rn(s2.r, s1.r), 2.0f));
+  return __fadd_rn(__fmul_rn(__fadd_rn(s1.r, s2.r), 0.5f), q);
+}
+
 // Geometry of one warp's work item.
 struct Sweep {
   int L;             // column length (rows)
   int a0_base;       // column coordinate of lane 0 (x0 for pass Y, y0 for pass X)
-  int c0;            // slice (z)
   int valid;         // valid lanes
   uint32_t* slice;   // map + z * layer
   int X;             // map row length
 };
 
-// Issue the cp.async copies of chunk `c` into `tile`.
-template <bool kXPass>
+template <int kRows>
+struct SweepCfg {
+  static constexpr int kWarps = 8;                       // warps per CTA
+  static constexpr int kTileWords = kRows * 33;          // one staging tile
+  static constexpr int kRing = 16;                       // ring slots per lane
+  static constexpr int kWarpWords = 2 * kTileWords + 2 * kRing * 32;
+  static_assert(2 * kRing >= 32, "the phase-3 window (32 entries per lane) aliases the ring");
+};
+
+// Issue the cp.async copies of chunk `c` (rows c*kRows ..) into `tile`.
+// Pass Y: tile[r*32 + lane] = row r of column lane.  Pass X: the chunk holds
+// x positions, transposed: tile[(x - r0)*33 + t] = element x of row t.
+template <bool kXPass, int kRows>
 __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int c, bool vec16) {
   const int lane = threadIdx.x & 31;
-  const int r0 = c * kChunk;
-  const int rows = min(kChunk, s.L - r0);
+  const int r0 = c * kRows;
+  const int rows = min(kRows, s.L - r0);
   if (!kXPass) {
-    // rows r0.. of columns a0_base..a0_base+31: tile[r*32 + lane]
     const uint32_t* src = s.slice + (uint64_t)r0 * s.X + s.a0_base;
     if (vec16) {
       const int part = lane & 7;
@@ -151,135 +236,237 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
       for (int r = 0; r < rows; ++r) tile[r * 32 + lane] = kDvUninit;
     }
   } else {
-    // x positions r0+lane of rows a0_base+t, transposed: tile[(x - r0) * 33 + t]
-    const uint32_t* src = s.slice + (uint64_t)s.a0_base * s.X + r0 + lane;
-    const bool in_row = lane < rows;
-    for (int t = 0; t < 32; ++t) {
-      if (!in_row) continue;
-      if (t < s.valid) cp_async4(tile + lane * 33 + t, src + (uint64_t)t * s.X);
-      else tile[lane * 33 + t] = kDvUninit;
+    const int xl = lane % kRows;  // x within the chunk
+    const int t0 = lane / kRows;
+    if (xl < rows) {
+      const uint32_t* src = s.slice + (uint64_t)s.a0_base * s.X + r0 + xl;
+      for (int t = t0; t < 32; t += 32 / kRows) {
+        if (t < s.valid) cp_async4(tile + xl * 33 + t, src + (uint64_t)t * s.X);
+        else tile[xl * 33 + t] = kDvUninit;
+      }
     }
   }
 }
 
-template <bool kXPass>
-__device__ __forceinline__ uint32_t tile_at(const uint32_t* tile, int r) {
+// One warp item of pass Y (kXPass false) or X: 32 adjacent columns of one
+// z slice; wbase = the warp's kWarpWords of shared memory; the item's stack
+// area in the workspace starts at scratch + item * L * 32.
+template <bool kXPass, int kRows>
+__device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t* __restrict__ scratch, int X, int Y,
+                                           int Z, long long item, uint32_t* wbase) {
+  using Cfg = SweepCfg<kRows>;
   const int lane = threadIdx.x & 31;
-  return kXPass ? tile[r * 33 + lane] : tile[r * 32 + lane];
-}
-
-template <bool kXPass>
-__global__ void __launch_bounds__(kSweepWarps * 32, 3) edt_sweep(uint32_t* __restrict__ map, uint32_t* __restrict__ scratch,
-                                                                 int X, int Y, int Z) {
-  extern __shared__ __align__(16) uint32_t s_tiles[];  // [kSweepWarps][2][kTileWords]
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int cols = kXPass ? Y : X;  // columns per slice
   const int L = kXPass ? X : Y;
   const int nblk = (cols + 31) >> 5;
-  const long long item = (long long)blockIdx.x * kSweepWarps + warp;
-  if (item >= (long long)nblk * Z) return;
   const int blk = (int)(item % nblk), z = (int)(item / nblk);
   Sweep s;
   s.L = L;
   s.a0_base = blk * 32;
-  s.c0 = z;
   s.valid = min(32, cols - s.a0_base);
   s.slice = map + (uint64_t)z * X * Y;
   s.X = X;
   const bool vec16 = !kXPass && s.valid == 32 && (X & 3) == 0;
-  uint32_t* tiles[2] = {s_tiles + (2 * warp) * kTileWords, s_tiles + (2 * warp + 1) * kTileWords};
-  uint32_t* stk = scratch + ((uint64_t)item * L) * 32 + lane;  // entry of row p: stk[p * 32]
-  const int a0 = s.a0_base + lane;
-  const int c0 = z;
-  const int nchunks = (L + kChunk - 1) / kChunk;
+  uint32_t* tile0 = wbase;
+  uint32_t* tile1 = wbase + Cfg::kTileWords;
+  uint32_t* ringE = wbase + 2 * Cfg::kTileWords + lane;  // slot k: ringE[k * 32]
+  float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
+  uint32_t* gstk = scratch + ((uint64_t)item * L) * 32 + lane;  // depth d: gstk[d * 32]
+  const float a0f = small_to_float(s.a0_base + lane);  // this lane's column coordinate
+  const float c0f = small_to_float(z);
+  const int nchunks = (L + kRows - 1) / kRows;
+  const int tpitch = kXPass ? 33 : 32;
 
-  // ---- phase 2: proximate sites, positional stack with back-pointers ----
-  stage_chunk<kXPass>(tiles[0], s, 0, vec16);
+  // ---- phase 2: proximate sites ------------------------------------------
+  // Rows advance in lockstep (the per-row work runs on all 32 lanes); the pops
+  // a row triggers run as a loop over just the lanes that need them.  The ring
+  // keeps each entry's bisector with the entry below, so a pop reads the new
+  // (second, bisector) pair instead of recomputing it.
+  stage_chunk<kXPass, kRows>(tile0, s, 0, vec16);
   cp_async_commit();
-  if (nchunks > 1) stage_chunk<kXPass>(tiles[1], s, 1, vec16);
+  if (nchunks > 1) stage_chunk<kXPass, kRows>(tile1, s, 1, vec16);
   cp_async_commit();
 
-  int last_y = (int)kUninit;  // row of the stack top, UNINIT when empty
-  Site top{kUninit, kUninit, kUninit}, second{kUninit, kUninit, kUninit};
-  float i_top = 0.0f;  // intersection of (second, top); valid when top.b != UNINIT
-  uint32_t cur_a = kUninit;
+  int n = 0;   // stack depth
+  int lo = 0;  // lowest depth guaranteed to be in the ring
+  Col top{0u, 0.f, 0.f}, sec{0u, 0.f, 0.f};
+  float top_i = 0.f, sec_i = 0.f;  // bisector(second, top), bisector(third, second)
   for (int c = 0; c < nchunks; ++c) {
     cp_async_wait1();
     __syncwarp();
-    const uint32_t* tile = tiles[c & 1];
-    const int r0 = c * kChunk;
-    const int rows = min(kChunk, L - r0);
+    const uint32_t* tile = (c & 1) ? tile1 : tile0;
+    const int r0 = c * kRows;
+    const int rows = min(kRows, L - r0);
     for (int r = 0; r < rows; ++r) {
-      const int ty = r0 + r;
-      const uint32_t v = tile_at<kXPass>(tile, r);
-      cur_a = kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
-      if (cur_a != kUninit) {
-        const uint32_t cur_c = v >> 20;
-        float i2 = 0.0f;
-        bool have_i2 = false;
-        while (top.b != kUninit) {
-          i2 = pba_isect((int)top.a, last_y, (int)top.c, (int)cur_a, ty, (int)cur_c, a0, c0);
-          have_i2 = true;
-          if (i_top < i2) break;
-          last_y = (int)top.b;  // pop
-          top = second;
-          have_i2 = false;
-          if (top.b != kUninit) {
-            second = unpack(stk[(int)top.b * 32]);
-            i_top = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
+      const uint32_t v = tile[r * tpitch + lane];
+      const uint32_t a = kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
+      if (a == kUninit) continue;
+      const Col cur = make_col(a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u), a0f, c0f);
+      float i2 = 0.f;
+      if (n >= 1) i2 = bisect(top, cur);
+      while (n >= 2 && !(top_i < i2)) {  // top is dominated by (second, current): pop
+        --n;
+        top = sec;
+        top_i = sec_i;
+        if (n >= 2) {
+          const int d = n - 2;
+          if (d >= lo) {
+            sec = make_col(ringE[(d % Cfg::kRing) * 32], a0f, c0f);
+            sec_i = ringI[(d % Cfg::kRing) * 32];
+          } else {  // below the ring: the workspace has the entries
+            sec = make_col(gstk[d * 32], a0f, c0f);
+            sec_i = d >= 1 ? bisect(make_col(gstk[(d - 1) * 32], a0f, c0f), sec) : 0.f;
           }
         }
-        if (last_y != (int)kUninit)
-          i_top = have_i2 ? i2 : pba_isect((int)top.a, last_y, (int)top.c, (int)cur_a, ty, (int)cur_c, a0, c0);
-        second = top;
-        top = Site{cur_a, (uint32_t)last_y, cur_c};
-        last_y = ty;
-        stk[ty * 32] = dv_pack(top.a, top.b, top.c);
+        i2 = bisect(top, cur);
       }
+      const int slot = (n % Cfg::kRing) * 32;  // push the current site
+      ringE[slot] = cur.e;
+      ringI[slot] = i2;
+      gstk[n * 32] = cur.e;
+      lo = max(lo, n - Cfg::kRing + 1);
+      ++n;
+      sec = top;
+      sec_i = top_i;
+      top = cur;
+      top_i = i2;
     }
     __syncwarp();
-    if (c + 2 < nchunks) stage_chunk<kXPass>(tiles[c & 1], s, c + 2, vec16);
+    if (c + 2 < nchunks) stage_chunk<kXPass, kRows>((c & 1) ? tile1 : tile0, s, c + 2, vec16);
     cp_async_commit();
   }
   cp_async_wait_all();
-  if (cur_a == kUninit) stk[(L - 1) * 32] = dv_pack(kUninit, (uint32_t)last_y, kUninit);  // tail pointer
+  __syncwarp();
 
-  // ---- phase 3: walk rows downward, popping sites that fall behind ----
-  float inter = 0.0f;
-  last_y = L - 1;
-  top = unpack(stk[last_y * 32]);
-  if (top.a == kUninit) {
-    last_y = (int)top.b;
-    if (last_y != (int)kUninit) top = unpack(stk[last_y * 32]);
-  }
-  if (top.b != kUninit) {
-    second = unpack(stk[(int)top.b * 32]);
-    inter = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
-  }
-  uint32_t* stage = tiles[0];
-  for (int ty = L - 1; ty >= 0; --ty) {
-    while (top.b != kUninit) {
-      if ((float)ty > inter) break;
-      last_y = (int)top.b;
-      top = second;
-      if (top.b != kUninit) {
-        second = unpack(stk[(int)top.b * 32]);
-        inter = pba_isect((int)second.a, (int)top.b, (int)second.c, (int)top.a, last_y, (int)top.c, a0, c0);
-      }
+  // ---- phase 3: rows downward, popping sites that fall behind ----
+  // The stack streams back from the workspace through a 32-entry window per
+  // lane (slot = depth mod 32, in the ring's memory).  At each chunk start
+  // every lane requests the entries down to 32 below its top (cp.async), so
+  // the pops of the next chunk find them on chip; a lane that pops past its
+  // window waits for the request or reads the workspace directly.
+  uint32_t* win = ringE;  // depth d: win[(d & 31) * 32]
+  int k = n - 1;          // index of the current top
+  int flo = n;            // lowest depth requested into the window
+  int safe_lo = n;        // depths >= safe_lo have landed
+  auto request = [&](int new_lo) {
+    for (int d = flo - 1; d >= new_lo; --d) cp_async4(win + (d & 31) * 32, gstk + d * 32);
+    cp_async_commit();
+    flo = min(flo, new_lo);
+  };
+  auto entry = [&](int d) -> uint32_t {
+    if (d < safe_lo) {
+      cp_async_wait_all();
+      safe_lo = flo;
+      if (d < flo) return gstk[d * 32];
     }
-    if (!kXPass) {
-      if (lane < s.valid) s.slice[(uint64_t)ty * X + s.a0_base + lane] = dv_pack(top.a, (uint32_t)last_y, top.c);
-    } else {
-      // original frame: x-field = row of the site, y-field = a
-      stage[(ty & 31) * 33 + lane] = dv_pack((uint32_t)last_y, top.a, top.c);
-      if ((ty & 31) == 0) {
-        __syncwarp();
-        if (ty + lane < X) {
-          for (int r = 0; r < s.valid; ++r) s.slice[(uint64_t)(s.a0_base + r) * X + ty + lane] = stage[lane * 33 + r];
+    return win[(d & 31) * 32];
+  };
+  Col prev{0u, 0.f, 0.f};  // entry k-1
+  if (n > 0) {
+    request(max(0, n - 32));
+    cp_async_wait_all();
+    safe_lo = flo;
+    top = make_col(entry(k), a0f, c0f);
+    if (k >= 1) {
+      prev = make_col(entry(k - 1), a0f, c0f);
+      top_i = bisect(prev, top);
+    }
+  }
+  uint32_t* stage = tile0;
+  for (int c = nchunks - 1; c >= 0; --c) {
+    const int r0 = c * kRows;
+    const int rows = min(kRows, L - r0);
+    cp_async_wait_all();  // the previous chunk's request
+    safe_lo = flo;
+    if (k >= 1) request(max(0, k - 32));
+    float tyf = small_to_float(r0 + rows - 1);
+    for (int r = rows - 1; r >= 0; --r, tyf -= 1.0f) {
+      while (k >= 1 && tyf <= top_i) {  // pop
+        --k;
+        top = prev;
+        if (k >= 1) {
+          prev = make_col(entry(k - 1), a0f, c0f);
+          top_i = bisect(prev, top);
         }
-        __syncwarp();
       }
+      uint32_t out = kDvUninit;
+      if (n > 0) {
+        const uint32_t a = top.e & 0x3ffu, row = (top.e >> 10) & 0x3ffu, cc = top.e >> 20;
+        out = kXPass ? dv_pack(row, a, cc) : dv_pack(a, row, cc);
+      }
+      stage[r * tpitch + lane] = out;
     }
+    __syncwarp();
+    if (!kXPass) {
+      if (lane < s.valid)
+        for (int rr = 0; rr < rows; ++rr) s.slice[(uint64_t)(r0 + rr) * X + s.a0_base + lane] = stage[rr * 32 + lane];
+    } else {
+      const int xl = lane % kRows, t0 = lane / kRows;
+      if (xl < rows)
+        for (int t = t0; t < s.valid; t += 32 / kRows) s.slice[(uint64_t)(s.a0_base + t) * X + r0 + xl] = stage[xl * 33 + t];
+    }
+    __syncwarp();
+  }
+  cp_async_wait_all();
+}
+
+// Map owning warp item g of a batch pass: last k with prefix[k] <= g.
+__device__ __forceinline__ uint32_t batch_owner(const long long* __restrict__ prefix, uint32_t n, long long g) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(prefix + mid) <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z(uint32_t* __restrict__ map, int X, int Y, int Z) {
+  extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][kZWarpWords]
+  const int warp = threadIdx.x >> 5;
+  const long long item = (long long)blockIdx.x * kZWarps + warp;
+  if (item >= (long long)((X + 31) >> 5) * Y) return;
+  pass_z_item(map, X, Y, Z, item, s_z + (size_t)warp * kZWarpWords);
+}
+
+// Pass Z over every map of a batch: persistent warps stride over the items of
+// all maps.
+__global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z_batch(const BatchMap* __restrict__ maps,
+                                                                     const long long* __restrict__ prefix,
+                                                                     uint32_t n_maps, long long total) {
+  extern __shared__ __align__(16) uint32_t s_z[];
+  const int warp = threadIdx.x >> 5;
+  for (long long g = (long long)blockIdx.x * kZWarps + warp; g < total; g += (long long)gridDim.x * kZWarps) {
+    const uint32_t k = batch_owner(prefix, n_maps, g);
+    const BatchMap m = maps[k];
+    pass_z_item(m.vox, m.X, m.Y, m.Z, g - __ldg(prefix + k), s_z + (size_t)warp * kZWarpWords);
+    __syncwarp();
+  }
+}
+
+template <bool kXPass, int kRows>
+__global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
+    edt_sweep(uint32_t* __restrict__ map, uint32_t* __restrict__ scratch, int X, int Y, int Z) {
+  using Cfg = SweepCfg<kRows>;
+  extern __shared__ __align__(16) uint32_t s_sweep[];  // [kWarps][kWarpWords]
+  const int warp = threadIdx.x >> 5;
+  const long long item = (long long)blockIdx.x * Cfg::kWarps + warp;
+  if (item >= (long long)(((kXPass ? Y : X) + 31) >> 5) * Z) return;
+  sweep_item<kXPass, kRows>(map, scratch, X, Y, Z, item, s_sweep + (size_t)warp * Cfg::kWarpWords);
+}
+
+template <bool kXPass, int kRows>
+__global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
+    edt_sweep_batch(const BatchMap* __restrict__ maps, const long long* __restrict__ prefix, uint32_t n_maps,
+                    long long total) {
+  using Cfg = SweepCfg<kRows>;
+  extern __shared__ __align__(16) uint32_t s_sweep[];
+  const int warp = threadIdx.x >> 5;
+  for (long long g = (long long)blockIdx.x * Cfg::kWarps + warp; g < total; g += (long long)gridDim.x * Cfg::kWarps) {
+    const uint32_t k = batch_owner(prefix, n_maps, g);
+    const BatchMap m = maps[k];
+    sweep_item<kXPass, kRows>(m.vox, m.scratch, m.X, m.Y, m.Z, g - __ldg(prefix + k),
+                              s_sweep + (size_t)warp * Cfg::kWarpWords);
+    __syncwarp();
   }
 }
 
@@ -296,31 +483,29 @@ int max_smem_optin() {
 }
 
 cudaError_t launch_pass_z(uint32_t* map, gvx_dims d, cudaStream_t s) {
-  const size_t per_warp = (size_t)d.z * 32 * 4;
-  int w = (int)std::max<size_t>(1, std::min<size_t>(8, 98304 / per_warp));
-  const size_t smem = per_warp * w;
-  if ((int)smem > max_smem_optin()) return cudaErrorInvalidConfiguration;
-  cudaError_t e = cudaFuncSetAttribute(edt_pass_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int smem = kZWarps * kZWarpWords * 4;
+  if (smem > max_smem_optin()) return cudaErrorInvalidConfiguration;
+  cudaError_t e = cudaFuncSetAttribute(edt_pass_z, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(edt_pass_z, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   const long long items = (long long)((d.x + 31) / 32) * d.y;
-  edt_pass_z<<<(unsigned)((items + w - 1) / w), 32 * w, smem, s>>>(map, (int)d.x, (int)d.y, (int)d.z, w);
+  edt_pass_z<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(map, (int)d.x, (int)d.y, (int)d.z);
   return cudaGetLastError();
 }
 
-template <bool kXPass>
+template <bool kXPass, int kRows>
 cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStream_t s) {
+  using Cfg = SweepCfg<kRows>;
   const long long cols = kXPass ? d.y : d.x;
   const long long items = ((cols + 31) / 32) * d.z;
-  const int smem = kSweepWarps * 2 * kTileWords * 4;
-  cudaError_t e = cudaFuncSetAttribute(edt_sweep<kXPass>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(edt_sweep<kXPass>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
+  const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
+  auto kern = edt_sweep<kXPass, kRows>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  edt_sweep<kXPass><<<(unsigned)((items + kSweepWarps - 1) / kSweepWarps), kSweepWarps * 32, smem, s>>>(
-      map, scratch, (int)d.x, (int)d.y, (int)d.z);
+  kern<<<(unsigned)((items + Cfg::kWarps - 1) / Cfg::kWarps), Cfg::kWarps * 32, smem, s>>>(map, scratch, (int)d.x,
+                                                                                          (int)d.y, (int)d.z);
   return cudaGetLastError();
 }
 
@@ -332,13 +517,78 @@ uint64_t edt_scratch_words(gvx_dims d) {
   return std::max(y_pass, x_pass);
 }
 
+// Sweep variant: rows per staging chunk (16 or 32).  The environment
+// variable GVX_EDT_SWEEP_ROWS overrides the default for experiments.
+static int g_sweep_rows = -1;
+void set_edt_sweep_rows(int rows) { g_sweep_rows = rows; }
+
 cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s) {
+  if (g_sweep_rows < 0) {
+    const char* env = getenv("GVX_EDT_SWEEP_ROWS");
+    g_sweep_rows = env ? atoi(env) : 16;
+  }
+  const bool big = g_sweep_rows == 32;
   switch (pass) {
     case 0: return launch_pass_z(d_vox, d, s);
-    case 1: return launch_sweep<false>(d_vox, d_scratch, d, s);
-    case 2: return launch_sweep<true>(d_vox, d_scratch, d, s);
+    case 1: return big ? launch_sweep<false, 32>(d_vox, d_scratch, d, s) : launch_sweep<false, 16>(d_vox, d_scratch, d, s);
+    case 2: return big ? launch_sweep<true, 32>(d_vox, d_scratch, d, s) : launch_sweep<true, 16>(d_vox, d_scratch, d, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+long long edt_pass_items(gvx_dims d, int pass) {
+  switch (pass) {
+    case 0: return (long long)((d.x + 31) / 32) * d.y;
+    case 1: return (long long)((d.x + 31) / 32) * d.z;
+    default: return (long long)((d.y + 31) / 32) * d.z;
+  }
+}
+
+namespace {
+
+template <typename K>
+cudaError_t launch_persistent(K kern, int warps, int smem, const BatchMap* table, const long long* prefix, uint32_t n,
+                              long long total, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, dev = 0, sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
+  if (e != cudaSuccess) return e;
+  const long long need = (total + warps - 1) / warps;
+  const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)std::max(per_sm, 1) * std::max(sm, 1)));
+  kern<<<(unsigned)grid, warps * 32, smem, s>>>(table, prefix, n, total);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s) {
+  if (g_sweep_rows < 0) {
+    const char* env = getenv("GVX_EDT_SWEEP_ROWS");
+    g_sweep_rows = env ? atoi(env) : 16;
+  }
+  cudaError_t e = launch_persistent(edt_pass_z_batch, kZWarps, kZWarps * kZWarpWords * 4, d_table, it.d_prefix[0],
+                                    it.n_maps, it.total[0], s);
+  if (e != cudaSuccess) return e;
+  if (g_sweep_rows == 32) {
+    using C = SweepCfg<32>;
+    e = launch_persistent(edt_sweep_batch<false, 32>, C::kWarps, C::kWarps * C::kWarpWords * 4, d_table, it.d_prefix[1],
+                          it.n_maps, it.total[1], s);
+    if (e == cudaSuccess)
+      e = launch_persistent(edt_sweep_batch<true, 32>, C::kWarps, C::kWarps * C::kWarpWords * 4, d_table,
+                            it.d_prefix[2], it.n_maps, it.total[2], s);
+  } else {
+    using C = SweepCfg<16>;
+    e = launch_persistent(edt_sweep_batch<false, 16>, C::kWarps, C::kWarps * C::kWarpWords * 4, d_table, it.d_prefix[1],
+                          it.n_maps, it.total[1], s);
+    if (e == cudaSuccess)
+      e = launch_persistent(edt_sweep_batch<true, 16>, C::kWarps, C::kWarps * C::kWarpWords * 4, d_table,
+                            it.d_prefix[2], it.n_maps, it.total[2], s);
+  }
+  return e;
 }
 
 cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s) {

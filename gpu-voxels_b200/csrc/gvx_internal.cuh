@@ -64,6 +64,23 @@ struct gvx_blist {
 
 namespace gvx {
 
+// One map of a batch, as the batched kernels see it.
+struct BatchMap {
+  uint32_t* vox;
+  uint32_t* scratch;
+  int X, Y, Z;
+  float side;
+  uint64_t nvox;
+};
+
+// Work-item layout of the batched EDT: for pass p, map k owns warp items
+// [prefix[p][k], prefix[p][k+1]).
+struct BatchItems {
+  long long* d_prefix[3];
+  long long total[3];
+  uint32_t n_maps;
+};
+
 // Error reporting shared by the ABI units.
 void set_error(const std::string& msg);
 gvx_status cuda_status(cudaError_t e, const char* what);
@@ -81,6 +98,10 @@ cudaError_t launch_bvm_insert(uint8_t* d_vox, gvx_dims d, float side, const floa
 uint64_t edt_scratch_words(gvx_dims d);
 cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s);
 cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s);
+// Warp work items of one EDT pass for a map of dims d.
+long long edt_pass_items(gvx_dims d, int pass);
+// All maps of a batch, one persistent launch per pass.
+cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& items, cudaStream_t s);
 cudaError_t launch_dvm_sqdist(const uint32_t* d_vox, gvx_dims d, const uint32_t* d_ids, uint64_t n, int32_t* d_out,
                               int mode, cudaStream_t s);
 cudaError_t launch_dvm_sqdist_map(const uint32_t* d_vox, gvx_dims d, int32_t* d_out, cudaStream_t s);

@@ -82,6 +82,14 @@ PROTOTYPES = {
     "gvx_sphere_clearance": [_vp, ctypes.POINTER(Arm), _vp, _u64, _vp, _vp],
     "gvx_traj_cost": [_vp, ctypes.POINTER(Arm), _vp, _u64, _u32, _f, _vp, _vp],
     "gvx_traj_cost_bwd": [_vp, ctypes.POINTER(Arm), _vp, _u64, _u32, _f, _vp, _vp, _vp],
+    "gvx_batch_create": [ctypes.POINTER(_vp), _u32, ctypes.POINTER(_vp)],
+    "gvx_batch_destroy": [_vp],
+    "gvx_batch_clear": [_vp, _vp],
+    "gvx_batch_insert_points": [_vp, _vp, _vp, _u64, _vp],
+    "gvx_batch_edt": [_vp, _vp],
+    "gvx_batch_query_trilinear": [_vp, _vp, _vp, _u64, _vp, _vp, _vp],
+    "gvx_batch_graph_capture": [_vp, _vp, _vp, _u64, _vp, _vp, _u64, _vp, _vp, _vp],
+    "gvx_batch_graph_launch": [_vp, _vp],
     "gvx_bvm_create": [ctypes.POINTER(Dims), _f, ctypes.POINTER(_vp)],
     "gvx_bvm_destroy": [_vp],
     "gvx_bvm_info": [_vp, ctypes.POINTER(Dims), ctypes.POINTER(_f), ctypes.POINTER(_vp)],

@@ -164,6 +164,34 @@ GVX_API gvx_status gvx_traj_cost(const gvx_dvm *m, const gvx_arm *arm, const flo
 GVX_API gvx_status gvx_traj_cost_bwd(const gvx_dvm *m, const gvx_arm *arm, const float *d_q, uint64_t n_traj, uint32_t n_wp,
                              float margin, const float *d_grad_cost, float *d_grad_q, gvx_stream stream);
 
+/* ---- batches of maps (no reference counterpart) ------------------------- */
+
+/* Many DistanceVoxelMaps of uneven dims processed together.  The reference
+ * runs one map per call with device synchronisations in between
+ * (DistanceVoxelMap.hpp:284-645); a batch runs clear, voxelisation, the EDT
+ * passes and trilinear queries as one launch each over all maps, and can
+ * record the whole step as a CUDA graph.  The maps stay owned by the caller
+ * and must outlive the batch. */
+typedef struct gvx_batch gvx_batch;
+GVX_API gvx_status gvx_batch_create(gvx_dvm *const *maps, uint32_t n_maps, gvx_batch **out);
+GVX_API gvx_status gvx_batch_destroy(gvx_batch *b);
+GVX_API gvx_status gvx_batch_clear(gvx_batch *b, gvx_stream stream);
+/* Points of all maps concatenated; map k owns points [d_offsets[k], d_offsets[k+1]). */
+GVX_API gvx_status gvx_batch_insert_points(gvx_batch *b, const float *d_xyz, const uint64_t *d_offsets, uint64_t n_total,
+                                           gvx_stream stream);
+/* EDT of every map, bit-identical to gvx_dvm_edt per map. */
+GVX_API gvx_status gvx_batch_edt(gvx_batch *b, gvx_stream stream);
+/* Query i is answered on map d_map[i]; d_grad optional. */
+GVX_API gvx_status gvx_batch_query_trilinear(gvx_batch *b, const float *d_xyz, const uint32_t *d_map, uint64_t n,
+                                             float *d_dist, float *d_grad, gvx_stream stream);
+/* Record clear -> insert -> EDT -> queries on the given device buffers as one
+ * CUDA graph (runs the step once outside the capture first); replay it with
+ * gvx_batch_graph_launch.  Blocking. */
+GVX_API gvx_status gvx_batch_graph_capture(gvx_batch *b, const float *d_xyz, const uint64_t *d_offsets, uint64_t n_total,
+                                           const float *d_qxyz, const uint32_t *d_qmap, uint64_t n_q, float *d_dist,
+                                           float *d_grad, gvx_stream stream);
+GVX_API gvx_status gvx_batch_graph_launch(gvx_batch *b, gvx_stream stream);
+
 /* ---- BitVectorVoxelMap (GV/voxelmap/BitVoxelMap.h) ---------------------- */
 
 /* Replaces BitVoxelMap<256>(dim, side, MT_BITVECTOR_VOXELMAP).  Unlike the
