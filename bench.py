@@ -318,13 +318,78 @@ def section_c4(hbm_peak):
             "traj_per_trajectory_loop_ms": round(ms_trl, 2), "traj_speedup_vs_loop": round(ms_trl / ms_tr, 1)}
 
 
+def section_c5(hbm_peak):
+    """64 uneven maps: voxelise + EDT + 10k trilinear distance/gradient queries
+    each, as (a) a per-map loop of the plain calls, (b) the batch API eagerly
+    (one launch per stage over all maps), (c) the batch step replayed as one
+    CUDA graph.  The batch results are checked bit-equal to the loop's."""
+    import torch
+    import gvx
+    from gvx import workloads
+    from gvx.batch import Batch
+    scenes = workloads.c5_maps()
+    maps = [gvx.DistanceVoxelMap(s.dims, s.side) for s in scenes]
+    pts_list = [torch.as_tensor(s.points).cuda() for s in scenes]
+    pts = torch.cat(pts_list)
+    offs = torch.zeros(len(scenes) + 1, dtype=torch.int64)
+    offs[1:] = torch.cumsum(torch.tensor([p.shape[0] for p in pts_list]), 0)
+    offs = offs.cuda()
+    rng = np.random.default_rng(11)
+    q_list, qm_list = [], []
+    for k, s in enumerate(scenes):
+        q_list.append(((0.5 + rng.random((10_000, 3)) * (np.asarray(s.dims) - 1)) * s.side).astype(np.float32))
+        qm_list.append(np.full(10_000, k, dtype=np.int32))
+    q = torch.as_tensor(np.concatenate(q_list)).cuda()
+    qm = torch.as_tensor(np.concatenate(qm_list)).cuda()
+    q_views = [q[k * 10_000:(k + 1) * 10_000] for k in range(len(scenes))]
+    nvox = sum(int(np.prod(s.dims)) for s in scenes)
+
+    def loop():
+        for k, m in enumerate(maps):
+            m.clearMap()
+            m.insertPointCloud(pts_list[k])
+            m.parallelBanding3D()
+            m.trilinear(q_views[k])
+
+    ms_loop = _time(loop, 3, warm=1)
+    torch.cuda.synchronize()
+    want = [m.data().clone() for m in maps]
+    want_q = [m.trilinear(q_views[k]) for k, m in enumerate(maps)]
+    b = Batch(maps)
+
+    def eager():
+        b.clear()
+        b.insert(pts, offs)
+        b.edt()
+        b.query(q, qm)
+
+    ms_eager = _time(eager, 5)
+    dist, grad = b.capture(pts, offs, q, qm)
+    ms_graph = _time(b.replay, 10)
+    torch.cuda.synchronize()
+    exact = all(torch.equal(m.data(), w) for m, w in zip(maps, want))
+    exact_q = all(torch.equal(dist[k * 10_000:(k + 1) * 10_000], want_q[k][0]) and
+                  torch.equal(grad[k * 10_000:(k + 1) * 10_000], want_q[k][1]) for k in range(len(maps)))
+    dims = [s.dims for s in scenes]
+    return {"workload": "64 maps, dims log-uniform in [64,384] per axis, 10k-1M box-scene points each; "
+                        "voxelise + exact EDT + 10k trilinear distance+gradient queries per map",
+            "total_voxels": nvox, "total_points": int(pts.shape[0]), "min_dims": list(min(dims, key=np.prod)),
+            "max_dims": list(max(dims, key=np.prod)),
+            "per_map_loop_ms": round(ms_loop, 3), "batch_eager_ms": round(ms_eager, 3),
+            "batch_graph_ms": round(ms_graph, 3),
+            "loop_gvoxel_per_s": round(nvox / ms_loop / 1e6, 3), "graph_gvoxel_per_s": round(nvox / ms_graph / 1e6, 3),
+            "graph_speedup_vs_loop": round(ms_loop / ms_graph, 2),
+            "bit_equal_to_loop": bool(exact and exact_q)}
+
+
 def run_sections(args, hbm_peak, pts_host):
     import torch
     out = {}
     for name, fn in (("c1_128", lambda: section_c1(hbm_peak)),
                      ("c2_collide_512", lambda: section_c2_collide(hbm_peak, pts_host)),
                      ("c3_spheres_lists", lambda: section_c3(hbm_peak)),
-                     ("c4_gradients", lambda: section_c4(hbm_peak))):
+                     ("c4_gradients", lambda: section_c4(hbm_peak)),
+                     ("c5_uneven_batch", lambda: section_c5(hbm_peak))):
         if args.sections not in ("all", "") and name not in args.sections.split(","):
             continue
         try:

@@ -19,11 +19,13 @@
 // streams them through shared memory in chunks of rows (cp.async, double
 // buffered; pass X transposes each chunk on the way in and out).  Within a
 // chunk the rows advance in lockstep and only the stack pops a row triggers
-// run divergently.  The proximate-site stack is compact (depth-indexed, each
-// entry carries its row): its top lives in an on-chip ring per lane together
-// with each entry's bisector, every push is written through to the map's
-// workspace, and phase 3 streams the stack back top-down in prefetched
-// blocks.  Stack order, tests and tie rules are the reference's.
+// run divergently; a lane with a long run of pops hands it to the whole warp,
+// which tests 31 stack entries per round.  The proximate-site stack is
+// compact (depth-indexed, each entry carries its row): its top lives in an
+// on-chip ring per lane together with each entry's bisector, every push is
+// written through to the map's workspace, and phase 3 streams the stack back
+// top-down through a prefetched on-chip window.  Stack order, tests and tie
+// rules are the reference's.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -34,6 +36,8 @@
 
 namespace gvx {
 namespace {
+
+constexpr unsigned kFullMask = 0xffffffffu;
 
 __device__ __forceinline__ void cp_async4(uint32_t* smem_dst, const uint32_t* gmem_src) {
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
@@ -217,6 +221,75 @@ struct SweepCfg {
   static_assert(2 * kRing >= 32, "the phase-3 window (32 entries per lane) aliases the ring");
 };
 
+// Finish the pops of lane `o` with the whole warp.  The stack entries of a
+// column are e_0 .. e_{n-1} with I_j = bisect(e_{j-1}, e_j); the sequential
+// loop pops e_j while !(I_j < bisect(e_j, cur)) and stops at j = 0.  Each
+// test depends only on e_j, I_j and cur, so lane t tests depth start - t and
+// the first kept depth (lowest t) is exactly where the sequential loop stops.
+// Lane 31 only supplies the entry below lane 30's, so a round covers 31
+// depths.  All 32 lanes call this; only lane o's state changes.
+template <class Cfg>
+__device__ __forceinline__ void coop_pops(int o, int a0_base, float c0f, uint32_t* ring_base, const uint32_t* gstk_base,
+                                          int& n, int& lo, const Col& cur, Col& top, float& top_i, Col& sec,
+                                          float& sec_i, float& i2) {
+  const int lane = threadIdx.x & 31;
+  const int on = __shfl_sync(kFullMask, n, o);
+  const int olo = __shfl_sync(kFullMask, lo, o);
+  const uint32_t ce = __shfl_sync(kFullMask, cur.e, o);
+  const float oa0f = small_to_float(a0_base + o);
+  const Col oc = make_col(ce, oa0f, c0f);
+  uint32_t* ringE = ring_base + o;
+  float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
+  const uint32_t* gstk = gstk_base + o;
+  for (int start = on - 1;; start -= 31) {
+    const int j = start - lane;
+    const int jc = max(j, 0);
+    uint32_t e;
+    float I = 0.f;
+    Col ec;
+    if (jc >= olo) {
+      e = ringE[(jc % Cfg::kRing) * 32];
+      I = ringI[(jc % Cfg::kRing) * 32];
+      ec = make_col(e, oa0f, c0f);
+    } else {
+      e = gstk[jc * 32];
+      ec = make_col(e, oa0f, c0f);
+      if (jc >= 1) I = bisect(make_col(gstk[(jc - 1) * 32], oa0f, c0f), ec);
+    }
+    const float b = bisect(ec, oc);
+    const bool keep = j <= 0 || I < b;
+    const unsigned kb = __ballot_sync(kFullMask, keep) & 0x7fffffffu;
+    if (kb) {
+      const int t = __ffs(kb) - 1;
+      // Refill lane o's ring with the tested entries from the kept depth
+      // down (their slots belong to popped depths), so its next pops stay on
+      // chip: after the push the ring holds depths >= new_lo.
+      const int u_last = min(t + Cfg::kRing - 2, 31);
+      const int new_lo = max(start - u_last, 0);
+      if (lane >= t && lane <= u_last && j >= 0 && jc < olo) {
+        ringE[(jc % Cfg::kRing) * 32] = e;
+        ringI[(jc % Cfg::kRing) * 32] = I;
+      }
+      const uint32_t e_top = __shfl_sync(kFullMask, e, t);
+      const float i_top = __shfl_sync(kFullMask, I, t);
+      const float b_top = __shfl_sync(kFullMask, b, t);
+      const uint32_t e_sec = __shfl_sync(kFullMask, e, t + 1);
+      const float i_sec = __shfl_sync(kFullMask, I, t + 1);
+      if (lane == o) {
+        n = start - t + 1;
+        lo = min(lo, new_lo);
+        top = make_col(e_top, oa0f, c0f);
+        top_i = i_top;
+        i2 = b_top;
+        sec = make_col(e_sec, oa0f, c0f);
+        sec_i = i_sec;
+      }
+      __syncwarp();  // the refill before lane o's next ring access
+      return;
+    }
+  }
+}
+
 // Issue the cp.async copies of chunk `c` (rows c*kRows ..) into `tile`.
 // Pass Y: tile[r*32 + lane] = row r of column lane.  Pass X: the chunk holds
 // x positions, transposed: tile[(x - r0)*33 + t] = element x of row t.
@@ -276,6 +349,11 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   const float c0f = small_to_float(z);
   const int nchunks = (L + kRows - 1) / kRows;
   const int tpitch = kXPass ? 33 : 32;
+  // Pops a lane runs alone per row before the warp takes over.  Pass Y (input:
+  // the nearest site per z column) has rare, long pop runs; in pass X nearly
+  // every row pushes and runs stay short, so there the warp never takes over
+  // (0) -- measured faster at 512^3.
+  constexpr int kSoloPops = kXPass ? 0 : 2;
 
   // ---- phase 2: proximate sites ------------------------------------------
   // Rows advance in lockstep (the per-row work runs on all 32 lanes); the pops
@@ -300,36 +378,57 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     for (int r = 0; r < rows; ++r) {
       const uint32_t v = tile[r * tpitch + lane];
       const uint32_t a = kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
-      if (a == kUninit) continue;
-      const Col cur = make_col(a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u), a0f, c0f);
+      const bool has = a != kUninit;
+      Col cur{0u, 0.f, 0.f};
       float i2 = 0.f;
-      if (n >= 1) i2 = bisect(top, cur);
-      while (n >= 2 && !(top_i < i2)) {  // top is dominated by (second, current): pop
-        --n;
-        top = sec;
-        top_i = sec_i;
-        if (n >= 2) {
-          const int d = n - 2;
-          if (d >= lo) {
-            sec = make_col(ringE[(d % Cfg::kRing) * 32], a0f, c0f);
-            sec_i = ringI[(d % Cfg::kRing) * 32];
-          } else {  // below the ring: the workspace has the entries
-            sec = make_col(gstk[d * 32], a0f, c0f);
-            sec_i = d >= 1 ? bisect(make_col(gstk[(d - 1) * 32], a0f, c0f), sec) : 0.f;
+      bool deep = false;
+      if (has) {
+        cur = make_col(a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u), a0f, c0f);
+        if (n >= 1) i2 = bisect(top, cur);
+        for (int p = 0; n >= 2 && !(top_i < i2); ++p) {  // top is dominated by (second, current): pop
+          if (kSoloPops > 0 && p == kSoloPops) {
+            deep = true;
+            break;
           }
+          --n;
+          top = sec;
+          top_i = sec_i;
+          if (n >= 2) {
+            const int d = n - 2;
+            if (d >= lo) {
+              sec = make_col(ringE[(d % Cfg::kRing) * 32], a0f, c0f);
+              sec_i = ringI[(d % Cfg::kRing) * 32];
+            } else {  // below the ring: the workspace has the entries
+              sec = make_col(gstk[d * 32], a0f, c0f);
+              sec_i = d >= 1 ? bisect(make_col(gstk[(d - 1) * 32], a0f, c0f), sec) : 0.f;
+            }
+          }
+          i2 = bisect(top, cur);
         }
-        i2 = bisect(top, cur);
       }
-      const int slot = (n % Cfg::kRing) * 32;  // push the current site
-      ringE[slot] = cur.e;
-      ringI[slot] = i2;
-      gstk[n * 32] = cur.e;
-      lo = max(lo, n - Cfg::kRing + 1);
-      ++n;
-      sec = top;
-      sec_i = top_i;
-      top = cur;
-      top_i = i2;
+      // Long pop runs: the warp tests 31 entries of one lane's stack per round.
+      if constexpr (kSoloPops > 0) {
+        unsigned deep_lanes = __ballot_sync(kFullMask, deep);
+        if (deep_lanes) __syncwarp();  // the owners' ring and workspace writes
+        while (deep_lanes) {
+          const int o = __ffs(deep_lanes) - 1;
+          deep_lanes &= deep_lanes - 1;
+          coop_pops<Cfg>(o, s.a0_base, c0f, wbase + 2 * Cfg::kTileWords, gstk - lane, n, lo, cur, top, top_i, sec,
+                         sec_i, i2);
+        }
+      }
+      if (has) {
+        const int slot = (n % Cfg::kRing) * 32;  // push the current site
+        ringE[slot] = cur.e;
+        ringI[slot] = i2;
+        gstk[n * 32] = cur.e;
+        lo = max(lo, n - Cfg::kRing + 1);
+        ++n;
+        sec = top;
+        sec_i = top_i;
+        top = cur;
+        top_i = i2;
+      }
     }
     __syncwarp();
     if (c + 2 < nchunks) stage_chunk<kXPass, kRows>((c & 1) ? tile1 : tile0, s, c + 2, vec16);

@@ -23,12 +23,13 @@ class Batch:
         h = ctypes.c_void_p()
         call("gvx_batch_create", arr, len(self.maps), ctypes.byref(h))
         self._h = h
+        self._destroy = lib().gvx_batch_destroy  # bound now: module globals may be gone at exit
         self._graph_bufs = None
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            lib().gvx_batch_destroy(h)
+            getattr(self, "_destroy", None) and self._destroy(h)
             self._h = None
 
     def clear(self) -> None:

@@ -65,11 +65,13 @@ class DistanceVoxelMap:
             self._owner = voxels
             call("gvx_dvm_wrap", ctypes.byref(d), self.voxel_side_length, _ptr(voxels), ctypes.byref(h))
         self._h = h
+        self._destroy = _abi.lib().gvx_dvm_destroy
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _abi.lib().gvx_dvm_destroy(h)
+            # bound at creation: module globals may already be gone at interpreter exit
+            getattr(self, "_destroy", None) and self._destroy(h)
             self._h = None
 
     @property
@@ -198,12 +200,14 @@ class BitVectorVoxelMap:
         h = ctypes.c_void_p()
         call("gvx_bvm_create", ctypes.byref(Dims(*self.dims)), self.voxel_side_length, ctypes.byref(h))
         self._h = h
+        self._destroy = _abi.lib().gvx_bvm_destroy
         self._count = torch.zeros(1, dtype=torch.int64, device="cuda")
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _abi.lib().gvx_bvm_destroy(h)
+            # bound at creation: module globals may already be gone at interpreter exit
+            getattr(self, "_destroy", None) and self._destroy(h)
             self._h = None
 
     @property
@@ -247,12 +251,14 @@ class BitVectorVoxelList:
         h = ctypes.c_void_p()
         call("gvx_blist_create", ctypes.byref(Dims(*self.dims)), self.voxel_side_length, ctypes.byref(h))
         self._h = h
+        self._destroy = _abi.lib().gvx_blist_destroy
         self._count = torch.zeros(1, dtype=torch.int64, device="cuda")
 
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _abi.lib().gvx_blist_destroy(h)
+            # bound at creation: module globals may already be gone at interpreter exit
+            getattr(self, "_destroy", None) and self._destroy(h)
             self._h = None
 
     @property
