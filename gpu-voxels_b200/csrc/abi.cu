@@ -171,8 +171,17 @@ gvx_status gvx_dvm_edt(gvx_dvm* m, uint32_t m1, uint32_t m2, uint32_t m3, gvx_st
 }
 
 gvx_status gvx_dvm_edt_pass(gvx_dvm* m, int pass, gvx_stream stream) {
-  if (m == nullptr || pass < 0 || pass > 2) return fail(GVX_ERR_INVALID_ARG, "map is null or pass not in {0,1,2}");
+  if (m == nullptr || pass < 0 || pass > 3) return fail(GVX_ERR_INVALID_ARG, "map is null or pass not in {0,1,2,3}");
   return cuda_status(launch_edt_pass(m->d_vox, m->d_scratch, m->dims, pass, as_stream(stream)), "EDT pass");
+}
+
+gvx_status gvx_dvm_edt_check(gvx_dvm* m, uint32_t* flags) {
+  if (m == nullptr || flags == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = edt_read_error(m->d_scratch, m->dims, flags);
+  if (e != cudaSuccess) return cuda_status(e, "EDT check");
+  if (*flags != 0) return fail(GVX_ERR_TIMEOUT, "EDT: a slice wait of the fused y->x sweep gave up (results invalid)");
+  return GVX_OK;
 }
 
 gvx_status gvx_dvm_sqdist(const gvx_dvm* m, const uint32_t* d_ids, uint64_t n, int32_t* d_out, gvx_stream stream) {

@@ -98,6 +98,8 @@ struct gvx_batch {
   gvx::BatchMap* d_table = nullptr;
   gvx::BatchItems items{};
   long long* d_prefix = nullptr;  // 3 x (n_maps + 1)
+  uint32_t* d_stacks = nullptr;   // fused Y -> X: one stack per resident warp
+  unsigned* d_sync = nullptr;     // slice counters of all maps, queue head, error word
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -110,11 +112,17 @@ gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** o
   if (out == nullptr || maps == nullptr || n_maps == 0) return fail(GVX_ERR_INVALID_ARG, "need at least one map");
   *out = nullptr;
   std::vector<BatchMap> table(n_maps);
+  uint32_t sync_words = 0, stack_len = 1;
   for (uint32_t k = 0; k < n_maps; ++k) {
     if (maps[k] == nullptr) return fail(GVX_ERR_INVALID_ARG, "null map in batch");
     const gvx_dvm* m = maps[k];
-    table[k] = BatchMap{m->d_vox, m->d_scratch, (int)m->dims.x, (int)m->dims.y, (int)m->dims.z, m->side, num_voxels(m->dims)};
+    table[k] = BatchMap{m->d_vox,  m->d_scratch, (int)m->dims.x,     (int)m->dims.y,
+                        (int)m->dims.z, m->side, num_voxels(m->dims), sync_words};
+    sync_words += m->dims.z;
+    stack_len = std::max(stack_len, std::max(m->dims.x, m->dims.y));
   }
+  const long long stack_warps = edt_batch_stack_warps();
+  if (stack_warps <= 0) return fail(GVX_ERR_CUDA, "occupancy query for the batched EDT failed");
   gvx_batch* b = new (std::nothrow) gvx_batch();
   if (b == nullptr) return fail(GVX_ERR_OOM, "host allocation failed");
   b->maps.assign(maps, maps + n_maps);
@@ -129,13 +137,23 @@ gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** o
   if (e == cudaSuccess) e = cudaMemcpy(b->d_table, table.data(), n_maps * sizeof(BatchMap), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_prefix, prefix.size() * sizeof(long long));
   if (e == cudaSuccess) e = cudaMemcpy(b->d_prefix, prefix.data(), prefix.size() * sizeof(long long), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_stacks, (size_t)stack_warps * stack_len * 32 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_sync, (sync_words + 2) * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(b->d_sync, 0, (sync_words + 2) * sizeof(unsigned));
   if (e != cudaSuccess) {
     if (b->d_table) cudaFree(b->d_table);
     if (b->d_prefix) cudaFree(b->d_prefix);
+    if (b->d_stacks) cudaFree(b->d_stacks);
+    if (b->d_sync) cudaFree(b->d_sync);
     delete b;
     return cuda_status(e, "batch table");
   }
   for (int p = 0; p < 3; ++p) b->items.d_prefix[p] = b->d_prefix + p * (size_t)(n_maps + 1);
+  b->items.d_stacks = b->d_stacks;
+  b->items.stack_warps = stack_warps;
+  b->items.stack_len = stack_len;
+  b->items.d_sync = b->d_sync;
+  b->items.sync_words = sync_words;
   *out = b;
   return GVX_OK;
 }
@@ -146,6 +164,8 @@ gvx_status gvx_batch_destroy(gvx_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->d_table) cudaFree(b->d_table);
   if (b->d_prefix) cudaFree(b->d_prefix);
+  if (b->d_stacks) cudaFree(b->d_stacks);
+  if (b->d_sync) cudaFree(b->d_sync);
   delete b;
   return GVX_OK;
 }
@@ -170,6 +190,15 @@ gvx_status gvx_batch_insert_points(gvx_batch* b, const float* d_xyz, const uint6
 gvx_status gvx_batch_edt(gvx_batch* b, gvx_stream stream) {
   if (b == nullptr) return fail(GVX_ERR_INVALID_ARG, "batch is null");
   return cuda_status(launch_edt_batch(b->d_table, b->items, as_stream(stream)), "batch EDT");
+}
+
+gvx_status gvx_batch_edt_check(gvx_batch* b, uint32_t* flags) {
+  if (b == nullptr || flags == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(flags, b->d_sync + b->items.sync_words + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e, "batch EDT check");
+  if (*flags != 0) return fail(GVX_ERR_TIMEOUT, "batched EDT: a slice wait gave up (results invalid)");
+  return GVX_OK;
 }
 
 gvx_status gvx_batch_query_trilinear(gvx_batch* b, const float* d_xyz, const uint32_t* d_map, uint64_t n, float* d_dist,

@@ -5,7 +5,7 @@
 // nearest site, including the reference's tie-breaking -- for any dims in
 // [1,1023]^3 (the reference itself needs x == y and x % 64 == 0).
 //
-// Three sweeps, one kernel each:
+// Three sweeps (pass Z one launch, passes Y and X one fused launch):
 //   pass Z : phase 1 (kernelPBAphase1FloodZ, VoxelMapOperationsPBA.hpp:63-124)
 //            per (x,y) column.
 //   pass Y : phase 2 + 3 (kernelPBAphase2ProximateBackpointers :289-379,
@@ -322,10 +322,10 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
 }
 
 // One warp item of pass Y (kXPass false) or X: 32 adjacent columns of one
-// z slice; wbase = the warp's kWarpWords of shared memory; the item's stack
-// area in the workspace starts at scratch + item * L * 32.
+// z slice; wbase = the warp's kWarpWords of shared memory; stack = the item's
+// L * 32 words of workspace (entry d of lane l at stack[d * 32 + l]).
 template <bool kXPass, int kRows>
-__device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t* __restrict__ scratch, int X, int Y,
+__device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t* __restrict__ stack, int X, int Y,
                                            int Z, long long item, uint32_t* wbase) {
   using Cfg = SweepCfg<kRows>;
   const int lane = threadIdx.x & 31;
@@ -344,7 +344,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   uint32_t* tile1 = wbase + Cfg::kTileWords;
   uint32_t* ringE = wbase + 2 * Cfg::kTileWords + lane;  // slot k: ringE[k * 32]
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
-  uint32_t* gstk = scratch + ((uint64_t)item * L) * 32 + lane;  // depth d: gstk[d * 32]
+  uint32_t* gstk = stack + lane;  // depth d: gstk[d * 32]
   const float a0f = small_to_float(s.a0_base + lane);  // this lane's column coordinate
   const float c0f = small_to_float(z);
   const int nchunks = (L + kRows - 1) / kRows;
@@ -542,6 +542,8 @@ __global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z_batch(const BatchM
   }
 }
 
+// One pass (Y or X) on its own, one warp per item (per-pass timing and the
+// fallback of the fused schedule below for maps too small for its stacks).
 template <bool kXPass, int kRows>
 __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     edt_sweep(uint32_t* __restrict__ map, uint32_t* __restrict__ scratch, int X, int Y, int Z) {
@@ -550,21 +552,127 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
   const int warp = threadIdx.x >> 5;
   const long long item = (long long)blockIdx.x * Cfg::kWarps + warp;
   if (item >= (long long)(((kXPass ? Y : X) + 31) >> 5) * Z) return;
-  sweep_item<kXPass, kRows>(map, scratch, X, Y, Z, item, s_sweep + (size_t)warp * Cfg::kWarpWords);
+  const int L = kXPass ? X : Y;
+  sweep_item<kXPass, kRows>(map, scratch + (uint64_t)item * L * 32, X, Y, Z, item, s_sweep + (size_t)warp * Cfg::kWarpWords);
 }
 
-template <bool kXPass, int kRows>
+// ---------------------------------------------------------------------------
+// Fused Y -> X schedule.  Pass X on slice z reads only what pass Y wrote to
+// slice z, so one persistent launch runs both: warps take items from a queue
+// (all Y items in z order, then all X items in z order), a Y item bumps its
+// slice's completion counter, and an X item first waits for its slice's
+// counter to reach the slice's Y item count.  Every item a wait depends on
+// sits earlier in the queue and was taken by a running warp that waits on
+// nothing, so the waits end; they are bounded all the same (kSpinLimit
+// sleeps, then the error word is set and the item is skipped).  The tail of
+// pass Y overlaps the start of pass X, and no warp idles while its block's
+// other warps finish.  Stacks are per resident warp (a warp's items run one
+// after the other).
+// ---------------------------------------------------------------------------
+constexpr unsigned kSpinLimit = 1u << 24;  // x ~128 ns sleeps: seconds
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// After a Y item: its output stores, then the slice counter.
+__device__ __forceinline__ void publish_slice(unsigned* done) {
+  __threadfence();
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) {
+    __threadfence();
+    atomicAdd(done, 1u);
+  }
+}
+
+// Before an X item: wait (bounded) until `need` Y items of the slice are done.
+__device__ __forceinline__ bool wait_slice(const unsigned* done, unsigned need, unsigned* err) {
+  int ok = 1;
+  if ((threadIdx.x & 31) == 0) {
+    unsigned spins = 0;
+    while (ld_acquire_gpu(done) < need) {
+      if (++spins > kSpinLimit) {
+        atomicOr(err, 1u);
+        ok = 0;
+        break;
+      }
+      __nanosleep(128);
+    }
+  }
+  __syncwarp();  // orders lane 0's acquire before every lane's loads
+  ok = __shfl_sync(kFullMask, ok, 0);
+  __threadfence();
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned next_item(unsigned* head) {
+  unsigned g = 0;
+  if ((threadIdx.x & 31) == 0) g = atomicAdd(head, 1u);
+  return __shfl_sync(kFullMask, g, 0);
+}
+
+// sync = [done: Z words][head][err], zeroed before the launch.
+template <int kRows>
 __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
-    edt_sweep_batch(const BatchMap* __restrict__ maps, const long long* __restrict__ prefix, uint32_t n_maps,
-                    long long total) {
+    edt_sweep_yx(uint32_t* __restrict__ map, uint32_t* __restrict__ stacks, unsigned* __restrict__ sync, int X, int Y,
+                 int Z) {
   using Cfg = SweepCfg<kRows>;
   extern __shared__ __align__(16) uint32_t s_sweep[];
   const int warp = threadIdx.x >> 5;
-  for (long long g = (long long)blockIdx.x * Cfg::kWarps + warp; g < total; g += (long long)gridDim.x * Cfg::kWarps) {
-    const uint32_t k = batch_owner(prefix, n_maps, g);
+  uint32_t* wbase = s_sweep + (size_t)warp * Cfg::kWarpWords;
+  uint32_t* stack = stacks + ((uint64_t)blockIdx.x * Cfg::kWarps + warp) * (uint64_t)max(X, Y) * 32;
+  unsigned* done = sync;
+  unsigned* head = sync + Z;
+  unsigned* err = head + 1;
+  const unsigned nxb = (X + 31) >> 5, nyb = (Y + 31) >> 5;
+  const unsigned ny = nxb * Z, nall = ny + nyb * Z;
+  for (unsigned g = next_item(head); g < nall; g = next_item(head)) {
+    if (g < ny) {
+      sweep_item<false, kRows>(map, stack, X, Y, Z, g, wbase);
+      publish_slice(done + g / nxb);
+    } else {
+      const unsigned item = g - ny;
+      if (wait_slice(done + item / nyb, nxb, err)) sweep_item<true, kRows>(map, stack, X, Y, Z, item, wbase);
+    }
+    __syncwarp();
+  }
+}
+
+// The same schedule over every map of a batch: the queue holds all maps' Y
+// items, then all maps' X items.  maps[k].sync_off locates map k's slice
+// counters in `sync`; the queue head and error word follow them.
+template <int kRows>
+__global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
+    edt_sweep_yx_batch(const BatchMap* __restrict__ maps, const long long* __restrict__ prefix_y,
+                       const long long* __restrict__ prefix_x, uint32_t n_maps, unsigned total_y, unsigned total_x,
+                       uint32_t* __restrict__ stacks, uint32_t stack_len, unsigned* __restrict__ sync,
+                       unsigned sync_words) {
+  using Cfg = SweepCfg<kRows>;
+  extern __shared__ __align__(16) uint32_t s_sweep[];
+  const int warp = threadIdx.x >> 5;
+  uint32_t* wbase = s_sweep + (size_t)warp * Cfg::kWarpWords;
+  uint32_t* stack = stacks + ((uint64_t)blockIdx.x * Cfg::kWarps + warp) * (uint64_t)stack_len * 32;
+  unsigned* head = sync + sync_words;
+  unsigned* err = head + 1;
+  const unsigned nall = total_y + total_x;
+  for (unsigned g = next_item(head); g < nall; g = next_item(head)) {
+    const bool x_item = g >= total_y;
+    const long long q = x_item ? (long long)(g - total_y) : (long long)g;
+    const long long* prefix = x_item ? prefix_x : prefix_y;
+    const uint32_t k = batch_owner(prefix, n_maps, q);
     const BatchMap m = maps[k];
-    sweep_item<kXPass, kRows>(m.vox, m.scratch, m.X, m.Y, m.Z, g - __ldg(prefix + k),
-                              s_sweep + (size_t)warp * Cfg::kWarpWords);
+    const unsigned item = (unsigned)(q - __ldg(prefix + k));
+    unsigned* done = sync + m.sync_off;
+    const unsigned nxb = (m.X + 31) >> 5;
+    if (!x_item) {
+      sweep_item<false, kRows>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+      publish_slice(done + item / nxb);
+    } else {
+      const unsigned nyb = (m.Y + 31) >> 5;
+      if (wait_slice(done + item / nyb, nxb, err)) sweep_item<true, kRows>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+    }
     __syncwarp();
   }
 }
@@ -581,12 +689,28 @@ int max_smem_optin() {
   return g_smem_optin;
 }
 
+template <typename K>
+cudaError_t prepare(K kern, int smem) {
+  if (smem > max_smem_optin()) return cudaErrorInvalidConfiguration;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  return e;
+}
+
+// Resident blocks of `kern` on the whole device.
+template <typename K>
+cudaError_t resident_blocks(K kern, int threads, int smem, long long* out) {
+  int per_sm = 0, dev = 0, sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  *out = (long long)std::max(per_sm, 1) * std::max(sm, 1);
+  return e;
+}
+
 cudaError_t launch_pass_z(uint32_t* map, gvx_dims d, cudaStream_t s) {
   const int smem = kZWarps * kZWarpWords * 4;
-  if (smem > max_smem_optin()) return cudaErrorInvalidConfiguration;
-  cudaError_t e = cudaFuncSetAttribute(edt_pass_z, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(edt_pass_z, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  cudaError_t e = prepare(edt_pass_z, smem);
   if (e != cudaSuccess) return e;
   const long long items = (long long)((d.x + 31) / 32) * d.y;
   edt_pass_z<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(map, (int)d.x, (int)d.y, (int)d.z);
@@ -600,39 +724,114 @@ cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStrea
   const long long items = ((cols + 31) / 32) * d.z;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
   auto kern = edt_sweep<kXPass, kRows>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  cudaError_t e = prepare(kern, smem);
   if (e != cudaSuccess) return e;
   kern<<<(unsigned)((items + Cfg::kWarps - 1) / Cfg::kWarps), Cfg::kWarps * 32, smem, s>>>(map, scratch, (int)d.x,
                                                                                           (int)d.y, (int)d.z);
   return cudaGetLastError();
 }
 
-}  // namespace
-
-uint64_t edt_scratch_words(gvx_dims d) {
+uint64_t stack_words(gvx_dims d) {
   const uint64_t y_pass = (uint64_t)((d.x + 31) / 32) * 32 * d.y * d.z;
   const uint64_t x_pass = (uint64_t)((d.y + 31) / 32) * 32 * d.x * d.z;
   return std::max(y_pass, x_pass);
 }
 
-// Sweep variant: rows per staging chunk (16 or 32).  The environment
-// variable GVX_EDT_SWEEP_ROWS overrides the default for experiments.
-static int g_sweep_rows = -1;
-void set_edt_sweep_rows(int rows) { g_sweep_rows = rows; }
+// Fused Y -> X launch for one map: the per-warp stacks live in the per-item
+// stack area of the workspace, the slice counters right after it.  A map
+// whose stack area cannot hold one block's stacks runs the two passes as
+// separate launches instead.
+template <int kRows>
+cudaError_t launch_sweep_yx(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStream_t s) {
+  using Cfg = SweepCfg<kRows>;
+  const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
+  auto kern = edt_sweep_yx<kRows>;
+  cudaError_t e = prepare(kern, smem);
+  long long blocks = 0;
+  if (e == cudaSuccess) e = resident_blocks(kern, Cfg::kWarps * 32, smem, &blocks);
+  if (e != cudaSuccess) return e;
+  const uint64_t sw = stack_words(d);
+  const uint64_t per_block = (uint64_t)Cfg::kWarps * std::max(d.x, d.y) * 32;
+  const long long items = (long long)((d.x + 31) / 32) * d.z + (long long)((d.y + 31) / 32) * d.z;
+  blocks = std::min<long long>({blocks, (long long)(sw / per_block), (items + Cfg::kWarps - 1) / Cfg::kWarps});
+  if (blocks < 1) {
+    e = launch_sweep<false, kRows>(map, scratch, d, s);
+    return e == cudaSuccess ? launch_sweep<true, kRows>(map, scratch, d, s) : e;
+  }
+  unsigned* sync = scratch + sw;
+  e = cudaMemsetAsync(sync, 0, (d.z + 2) * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  kern<<<(unsigned)blocks, Cfg::kWarps * 32, smem, s>>>(map, scratch, sync, (int)d.x, (int)d.y, (int)d.z);
+  return cudaGetLastError();
+}
 
-cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s) {
+// Rows per staging chunk of the sweeps: 16 unless the environment variable
+// GVX_EDT_SWEEP_ROWS or set_edt_sweep_rows picks 32.
+int g_sweep_rows = -1;
+
+int sweep_rows() {
   if (g_sweep_rows < 0) {
     const char* env = getenv("GVX_EDT_SWEEP_ROWS");
-    g_sweep_rows = env ? atoi(env) : 16;
+    g_sweep_rows = (env && atoi(env) == 32) ? 32 : 16;
   }
-  const bool big = g_sweep_rows == 32;
+  return g_sweep_rows;
+}
+
+template <int kRows>
+cudaError_t launch_yx_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s) {
+  using Cfg = SweepCfg<kRows>;
+  const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
+  auto kern = edt_sweep_yx_batch<kRows>;
+  cudaError_t e = prepare(kern, smem);
+  long long blocks = 0;
+  if (e == cudaSuccess) e = resident_blocks(kern, Cfg::kWarps * 32, smem, &blocks);
+  if (e != cudaSuccess) return e;
+  blocks = std::min<long long>(blocks, it.stack_warps / Cfg::kWarps);
+  blocks = std::min<long long>(blocks, (it.total[1] + it.total[2] + Cfg::kWarps - 1) / Cfg::kWarps);
+  if (blocks < 1) return cudaErrorInvalidConfiguration;
+  e = cudaMemsetAsync(it.d_sync, 0, (it.sync_words + 2) * sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  kern<<<(unsigned)blocks, Cfg::kWarps * 32, smem, s>>>(d_table, it.d_prefix[1], it.d_prefix[2], it.n_maps,
+                                                        (unsigned)it.total[1], (unsigned)it.total[2], it.d_stacks,
+                                                        it.stack_len, it.d_sync, it.sync_words);
+  return cudaGetLastError();
+}
+
+template <int kRows>
+long long batch_stack_warps() {
+  using Cfg = SweepCfg<kRows>;
+  const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
+  long long blocks = 0;
+  if (prepare(edt_sweep_yx_batch<kRows>, smem) != cudaSuccess ||
+      resident_blocks(edt_sweep_yx_batch<kRows>, Cfg::kWarps * 32, smem, &blocks) != cudaSuccess)
+    return -1;
+  return blocks * Cfg::kWarps;
+}
+
+}  // namespace
+
+void set_edt_sweep_rows(int rows) { g_sweep_rows = rows == 32 ? 32 : 16; }
+
+uint64_t edt_scratch_words(gvx_dims d) { return stack_words(d) + ((uint64_t)d.z + 2 + 31) / 32 * 32; }
+
+cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s) {
+  const bool big = sweep_rows() == 32;
   switch (pass) {
     case 0: return launch_pass_z(d_vox, d, s);
     case 1: return big ? launch_sweep<false, 32>(d_vox, d_scratch, d, s) : launch_sweep<false, 16>(d_vox, d_scratch, d, s);
     case 2: return big ? launch_sweep<true, 32>(d_vox, d_scratch, d, s) : launch_sweep<true, 16>(d_vox, d_scratch, d, s);
+    case 3: return big ? launch_sweep_yx<32>(d_vox, d_scratch, d, s) : launch_sweep_yx<16>(d_vox, d_scratch, d, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s) {
+  cudaError_t e = launch_edt_pass(d_vox, d_scratch, d, 0, s);
+  return e == cudaSuccess ? launch_edt_pass(d_vox, d_scratch, d, 3, s) : e;
+}
+
+cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag) {
+  return cudaMemcpy(flag, d_scratch + stack_words(d) + d.z + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost);
 }
 
 long long edt_pass_items(gvx_dims d, int pass) {
@@ -643,59 +842,21 @@ long long edt_pass_items(gvx_dims d, int pass) {
   }
 }
 
-namespace {
-
-template <typename K>
-cudaError_t launch_persistent(K kern, int warps, int smem, const BatchMap* table, const long long* prefix, uint32_t n,
-                              long long total, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-  if (e != cudaSuccess) return e;
-  int per_sm = 0, dev = 0, sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
-  if (e != cudaSuccess) return e;
-  const long long need = (total + warps - 1) / warps;
-  const long long grid = std::max<long long>(1, std::min<long long>(need, (long long)std::max(per_sm, 1) * std::max(sm, 1)));
-  kern<<<(unsigned)grid, warps * 32, smem, s>>>(table, prefix, n, total);
-  return cudaGetLastError();
+long long edt_batch_stack_warps() {
+  return std::max(batch_stack_warps<16>(), batch_stack_warps<32>());
 }
-
-}  // namespace
 
 cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s) {
-  if (g_sweep_rows < 0) {
-    const char* env = getenv("GVX_EDT_SWEEP_ROWS");
-    g_sweep_rows = env ? atoi(env) : 16;
-  }
-  cudaError_t e = launch_persistent(edt_pass_z_batch, kZWarps, kZWarps * kZWarpWords * 4, d_table, it.d_prefix[0],
-                                    it.n_maps, it.total[0], s);
+  const int smem = kZWarps * kZWarpWords * 4;
+  cudaError_t e = prepare(edt_pass_z_batch, smem);
+  long long blocks = 0;
+  if (e == cudaSuccess) e = resident_blocks(edt_pass_z_batch, kZWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
-  if (g_sweep_rows == 32) {
-    using C = SweepCfg<32>;
-    e = launch_persistent(edt_sweep_batch<false, 32>, C::kWarps, C::kWarps * C::kWarpWords * 4, d_table, it.d_prefix[1],
-                          it.n_maps, it.total[1], s);
-    if (e == cudaSuccess)
-      e = launch_persistent(edt_sweep_batch<true, 32>, C::kWarps, C::kWarps * C::kWarpWords * 4, d_table,
-                            it.d_prefix[2], it.n_maps, it.total[2], s);
-  } else {
-    using C = SweepCfg<16>;
-    e = launch_persistent(edt_sweep_batch<false, 16>, C::kWarps, C::kWarps * C::kWarpWords * 4, d_table, it.d_prefix[1],
-                          it.n_maps, it.total[1], s);
-    if (e == cudaSuccess)
-      e = launch_persistent(edt_sweep_batch<true, 16>, C::kWarps, C::kWarps * C::kWarpWords * 4, d_table,
-                            it.d_prefix[2], it.n_maps, it.total[2], s);
-  }
-  return e;
-}
-
-cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s) {
-  for (int pass = 0; pass < 3; ++pass) {
-    cudaError_t e = launch_edt_pass(d_vox, d_scratch, d, pass, s);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+  blocks = std::max<long long>(1, std::min<long long>(blocks, (it.total[0] + kZWarps - 1) / kZWarps));
+  edt_pass_z_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0]);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return sweep_rows() == 32 ? launch_yx_batch<32>(d_table, it, s) : launch_yx_batch<16>(d_table, it, s);
 }
 
 }  // namespace gvx

@@ -11,10 +11,11 @@
 // that is part of the library image instead.
 //
 // The workspace is a file-scope __device__ array of kStaticWorkspaceWords
-// 32-bit words (64 MiB).  Every GPU on which the library's kernels are loaded
-// holds these 64 MiB until the process exits.  Maps whose EDT workspace would
-// exceed it (more than 16,777,216 voxels once x and y are rounded up to
-// multiples of 32; 256^3 fits) are rejected with GVX_ERR_OUT_OF_DOMAIN.
+// 32-bit words: 64 MiB of stack area plus 8 KiB for the EDT's per-slice
+// counters.  Every GPU on which the library's kernels are loaded holds it
+// until the process exits.  Maps whose EDT workspace would exceed it (more
+// than 16,777,216 voxels once x and y are rounded up to multiples of 32;
+// 256^3 fits) are rejected with GVX_ERR_OUT_OF_DOMAIN.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -25,7 +26,7 @@
 namespace gvx {
 namespace {
 
-constexpr uint64_t kStaticWorkspaceWords = 16ull * 1024 * 1024;  // 64 MiB
+constexpr uint64_t kStaticWorkspaceWords = 16ull * 1024 * 1024 + 2048;  // 64 MiB + 8 KiB
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) uint32_t g_edt_workspace[kStaticWorkspaceWords];

@@ -71,14 +71,22 @@ struct BatchMap {
   int X, Y, Z;
   float side;
   uint64_t nvox;
+  uint32_t sync_off;  // first of this map's Z slice counters in BatchItems::d_sync
 };
 
 // Work-item layout of the batched EDT: for pass p, map k owns warp items
-// [prefix[p][k], prefix[p][k+1]).
+// [prefix[p][k], prefix[p][k+1]).  The fused Y -> X launch keeps one stack of
+// stack_len rows per resident warp in d_stacks and its slice counters, queue
+// head and error word in d_sync (sync_words + 2 words).
 struct BatchItems {
   long long* d_prefix[3];
   long long total[3];
   uint32_t n_maps;
+  uint32_t* d_stacks;
+  long long stack_warps;
+  uint32_t stack_len;
+  unsigned* d_sync;
+  unsigned sync_words;
 };
 
 // Error reporting shared by the ABI units.
@@ -95,9 +103,18 @@ cudaError_t launch_dvm_insert(uint32_t* d_vox, gvx_dims d, float side, const flo
                               uint32_t* d_outside, cudaStream_t s);
 cudaError_t launch_bvm_insert(uint8_t* d_vox, gvx_dims d, float side, const float* d_xyz, uint64_t n, uint32_t meaning,
                               uint32_t* d_outside, cudaStream_t s);
+// EDT workspace: the per-item stack area, then Z slice counters, the queue
+// head and the error word of the fused Y -> X launch.
 uint64_t edt_scratch_words(gvx_dims d);
 cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s);
+// pass 0 = Z, 1 = Y, 2 = X (one launch each), 3 = fused Y -> X
 cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s);
+// Synchronous read of the error word the last fused launch left (0 = ok).
+cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag);
+// Resident warps of the fused batch launch (size of the batch stack pool).
+long long edt_batch_stack_warps();
+// Rows per staging chunk of the sweeps (16 or 32).
+void set_edt_sweep_rows(int rows);
 // Warp work items of one EDT pass for a map of dims d.
 long long edt_pass_items(gvx_dims d, int pass);
 // All maps of a batch, one persistent launch per pass.

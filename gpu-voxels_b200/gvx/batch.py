@@ -42,6 +42,12 @@ class Batch:
     def edt(self) -> None:
         call("gvx_batch_edt", self._h, _stream())
 
+    def edt_check(self) -> int:
+        """Synchronise and return the error word of the last batched EDT (0 = ok)."""
+        flags = ctypes.c_uint32(0)
+        call("gvx_batch_edt_check", self._h, ctypes.byref(flags))
+        return int(flags.value)
+
     def query(self, xyz: torch.Tensor, map_index: torch.Tensor, with_grad: bool = True):
         n = xyz.shape[0]
         dist = torch.empty(n, dtype=torch.float32, device="cuda")

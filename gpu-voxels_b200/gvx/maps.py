@@ -102,8 +102,16 @@ class DistanceVoxelMap:
         call("gvx_dvm_edt", self._h, m1, m2, m3, _stream())
 
     def edt_pass(self, pass_index: int) -> None:
-        """One EDT sweep (0: z, 1: y, 2: x)."""
+        """One EDT stage: 0 = z sweep, 1 = y sweep, 2 = x sweep, 3 = y and x
+        sweeps as the one fused launch parallelBanding3D uses."""
         call("gvx_dvm_edt_pass", self._h, int(pass_index), _stream())
+
+    def edt_check(self) -> int:
+        """Synchronise and return the error word of the last EDT (0 = ok);
+        raises GvxError (GVX_ERR_TIMEOUT) when a bounded wait gave up."""
+        flags = ctypes.c_uint32(0)
+        call("gvx_dvm_edt_check", self._h, ctypes.byref(flags))
+        return int(flags.value)
 
     def getSquaredDistances(self, ids: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
         ids = _dev_u32(ids)

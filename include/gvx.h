@@ -88,10 +88,17 @@ GVX_API gvx_status gvx_dvm_insert_points(gvx_dvm *m, const float *d_xyz, uint64_
  * reference with band counts (1,1,1).  The band counts are accepted for
  * API compatibility; results never depend on them. */
 GVX_API gvx_status gvx_dvm_edt(gvx_dvm *m, uint32_t m1, uint32_t m2, uint32_t m3, gvx_stream stream);
-/* One sweep of the EDT (0: z, 1: y, 2: x), in the order gvx_dvm_edt runs
- * them; for per-pass timing and tests.  Pass 0 alone equals the reference's
+/* One stage of the EDT, for per-pass timing and tests: 0 = the z sweep,
+ * 1 = the y sweep, 2 = the x sweep (one launch each), 3 = the y and x sweeps
+ * as the single fused launch gvx_dvm_edt uses (0 then 3 == gvx_dvm_edt;
+ * 0, 1, 2 gives the same result).  Pass 0 alone equals the reference's
  * phase 1 (kernelPBAphase1FloodZ, GV/voxelmap/kernels/VoxelMapOperationsPBA.hpp:63-124). */
 GVX_API gvx_status gvx_dvm_edt_pass(gvx_dvm *m, int pass, gvx_stream stream);
+/* Synchronises the device and reads the error word of the last EDT on this
+ * map: *flags = 0 when every bounded wait of the fused y -> x sweep ended in
+ * time, else non-zero with GVX_ERR_TIMEOUT (the map's content is then
+ * invalid).  No counterpart in the reference, whose EDT has no waits. */
+GVX_API gvx_status gvx_dvm_edt_check(gvx_dvm *m, uint32_t *flags);
 
 /* No counterpart in the reference.  The same EDT as gvx_dvm_edt, in place on
  * caller-owned device voxels (uint32 DistanceVoxels, x fastest, 16-byte
@@ -179,8 +186,11 @@ GVX_API gvx_status gvx_batch_clear(gvx_batch *b, gvx_stream stream);
 /* Points of all maps concatenated; map k owns points [d_offsets[k], d_offsets[k+1]). */
 GVX_API gvx_status gvx_batch_insert_points(gvx_batch *b, const float *d_xyz, const uint64_t *d_offsets, uint64_t n_total,
                                            gvx_stream stream);
-/* EDT of every map, bit-identical to gvx_dvm_edt per map. */
+/* EDT of every map, bit-identical to gvx_dvm_edt per map: one launch for the
+ * z sweeps of all maps, one fused launch for their y and x sweeps. */
 GVX_API gvx_status gvx_batch_edt(gvx_batch *b, gvx_stream stream);
+/* As gvx_dvm_edt_check, for the last gvx_batch_edt. */
+GVX_API gvx_status gvx_batch_edt_check(gvx_batch *b, uint32_t *flags);
 /* Query i is answered on map d_map[i]; d_grad optional. */
 GVX_API gvx_status gvx_batch_query_trilinear(gvx_batch *b, const float *d_xyz, const uint32_t *d_map, uint64_t n,
                                              float *d_dist, float *d_grad, gvx_stream stream);

@@ -50,7 +50,7 @@ def test_batch_edt_equals_per_map_and_oracle():
     b.edt()
     q, qm = _queries(scenes)
     dist, grad = b.query(q, qm)
-    torch.cuda.synchronize()
+    assert b.edt_check() == 0
     for k, (dims, side, p) in enumerate(scenes):
         want = oracle.dvm_empty(dims)
         oracle.dvm_insert(want, dims, side, p)

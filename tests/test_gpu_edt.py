@@ -40,6 +40,26 @@ def test_edt_random_scenes(dims, seed, npts):
     _check(dims, 1.0, pts)
 
 
+@pytest.mark.parametrize("dims", [(96, 40, 70), (33, 65, 129), (256, 256, 64), (1, 50, 50), (50, 1, 50), (7, 9, 3)])
+def test_fused_yx_sweep_equals_separate_passes(dims):
+    """The fused y -> x launch (stage 3, what parallelBanding3D runs) gives the
+    same map as the y and x sweeps launched one after the other, and its
+    bounded slice waits all end in time."""
+    rng = np.random.default_rng(sum(dims))
+    n = max(1, int(np.prod(dims)) // 200)
+    pts = torch.as_tensor((rng.random((n, 3)) * np.asarray(dims)).astype(np.float32)).cuda()
+    a = gvx.DistanceVoxelMap(dims, 1.0)
+    b = gvx.DistanceVoxelMap(dims, 1.0)
+    for m in (a, b):
+        m.insertPointCloud(pts)
+        m.edt_pass(0)
+    a.edt_pass(1)
+    a.edt_pass(2)
+    b.edt_pass(3)
+    assert b.edt_check() == 0
+    assert torch.equal(a.data(), b.data())
+
+
 def test_edt_tie_rich_lattice():
     dims = (128, 128, 131)
     _check(dims, 1.0, refgeom.equidistant_points_fast(10_000, dims, 1.0))
