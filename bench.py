@@ -59,7 +59,7 @@ class ClockSampler:
              "clocks_event_reasons.sw_power_cap")
         try:
             self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                           "--format=csv,noheader,nounits", "-lms", "100"],
+                                           "--format=csv,noheader,nounits", "-lms", "50"],
                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
@@ -93,8 +93,8 @@ class ClockSampler:
 
 
 def _traffic_from_profiles():
-    """DRAM bytes per voxel of the dominant EDT pass from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "edt_passes_512.txt")
+    """DRAM bytes per voxel of the EDT kernels from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "edt_kernels_c2_512cubed.txt")
     try:
         vals = {}
         with open(path) as f:
@@ -407,7 +407,7 @@ def run_sections(args, hbm_peak, pts_host):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sections", default="all", help="comma list of extra sections or 'none'")

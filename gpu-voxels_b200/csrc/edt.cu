@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 
 #include "gvx_internal.cuh"
 
@@ -689,33 +690,52 @@ int max_smem_optin() {
   return g_smem_optin;
 }
 
-template <typename K>
-cudaError_t prepare(K kern, int smem) {
-  if (smem > max_smem_optin()) return cudaErrorInvalidConfiguration;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-  return e;
-}
+// Per-kernel launch set-up, done once per device: the dynamic shared memory
+// attribute and the number of resident blocks on the whole device (the
+// queries cost microseconds, which small maps would pay on every call).
+constexpr int kMaxDevices = 64;
+struct KernelSetup {
+  std::once_flag once[kMaxDevices];
+  cudaError_t err[kMaxDevices] = {};
+  long long blocks[kMaxDevices] = {};
+};
 
-// Resident blocks of `kern` on the whole device.
-template <typename K>
-cudaError_t resident_blocks(K kern, int threads, int smem, long long* out) {
-  int per_sm = 0, dev = 0, sm = 0;
+template <auto kKernel>
+cudaError_t kernel_setup(int threads, int smem, long long* resident) {
+  static KernelSetup st;  // one per kernel
+  const auto kern = kKernel;
+  int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-  *out = (long long)std::max(per_sm, 1) * std::max(sm, 1);
-  return e;
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::call_once(st.once[dev], [&] {
+    cudaError_t r = smem > max_smem_optin() ? cudaErrorInvalidConfiguration : cudaSuccess;
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (r == cudaSuccess)
+      r = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    int per_sm = 0, sm = 0;
+    if (r == cudaSuccess) r = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+    if (r == cudaSuccess) r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    st.err[dev] = r;
+    st.blocks[dev] = (long long)std::max(per_sm, 1) * std::max(sm, 1);
+  });
+  if (resident) *resident = st.blocks[dev];
+  return st.err[dev];
 }
 
 cudaError_t launch_pass_z(uint32_t* map, gvx_dims d, cudaStream_t s) {
   const int smem = kZWarps * kZWarpWords * 4;
-  cudaError_t e = prepare(edt_pass_z, smem);
+  cudaError_t e = kernel_setup<edt_pass_z>(kZWarps * 32, smem, nullptr);
   if (e != cudaSuccess) return e;
   const long long items = (long long)((d.x + 31) / 32) * d.y;
   edt_pass_z<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(map, (int)d.x, (int)d.y, (int)d.z);
   return cudaGetLastError();
 }
+
+// Workspace layout: [slice counters, queue head, error word: sync_words(d)]
+// [stack area].  The per-pass launches index the stack area per item; the
+// fused launch uses it as one stack per resident warp.
+uint64_t sync_words(gvx_dims d) { return ((uint64_t)d.z + 2 + 31) / 32 * 32; }
 
 template <bool kXPass, int kRows>
 cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStream_t s) {
@@ -724,33 +744,41 @@ cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStrea
   const long long items = ((cols + 31) / 32) * d.z;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
   auto kern = edt_sweep<kXPass, kRows>;
-  cudaError_t e = prepare(kern, smem);
+  cudaError_t e = kernel_setup<edt_sweep<kXPass, kRows>>(Cfg::kWarps * 32, smem, nullptr);
   if (e != cudaSuccess) return e;
-  kern<<<(unsigned)((items + Cfg::kWarps - 1) / Cfg::kWarps), Cfg::kWarps * 32, smem, s>>>(map, scratch, (int)d.x,
-                                                                                          (int)d.y, (int)d.z);
+  kern<<<(unsigned)((items + Cfg::kWarps - 1) / Cfg::kWarps), Cfg::kWarps * 32, smem, s>>>(
+      map, scratch + sync_words(d), (int)d.x, (int)d.y, (int)d.z);
   return cudaGetLastError();
 }
 
+// Per-item stack area of the per-pass launches.
 uint64_t stack_words(gvx_dims d) {
   const uint64_t y_pass = (uint64_t)((d.x + 31) / 32) * 32 * d.y * d.z;
   const uint64_t x_pass = (uint64_t)((d.y + 31) / 32) * 32 * d.x * d.z;
   return std::max(y_pass, x_pass);
 }
 
-// Fused Y -> X launch for one map: the per-warp stacks live in the per-item
-// stack area of the workspace, the slice counters right after it.  A map
-// whose stack area cannot hold one block's stacks runs the two passes as
-// separate launches instead.
+// Stack area that lets the fused launch run one warp per item, up to
+// kFusedWarpCap warps (more than a B200 keeps resident).
+constexpr uint64_t kFusedWarpCap = 4096;
+uint64_t fused_stack_words(gvx_dims d) {
+  const uint64_t items = (uint64_t)((d.x + 31) / 32) * d.z + (uint64_t)((d.y + 31) / 32) * d.z;
+  const uint64_t warps = std::min<uint64_t>((items + 7) / 8 * 8, kFusedWarpCap);
+  return warps * std::max(d.x, d.y) * 32;
+}
+
+// Fused Y -> X launch for one map: as many blocks as are resident, as the
+// stack area holds and as there are items.  A workspace whose stack area
+// cannot hold one block's stacks runs the two passes as separate launches.
 template <int kRows>
-cudaError_t launch_sweep_yx(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStream_t s) {
+cudaError_t launch_sweep_yx(uint32_t* map, uint32_t* scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s) {
   using Cfg = SweepCfg<kRows>;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
   auto kern = edt_sweep_yx<kRows>;
-  cudaError_t e = prepare(kern, smem);
   long long blocks = 0;
-  if (e == cudaSuccess) e = resident_blocks(kern, Cfg::kWarps * 32, smem, &blocks);
+  cudaError_t e = kernel_setup<edt_sweep_yx<kRows>>(Cfg::kWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
-  const uint64_t sw = stack_words(d);
+  const uint64_t sw = scratch_words - sync_words(d);
   const uint64_t per_block = (uint64_t)Cfg::kWarps * std::max(d.x, d.y) * 32;
   const long long items = (long long)((d.x + 31) / 32) * d.z + (long long)((d.y + 31) / 32) * d.z;
   blocks = std::min<long long>({blocks, (long long)(sw / per_block), (items + Cfg::kWarps - 1) / Cfg::kWarps});
@@ -758,10 +786,11 @@ cudaError_t launch_sweep_yx(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaSt
     e = launch_sweep<false, kRows>(map, scratch, d, s);
     return e == cudaSuccess ? launch_sweep<true, kRows>(map, scratch, d, s) : e;
   }
-  unsigned* sync = scratch + sw;
+  unsigned* sync = scratch;
   e = cudaMemsetAsync(sync, 0, (d.z + 2) * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  kern<<<(unsigned)blocks, Cfg::kWarps * 32, smem, s>>>(map, scratch, sync, (int)d.x, (int)d.y, (int)d.z);
+  kern<<<(unsigned)blocks, Cfg::kWarps * 32, smem, s>>>(map, scratch + sync_words(d), sync, (int)d.x, (int)d.y,
+                                                        (int)d.z);
   return cudaGetLastError();
 }
 
@@ -782,9 +811,8 @@ cudaError_t launch_yx_batch(const BatchMap* d_table, const BatchItems& it, cudaS
   using Cfg = SweepCfg<kRows>;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
   auto kern = edt_sweep_yx_batch<kRows>;
-  cudaError_t e = prepare(kern, smem);
   long long blocks = 0;
-  if (e == cudaSuccess) e = resident_blocks(kern, Cfg::kWarps * 32, smem, &blocks);
+  cudaError_t e = kernel_setup<edt_sweep_yx_batch<kRows>>(Cfg::kWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
   blocks = std::min<long long>(blocks, it.stack_warps / Cfg::kWarps);
   blocks = std::min<long long>(blocks, (it.total[1] + it.total[2] + Cfg::kWarps - 1) / Cfg::kWarps);
@@ -802,9 +830,7 @@ long long batch_stack_warps() {
   using Cfg = SweepCfg<kRows>;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
   long long blocks = 0;
-  if (prepare(edt_sweep_yx_batch<kRows>, smem) != cudaSuccess ||
-      resident_blocks(edt_sweep_yx_batch<kRows>, Cfg::kWarps * 32, smem, &blocks) != cudaSuccess)
-    return -1;
+  if (kernel_setup<edt_sweep_yx_batch<kRows>>(Cfg::kWarps * 32, smem, &blocks) != cudaSuccess) return -1;
   return blocks * Cfg::kWarps;
 }
 
@@ -812,26 +838,31 @@ long long batch_stack_warps() {
 
 void set_edt_sweep_rows(int rows) { g_sweep_rows = rows == 32 ? 32 : 16; }
 
-uint64_t edt_scratch_words(gvx_dims d) { return stack_words(d) + ((uint64_t)d.z + 2 + 31) / 32 * 32; }
+uint64_t edt_scratch_words_min(gvx_dims d) { return sync_words(d) + stack_words(d); }
+uint64_t edt_scratch_words(gvx_dims d) { return sync_words(d) + std::max(stack_words(d), fused_stack_words(d)); }
 
-cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s) {
+cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, int pass,
+                            cudaStream_t s) {
+  if (pass != 0 && scratch_words < edt_scratch_words_min(d)) return cudaErrorInvalidValue;
   const bool big = sweep_rows() == 32;
   switch (pass) {
     case 0: return launch_pass_z(d_vox, d, s);
     case 1: return big ? launch_sweep<false, 32>(d_vox, d_scratch, d, s) : launch_sweep<false, 16>(d_vox, d_scratch, d, s);
     case 2: return big ? launch_sweep<true, 32>(d_vox, d_scratch, d, s) : launch_sweep<true, 16>(d_vox, d_scratch, d, s);
-    case 3: return big ? launch_sweep_yx<32>(d_vox, d_scratch, d, s) : launch_sweep_yx<16>(d_vox, d_scratch, d, s);
+    case 3:
+      return big ? launch_sweep_yx<32>(d_vox, d_scratch, scratch_words, d, s)
+                 : launch_sweep_yx<16>(d_vox, d_scratch, scratch_words, d, s);
     default: return cudaErrorInvalidValue;
   }
 }
 
-cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s) {
-  cudaError_t e = launch_edt_pass(d_vox, d_scratch, d, 0, s);
-  return e == cudaSuccess ? launch_edt_pass(d_vox, d_scratch, d, 3, s) : e;
+cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s) {
+  cudaError_t e = launch_edt_pass(d_vox, d_scratch, scratch_words, d, 0, s);
+  return e == cudaSuccess ? launch_edt_pass(d_vox, d_scratch, scratch_words, d, 3, s) : e;
 }
 
 cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag) {
-  return cudaMemcpy(flag, d_scratch + stack_words(d) + d.z + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  return cudaMemcpy(flag, d_scratch + d.z + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost);
 }
 
 long long edt_pass_items(gvx_dims d, int pass) {
@@ -848,9 +879,8 @@ long long edt_batch_stack_warps() {
 
 cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s) {
   const int smem = kZWarps * kZWarpWords * 4;
-  cudaError_t e = prepare(edt_pass_z_batch, smem);
   long long blocks = 0;
-  if (e == cudaSuccess) e = resident_blocks(edt_pass_z_batch, kZWarps * 32, smem, &blocks);
+  cudaError_t e = kernel_setup<edt_pass_z_batch>(kZWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
   blocks = std::max<long long>(1, std::min<long long>(blocks, (it.total[0] + kZWarps - 1) / kZWarps));
   edt_pass_z_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0]);

@@ -73,7 +73,7 @@ extern "C" gvx_status gvx_dvm_edt_static_workspace(uint32_t* d_voxels, const gvx
     set_error("voxel buffer must be 16-byte aligned");
     return GVX_ERR_INVALID_ARG;
   }
-  if (edt_scratch_words(*dims) > kStaticWorkspaceWords) {
+  if (edt_scratch_words_min(*dims) > kStaticWorkspaceWords) {
     set_error("map too large for the static EDT workspace: needs more than 16,777,216 voxels "
               "(x and y rounded up to multiples of 32); use gvx_dvm_create + gvx_dvm_edt");
     return GVX_ERR_OUT_OF_DOMAIN;
@@ -81,5 +81,5 @@ extern "C" gvx_status gvx_dvm_edt_static_workspace(uint32_t* d_voxels, const gvx
   uint32_t* workspace = nullptr;
   gvx_status st = workspace_address(&workspace);
   if (st != GVX_OK) return st;
-  return cuda_status(launch_edt(d_voxels, workspace, *dims, as_stream(stream)), "EDT (static workspace)");
+  return cuda_status(launch_edt(d_voxels, workspace, kStaticWorkspaceWords, *dims, as_stream(stream)), "EDT (static workspace)");
 }

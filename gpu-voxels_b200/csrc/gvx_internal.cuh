@@ -44,7 +44,8 @@ struct gvx_dvm {
   float side;
   uint32_t* d_vox;
   bool owns;
-  uint32_t* d_scratch;  // EDT workspace (positional proximate-site stacks), owned
+  uint32_t* d_scratch;  // EDT workspace (proximate-site stacks, slice counters), owned
+  uint64_t scratch_words;
 };
 
 struct gvx_bvm {
@@ -103,12 +104,16 @@ cudaError_t launch_dvm_insert(uint32_t* d_vox, gvx_dims d, float side, const flo
                               uint32_t* d_outside, cudaStream_t s);
 cudaError_t launch_bvm_insert(uint8_t* d_vox, gvx_dims d, float side, const float* d_xyz, uint64_t n, uint32_t meaning,
                               uint32_t* d_outside, cudaStream_t s);
-// EDT workspace: the per-item stack area, then Z slice counters, the queue
-// head and the error word of the fused Y -> X launch.
+// EDT workspace: the Z slice counters, queue head and error word of the
+// fused Y -> X launch, then the proximate-site stacks.  edt_scratch_words is
+// the size that lets the fused launch use every resident warp;
+// edt_scratch_words_min the least any launch needs.
 uint64_t edt_scratch_words(gvx_dims d);
-cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, cudaStream_t s);
+uint64_t edt_scratch_words_min(gvx_dims d);
+cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s);
 // pass 0 = Z, 1 = Y, 2 = X (one launch each), 3 = fused Y -> X
-cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, gvx_dims d, int pass, cudaStream_t s);
+cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, int pass,
+                            cudaStream_t s);
 // Synchronous read of the error word the last fused launch left (0 = ok).
 cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag);
 // Resident warps of the fused batch launch (size of the batch stack pool).
