@@ -137,7 +137,7 @@ gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** o
   if (e == cudaSuccess) e = cudaMemcpy(b->d_table, table.data(), n_maps * sizeof(BatchMap), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_prefix, prefix.size() * sizeof(long long));
   if (e == cudaSuccess) e = cudaMemcpy(b->d_prefix, prefix.data(), prefix.size() * sizeof(long long), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_stacks, (size_t)stack_warps * stack_len * 32 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_stacks, (size_t)stack_warps * stack_len * 64 * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_sync, (sync_words + 2) * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(b->d_sync, 0, (sync_words + 2) * sizeof(unsigned));
   if (e != cudaSuccess) {

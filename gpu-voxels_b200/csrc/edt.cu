@@ -44,6 +44,10 @@ __device__ __forceinline__ void cp_async4(uint32_t* smem_dst, const uint32_t* gm
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+  unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
 __device__ __forceinline__ void cp_async16(uint32_t* smem_dst, const uint32_t* gmem_src) {
   unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
@@ -219,7 +223,9 @@ struct SweepCfg {
   static constexpr int kTileWords = kRows * 33;          // one staging tile
   static constexpr int kRing = 16;                       // ring slots per lane
   static constexpr int kWarpWords = 2 * kTileWords + 2 * kRing * 32;
-  static_assert(2 * kRing >= 32, "the phase-3 window (32 entries per lane) aliases the ring");
+  static constexpr int kWin = 16;                        // phase-3 window entries per lane
+  static_assert(kWin * 2 <= 2 * kRing && (kWin & (kWin - 1)) == 0, "the phase-3 window aliases the ring");
+  static_assert(kTileWords % 2 == 0 && kWarpWords % 2 == 0, "8-byte window entries need even offsets");
 };
 
 // Finish the pops of lane `o` with the whole warp.  The stack entries of a
@@ -230,7 +236,7 @@ struct SweepCfg {
 // Lane 31 only supplies the entry below lane 30's, so a round covers 31
 // depths.  All 32 lanes call this; only lane o's state changes.
 template <class Cfg>
-__device__ __forceinline__ void coop_pops(int o, int a0_base, float c0f, uint32_t* ring_base, const uint32_t* gstk_base,
+__device__ __forceinline__ void coop_pops(int o, int a0_base, float c0f, uint32_t* ring_base, const uint2* gstk_base,
                                           int& n, int& lo, const Col& cur, Col& top, float& top_i, Col& sec,
                                           float& sec_i, float& i2) {
   const int lane = threadIdx.x & 31;
@@ -241,7 +247,7 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float c0f, uint32_
   const Col oc = make_col(ce, oa0f, c0f);
   uint32_t* ringE = ring_base + o;
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
-  const uint32_t* gstk = gstk_base + o;
+  const uint2* gstk = gstk_base + o;
   for (int start = on - 1;; start -= 31) {
     const int j = start - lane;
     const int jc = max(j, 0);
@@ -253,9 +259,10 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float c0f, uint32_
       I = ringI[(jc % Cfg::kRing) * 32];
       ec = make_col(e, oa0f, c0f);
     } else {
-      e = gstk[jc * 32];
+      const uint2 p = gstk[jc * 32];
+      e = p.x;
+      I = __uint_as_float(p.y);
       ec = make_col(e, oa0f, c0f);
-      if (jc >= 1) I = bisect(make_col(gstk[(jc - 1) * 32], oa0f, c0f), ec);
     }
     const float b = bisect(ec, oc);
     const bool keep = j <= 0 || I < b;
@@ -323,8 +330,9 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
 }
 
 // One warp item of pass Y (kXPass false) or X: 32 adjacent columns of one
-// z slice; wbase = the warp's kWarpWords of shared memory; stack = the item's
-// L * 32 words of workspace (entry d of lane l at stack[d * 32 + l]).
+// z slice; wbase = the warp's kWarpWords of shared memory; stack = L * 64
+// words of workspace: entry d of lane l is the pair (site, bisector with the
+// entry below) at ((uint2*)stack)[d * 32 + l].
 template <bool kXPass, int kRows>
 __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t* __restrict__ stack, int X, int Y,
                                            int Z, long long item, uint32_t* wbase) {
@@ -345,7 +353,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   uint32_t* tile1 = wbase + Cfg::kTileWords;
   uint32_t* ringE = wbase + 2 * Cfg::kTileWords + lane;  // slot k: ringE[k * 32]
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
-  uint32_t* gstk = stack + lane;  // depth d: gstk[d * 32]
+  uint2* gstk = reinterpret_cast<uint2*>(stack) + lane;  // depth d: gstk[d * 32]
   const float a0f = small_to_float(s.a0_base + lane);  // this lane's column coordinate
   const float c0f = small_to_float(z);
   const int nchunks = (L + kRows - 1) / kRows;
@@ -400,8 +408,9 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
               sec = make_col(ringE[(d % Cfg::kRing) * 32], a0f, c0f);
               sec_i = ringI[(d % Cfg::kRing) * 32];
             } else {  // below the ring: the workspace has the entries
-              sec = make_col(gstk[d * 32], a0f, c0f);
-              sec_i = d >= 1 ? bisect(make_col(gstk[(d - 1) * 32], a0f, c0f), sec) : 0.f;
+              const uint2 p = gstk[d * 32];
+              sec = make_col(p.x, a0f, c0f);
+              sec_i = __uint_as_float(p.y);
             }
           }
           i2 = bisect(top, cur);
@@ -422,7 +431,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
         const int slot = (n % Cfg::kRing) * 32;  // push the current site
         ringE[slot] = cur.e;
         ringI[slot] = i2;
-        gstk[n * 32] = cur.e;
+        gstk[n * 32] = make_uint2(cur.e, __float_as_uint(i2));
         lo = max(lo, n - Cfg::kRing + 1);
         ++n;
         sec = top;
@@ -439,38 +448,43 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   __syncwarp();
 
   // ---- phase 3: rows downward, popping sites that fall behind ----
-  // The stack streams back from the workspace through a 32-entry window per
-  // lane (slot = depth mod 32, in the ring's memory).  At each chunk start
-  // every lane requests the entries down to 32 below its top (cp.async), so
-  // the pops of the next chunk find them on chip; a lane that pops past its
-  // window waits for the request or reads the workspace directly.
-  uint32_t* win = ringE;  // depth d: win[(d & 31) * 32]
-  int k = n - 1;          // index of the current top
-  int flo = n;            // lowest depth requested into the window
-  int safe_lo = n;        // depths >= safe_lo have landed
-  auto request = [&](int new_lo) {
-    for (int d = flo - 1; d >= new_lo; --d) cp_async4(win + (d & 31) * 32, gstk + d * 32);
+  // Each stack entry carries its bisector with the entry below, so a pop is
+  // one read.  The stack streams back from the workspace through a kWin-entry
+  // window per lane (slot = depth mod kWin, in the ring's memory).  At each
+  // chunk start every lane requests the entries down to kWin below its top
+  // (cp.async), so the pops of the next chunk find them on chip; a lane that
+  // pops past its window waits for the request or reads the workspace.
+  constexpr int kWin = Cfg::kWin;
+  uint2* win = reinterpret_cast<uint2*>(wbase + 2 * Cfg::kTileWords) + lane;  // depth d: win[(d % kWin) * 32]
+  int k = n - 1;    // index of the current top
+  int flo = n;      // lowest depth requested into the window
+  int safe_lo = n;  // depths >= safe_lo have landed
+  // Copy depths [new_lo, hi) into the window.  hi never exceeds the lowest
+  // depth already requested nor, after the first request, the top (depths
+  // at or above it are dead), so one request spans at most kWin depths and
+  // no two copies in flight target the same slot.
+  auto request = [&](int hi, int new_lo) {
+    for (int d = hi - 1; d >= new_lo; --d) cp_async8(win + (d & (kWin - 1)) * 32, gstk + d * 32);
     cp_async_commit();
     flo = min(flo, new_lo);
   };
-  auto entry = [&](int d) -> uint32_t {
+  auto entry = [&](int d) -> uint2 {
     if (d < safe_lo) {
       cp_async_wait_all();
       safe_lo = flo;
       if (d < flo) return gstk[d * 32];
     }
-    return win[(d & 31) * 32];
+    return win[(d & (kWin - 1)) * 32];
   };
-  Col prev{0u, 0.f, 0.f};  // entry k-1
+  uint32_t top_e = 0u;
+  float top_b = 0.f;  // bisector of the top with the entry below
   if (n > 0) {
-    request(max(0, n - 32));
+    request(n, max(0, n - kWin));
     cp_async_wait_all();
     safe_lo = flo;
-    top = make_col(entry(k), a0f, c0f);
-    if (k >= 1) {
-      prev = make_col(entry(k - 1), a0f, c0f);
-      top_i = bisect(prev, top);
-    }
+    const uint2 t = entry(k);
+    top_e = t.x;
+    top_b = __uint_as_float(t.y);
   }
   uint32_t* stage = tile0;
   for (int c = nchunks - 1; c >= 0; --c) {
@@ -478,20 +492,18 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     const int rows = min(kRows, L - r0);
     cp_async_wait_all();  // the previous chunk's request
     safe_lo = flo;
-    if (k >= 1) request(max(0, k - 32));
+    if (k >= 1) request(min(flo, k), max(0, k - kWin));
     float tyf = small_to_float(r0 + rows - 1);
     for (int r = rows - 1; r >= 0; --r, tyf -= 1.0f) {
-      while (k >= 1 && tyf <= top_i) {  // pop
+      while (k >= 1 && tyf <= top_b) {  // pop
         --k;
-        top = prev;
-        if (k >= 1) {
-          prev = make_col(entry(k - 1), a0f, c0f);
-          top_i = bisect(prev, top);
-        }
+        const uint2 t = entry(k);
+        top_e = t.x;
+        top_b = __uint_as_float(t.y);
       }
       uint32_t out = kDvUninit;
       if (n > 0) {
-        const uint32_t a = top.e & 0x3ffu, row = (top.e >> 10) & 0x3ffu, cc = top.e >> 20;
+        const uint32_t a = top_e & 0x3ffu, row = (top_e >> 10) & 0x3ffu, cc = top_e >> 20;
         out = kXPass ? dv_pack(row, a, cc) : dv_pack(a, row, cc);
       }
       stage[r * tpitch + lane] = out;
@@ -543,18 +555,24 @@ __global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z_batch(const BatchM
   }
 }
 
-// One pass (Y or X) on its own, one warp per item (per-pass timing and the
-// fallback of the fused schedule below for maps too small for its stacks).
+// Words of stack one warp needs for a map (a pair per row per lane).
+__host__ __device__ __forceinline__ uint64_t warp_stack_words(int X, int Y) { return (uint64_t)max(X, Y) * 64; }
+
+// One pass (Y or X) on its own (per-pass timing and the fallback of the fused
+// schedule below): persistent warps stride over the items, one stack each.
 template <bool kXPass, int kRows>
 __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
-    edt_sweep(uint32_t* __restrict__ map, uint32_t* __restrict__ scratch, int X, int Y, int Z) {
+    edt_sweep(uint32_t* __restrict__ map, uint32_t* __restrict__ stacks, int X, int Y, int Z) {
   using Cfg = SweepCfg<kRows>;
   extern __shared__ __align__(16) uint32_t s_sweep[];  // [kWarps][kWarpWords]
   const int warp = threadIdx.x >> 5;
-  const long long item = (long long)blockIdx.x * Cfg::kWarps + warp;
-  if (item >= (long long)(((kXPass ? Y : X) + 31) >> 5) * Z) return;
-  const int L = kXPass ? X : Y;
-  sweep_item<kXPass, kRows>(map, scratch + (uint64_t)item * L * 32, X, Y, Z, item, s_sweep + (size_t)warp * Cfg::kWarpWords);
+  const long long gw = (long long)blockIdx.x * Cfg::kWarps + warp;
+  uint32_t* stack = stacks + (uint64_t)gw * warp_stack_words(X, Y);
+  const long long items = (long long)(((kXPass ? Y : X) + 31) >> 5) * Z;
+  for (long long item = gw; item < items; item += (long long)gridDim.x * Cfg::kWarps) {
+    sweep_item<kXPass, kRows>(map, stack, X, Y, Z, item, s_sweep + (size_t)warp * Cfg::kWarpWords);
+    __syncwarp();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -623,7 +641,7 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
   extern __shared__ __align__(16) uint32_t s_sweep[];
   const int warp = threadIdx.x >> 5;
   uint32_t* wbase = s_sweep + (size_t)warp * Cfg::kWarpWords;
-  uint32_t* stack = stacks + ((uint64_t)blockIdx.x * Cfg::kWarps + warp) * (uint64_t)max(X, Y) * 32;
+  uint32_t* stack = stacks + ((uint64_t)blockIdx.x * Cfg::kWarps + warp) * warp_stack_words(X, Y);
   unsigned* done = sync;
   unsigned* head = sync + Z;
   unsigned* err = head + 1;
@@ -654,7 +672,7 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
   extern __shared__ __align__(16) uint32_t s_sweep[];
   const int warp = threadIdx.x >> 5;
   uint32_t* wbase = s_sweep + (size_t)warp * Cfg::kWarpWords;
-  uint32_t* stack = stacks + ((uint64_t)blockIdx.x * Cfg::kWarps + warp) * (uint64_t)stack_len * 32;
+  uint32_t* stack = stacks + ((uint64_t)blockIdx.x * Cfg::kWarps + warp) * (uint64_t)stack_len * 64;
   unsigned* head = sync + sync_words;
   unsigned* err = head + 1;
   const unsigned nall = total_y + total_x;
@@ -733,29 +751,30 @@ cudaError_t launch_pass_z(uint32_t* map, gvx_dims d, cudaStream_t s) {
 }
 
 // Workspace layout: [slice counters, queue head, error word: sync_words(d)]
-// [stack area].  The per-pass launches index the stack area per item; the
-// fused launch uses it as one stack per resident warp.
+// [stack area: one stack of warp_stack_words per launched warp].
 uint64_t sync_words(gvx_dims d) { return ((uint64_t)d.z + 2 + 31) / 32 * 32; }
 
+// Blocks for a persistent sweep launch: resident, fitting the stack area, and
+// no more than the items need (0 when the area holds no block's stacks).
+long long sweep_blocks(long long resident, uint64_t stack_area, gvx_dims d, int warps, long long items) {
+  const uint64_t per_block = (uint64_t)warps * warp_stack_words((int)d.x, (int)d.y);
+  return std::min<long long>({resident, (long long)(stack_area / per_block), (items + warps - 1) / warps});
+}
+
 template <bool kXPass, int kRows>
-cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStream_t s) {
+cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s) {
   using Cfg = SweepCfg<kRows>;
   const long long cols = kXPass ? d.y : d.x;
   const long long items = ((cols + 31) / 32) * d.z;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
-  auto kern = edt_sweep<kXPass, kRows>;
-  cudaError_t e = kernel_setup<edt_sweep<kXPass, kRows>>(Cfg::kWarps * 32, smem, nullptr);
+  long long blocks = 0;
+  cudaError_t e = kernel_setup<edt_sweep<kXPass, kRows>>(Cfg::kWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
-  kern<<<(unsigned)((items + Cfg::kWarps - 1) / Cfg::kWarps), Cfg::kWarps * 32, smem, s>>>(
-      map, scratch + sync_words(d), (int)d.x, (int)d.y, (int)d.z);
+  blocks = sweep_blocks(blocks, scratch_words - sync_words(d), d, Cfg::kWarps, items);
+  if (blocks < 1) return cudaErrorInvalidValue;
+  edt_sweep<kXPass, kRows><<<(unsigned)blocks, Cfg::kWarps * 32, smem, s>>>(map, scratch + sync_words(d), (int)d.x,
+                                                                             (int)d.y, (int)d.z);
   return cudaGetLastError();
-}
-
-// Per-item stack area of the per-pass launches.
-uint64_t stack_words(gvx_dims d) {
-  const uint64_t y_pass = (uint64_t)((d.x + 31) / 32) * 32 * d.y * d.z;
-  const uint64_t x_pass = (uint64_t)((d.y + 31) / 32) * 32 * d.x * d.z;
-  return std::max(y_pass, x_pass);
 }
 
 // Stack area that lets the fused launch run one warp per item, up to
@@ -764,33 +783,26 @@ constexpr uint64_t kFusedWarpCap = 4096;
 uint64_t fused_stack_words(gvx_dims d) {
   const uint64_t items = (uint64_t)((d.x + 31) / 32) * d.z + (uint64_t)((d.y + 31) / 32) * d.z;
   const uint64_t warps = std::min<uint64_t>((items + 7) / 8 * 8, kFusedWarpCap);
-  return warps * std::max(d.x, d.y) * 32;
+  return warps * warp_stack_words((int)d.x, (int)d.y);
 }
 
 // Fused Y -> X launch for one map: as many blocks as are resident, as the
-// stack area holds and as there are items.  A workspace whose stack area
-// cannot hold one block's stacks runs the two passes as separate launches.
+// stack area holds and as there are items.
 template <int kRows>
 cudaError_t launch_sweep_yx(uint32_t* map, uint32_t* scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s) {
   using Cfg = SweepCfg<kRows>;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
-  auto kern = edt_sweep_yx<kRows>;
   long long blocks = 0;
   cudaError_t e = kernel_setup<edt_sweep_yx<kRows>>(Cfg::kWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
-  const uint64_t sw = scratch_words - sync_words(d);
-  const uint64_t per_block = (uint64_t)Cfg::kWarps * std::max(d.x, d.y) * 32;
   const long long items = (long long)((d.x + 31) / 32) * d.z + (long long)((d.y + 31) / 32) * d.z;
-  blocks = std::min<long long>({blocks, (long long)(sw / per_block), (items + Cfg::kWarps - 1) / Cfg::kWarps});
-  if (blocks < 1) {
-    e = launch_sweep<false, kRows>(map, scratch, d, s);
-    return e == cudaSuccess ? launch_sweep<true, kRows>(map, scratch, d, s) : e;
-  }
+  blocks = sweep_blocks(blocks, scratch_words - sync_words(d), d, Cfg::kWarps, items);
+  if (blocks < 1) return cudaErrorInvalidValue;
   unsigned* sync = scratch;
   e = cudaMemsetAsync(sync, 0, (d.z + 2) * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  kern<<<(unsigned)blocks, Cfg::kWarps * 32, smem, s>>>(map, scratch + sync_words(d), sync, (int)d.x, (int)d.y,
-                                                        (int)d.z);
+  edt_sweep_yx<kRows><<<(unsigned)blocks, Cfg::kWarps * 32, smem, s>>>(map, scratch + sync_words(d), sync, (int)d.x,
+                                                                       (int)d.y, (int)d.z);
   return cudaGetLastError();
 }
 
@@ -838,8 +850,12 @@ long long batch_stack_warps() {
 
 void set_edt_sweep_rows(int rows) { g_sweep_rows = rows == 32 ? 32 : 16; }
 
-uint64_t edt_scratch_words_min(gvx_dims d) { return sync_words(d) + stack_words(d); }
-uint64_t edt_scratch_words(gvx_dims d) { return sync_words(d) + std::max(stack_words(d), fused_stack_words(d)); }
+uint64_t edt_scratch_words_min(gvx_dims d) {
+  return sync_words(d) + (uint64_t)SweepCfg<32>::kWarps * warp_stack_words((int)d.x, (int)d.y);
+}
+uint64_t edt_scratch_words(gvx_dims d) {
+  return std::max(sync_words(d) + fused_stack_words(d), edt_scratch_words_min(d));
+}
 
 cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, int pass,
                             cudaStream_t s) {
@@ -847,8 +863,12 @@ cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scrat
   const bool big = sweep_rows() == 32;
   switch (pass) {
     case 0: return launch_pass_z(d_vox, d, s);
-    case 1: return big ? launch_sweep<false, 32>(d_vox, d_scratch, d, s) : launch_sweep<false, 16>(d_vox, d_scratch, d, s);
-    case 2: return big ? launch_sweep<true, 32>(d_vox, d_scratch, d, s) : launch_sweep<true, 16>(d_vox, d_scratch, d, s);
+    case 1:
+      return big ? launch_sweep<false, 32>(d_vox, d_scratch, scratch_words, d, s)
+                 : launch_sweep<false, 16>(d_vox, d_scratch, scratch_words, d, s);
+    case 2:
+      return big ? launch_sweep<true, 32>(d_vox, d_scratch, scratch_words, d, s)
+                 : launch_sweep<true, 16>(d_vox, d_scratch, scratch_words, d, s);
     case 3:
       return big ? launch_sweep_yx<32>(d_vox, d_scratch, scratch_words, d, s)
                  : launch_sweep_yx<16>(d_vox, d_scratch, scratch_words, d, s);

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "gvx_internal.cuh"
@@ -27,6 +28,7 @@ namespace gvx {
 namespace {
 
 constexpr uint64_t kStaticWorkspaceWords = 16ull * 1024 * 1024 + 2048;  // 64 MiB + 8 KiB
+constexpr uint64_t kStaticStackVoxels = 16ull * 1024 * 1024;               // the size limit callers see
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) uint32_t g_edt_workspace[kStaticWorkspaceWords];
@@ -73,7 +75,9 @@ extern "C" gvx_status gvx_dvm_edt_static_workspace(uint32_t* d_voxels, const gvx
     set_error("voxel buffer must be 16-byte aligned");
     return GVX_ERR_INVALID_ARG;
   }
-  if (edt_scratch_words_min(*dims) > kStaticWorkspaceWords) {
+  const uint64_t x32 = (dims->x + 31) / 32 * 32, y32 = (dims->y + 31) / 32 * 32;
+  const uint64_t padded = std::max(x32 * dims->y, (uint64_t)dims->x * y32) * dims->z;
+  if (padded > kStaticStackVoxels || edt_scratch_words_min(*dims) > kStaticWorkspaceWords) {
     set_error("map too large for the static EDT workspace: needs more than 16,777,216 voxels "
               "(x and y rounded up to multiples of 32); use gvx_dvm_create + gvx_dvm_edt");
     return GVX_ERR_OUT_OF_DOMAIN;

@@ -77,8 +77,8 @@ struct BatchMap {
 
 // Work-item layout of the batched EDT: for pass p, map k owns warp items
 // [prefix[p][k], prefix[p][k+1]).  The fused Y -> X launch keeps one stack of
-// stack_len rows per resident warp in d_stacks and its slice counters, queue
-// head and error word in d_sync (sync_words + 2 words).
+// stack_len rows (64 words each) per resident warp in d_stacks and its slice
+// counters, queue head and error word in d_sync (sync_words + 2 words).
 struct BatchItems {
   long long* d_prefix[3];
   long long total[3];
