@@ -172,24 +172,29 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
 // passes Y and X
 // ---------------------------------------------------------------------------
 
-// Exact small-integer -> float conversions on the FMA/ALU pipes (the
+// Exact small-integer -> float conversions on the ALU/FMA pipes (the
 // converter sits on the narrow XU pipe, which the reciprocal also needs):
-// for 0 <= v < 2^22 the bit pattern 0x4B400000 + v is the float 2^23 + 2^22 + v.
-__device__ __forceinline__ float small_to_float(int v) { return __int_as_float(0x4B400000 + v) - 12582912.0f; }
+// for 0 <= v < 2^22 the bit pattern 0x4B400000 | v is the float
+// kBias + v with kBias = 2^23 + 2^22, and a difference of two such floats is
+// exact.  A column coordinate is kept biased (kBias + a0, exact below 2^24).
+constexpr float kBias = 12582912.0f;
+__device__ __forceinline__ float biased(uint32_t v) { return __uint_as_float(0x4B400000u | v); }
+__device__ __forceinline__ float small_to_float(int v) { return biased((uint32_t)v) - kBias; }
 
-// A site in the column frame: packed entry (a | row << 10 | c << 20) plus its
-// row and squared offset from the column as exact floats (offset < 2^21).
+// A site in the column frame: packed entry (a | row << 10 | c << 20) plus
+// twice its row and its squared offset from the column as exact floats
+// (offset < 2^21).  A0, C0: the column's coordinates, biased.
 struct Col {
   uint32_t e;
-  float r, d;
+  float r2, d;
 };
 
-__device__ __forceinline__ Col make_col(uint32_t e, float a0f, float c0f) {
+__device__ __forceinline__ Col make_col(uint32_t e, float A0, float C0) {
   Col s;
   s.e = e;
-  s.r = small_to_float((int)((e >> 10) & 0x3ffu));
-  const float da = small_to_float((int)(e & 0x3ffu)) - a0f;
-  const float dc = small_to_float((int)(e >> 20)) - c0f;
+  s.r2 = biased((e >> 9) & 0x7feu) - kBias;  // 2 * row
+  const float da = biased(e & 0x3ffu) - A0;
+  const float dc = biased(e >> 20) - C0;
   s.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));  // exact: integers below 2^21
   return s;
 }
@@ -199,13 +204,12 @@ __device__ __forceinline__ Col make_col(uint32_t e, float a0f, float c0f) {
 // For integer coordinates below 1024 its numerator is exact in float and
 // equals (d2 - d1) / 2, d = squared offset of a site from the column, so the
 // value is fl(0.5*(r1 + r2) + fl((d2 - d1) / (2*(r2 - r1)))) with every operand
-// exact: bit for bit the reference's float.  Equal offsets give exactly the
-// midpoint; the divide is skipped when no lane of the warp needs it.
+// exact: bit for bit the reference's float.  With r2 = 2 * row the divisor is
+// r2' - r2 (never 0: stacked sites have distinct rows) and the midpoint
+// 0.25 * (r2 + r2'), both exact.
 __device__ __forceinline__ float bisect(const Col& s1, const Col& s2) {
-  const float num = __fsub_rn(s2.d, s1.d);
-  float q = 0.0f;
-  if (__any_sync(__activemask(), num != 0.0f)) q = __fdiv_rn(num, __fmul_rn(__fsub_rn(s2.r, s1.r), 2.0f));
-  return __fadd_rn(__fmul_rn(__fadd_rn(s1.r, s2.r), 0.5f), q);
+  const float q = __fdiv_rn(__fsub_rn(s2.d, s1.d), __fsub_rn(s2.r2, s1.r2));
+  return __fadd_rn(__fmul_rn(__fadd_rn(s1.r2, s2.r2), 0.25f), q);
 }
 
 // Geometry of one warp's work item.
@@ -222,10 +226,18 @@ struct SweepCfg {
   static constexpr int kWarps = 8;                       // warps per CTA
   static constexpr int kTileWords = kRows * 33;          // one staging tile
   static constexpr int kRing = 16;                       // ring slots per lane
-  static constexpr int kWarpWords = 2 * kTileWords + 2 * kRing * 32;
-  static constexpr int kWin = 16;                        // phase-3 window entries per lane
-  static_assert(kWin * 2 <= 2 * kRing && (kWin & (kWin - 1)) == 0, "the phase-3 window aliases the ring");
-  static_assert(kTileWords % 2 == 0 && kWarpWords % 2 == 0, "8-byte window entries need even offsets");
+  static constexpr int kPhase2Words = 2 * kTileWords + 2 * kRing * 32;
+  // Phase 3: pass X stages kStageRows output rows (pitch 36) before its
+  // transposed flush; pass Y stores rows directly.  The stack window (kWin
+  // (site, bisector) pairs per lane) follows the staging rows.
+  static constexpr int kStageRows = 8;
+  static constexpr int kStagePitch = 36;
+  static constexpr int kStageWords = kStageRows * kStagePitch;
+  static constexpr int kWin = 32;
+  static constexpr int kPhase3Words = kStageWords + kWin * 64;
+  static constexpr int kWarpWords = kPhase2Words > kPhase3Words ? kPhase2Words : kPhase3Words;
+  static_assert((kWin & (kWin - 1)) == 0, "window slots are depth mod kWin");
+  static_assert(kStageWords % 2 == 0 && kWarpWords % 2 == 0, "8-byte window entries need even offsets");
 };
 
 // Finish the pops of lane `o` with the whole warp.  The stack entries of a
@@ -236,15 +248,15 @@ struct SweepCfg {
 // Lane 31 only supplies the entry below lane 30's, so a round covers 31
 // depths.  All 32 lanes call this; only lane o's state changes.
 template <class Cfg>
-__device__ __forceinline__ void coop_pops(int o, int a0_base, float c0f, uint32_t* ring_base, const uint2* gstk_base,
+__device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t* ring_base, const uint2* gstk_base,
                                           int& n, int& lo, const Col& cur, Col& top, float& top_i, Col& sec,
                                           float& sec_i, float& i2) {
   const int lane = threadIdx.x & 31;
   const int on = __shfl_sync(kFullMask, n, o);
   const int olo = __shfl_sync(kFullMask, lo, o);
   const uint32_t ce = __shfl_sync(kFullMask, cur.e, o);
-  const float oa0f = small_to_float(a0_base + o);
-  const Col oc = make_col(ce, oa0f, c0f);
+  const float oA0 = biased((uint32_t)(a0_base + o));
+  const Col oc = make_col(ce, oA0, C0);
   uint32_t* ringE = ring_base + o;
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
   const uint2* gstk = gstk_base + o;
@@ -257,12 +269,12 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float c0f, uint32_
     if (jc >= olo) {
       e = ringE[(jc % Cfg::kRing) * 32];
       I = ringI[(jc % Cfg::kRing) * 32];
-      ec = make_col(e, oa0f, c0f);
+      ec = make_col(e, oA0, C0);
     } else {
       const uint2 p = gstk[jc * 32];
       e = p.x;
       I = __uint_as_float(p.y);
-      ec = make_col(e, oa0f, c0f);
+      ec = make_col(e, oA0, C0);
     }
     const float b = bisect(ec, oc);
     const bool keep = j <= 0 || I < b;
@@ -286,10 +298,10 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float c0f, uint32_
       if (lane == o) {
         n = start - t + 1;
         lo = min(lo, new_lo);
-        top = make_col(e_top, oa0f, c0f);
+        top = make_col(e_top, oA0, C0);
         top_i = i_top;
         i2 = b_top;
-        sec = make_col(e_sec, oa0f, c0f);
+        sec = make_col(e_sec, oA0, C0);
         sec_i = i_sec;
       }
       __syncwarp();  // the refill before lane o's next ring access
@@ -354,8 +366,8 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   uint32_t* ringE = wbase + 2 * Cfg::kTileWords + lane;  // slot k: ringE[k * 32]
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
   uint2* gstk = reinterpret_cast<uint2*>(stack) + lane;  // depth d: gstk[d * 32]
-  const float a0f = small_to_float(s.a0_base + lane);  // this lane's column coordinate
-  const float c0f = small_to_float(z);
+  const float A0 = biased((uint32_t)(s.a0_base + lane));  // this lane's column coordinate, biased
+  const float C0 = biased((uint32_t)z);
   const int nchunks = (L + kRows - 1) / kRows;
   const int tpitch = kXPass ? 33 : 32;
   // Pops a lane runs alone per row before the warp takes over.  Pass Y (input:
@@ -384,7 +396,8 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     const uint32_t* tile = (c & 1) ? tile1 : tile0;
     const int r0 = c * kRows;
     const int rows = min(kRows, L - r0);
-    for (int r = 0; r < rows; ++r) {
+    float row2f = small_to_float(2 * r0);  // 2 * row, exact
+    for (int r = 0; r < rows; ++r, row2f += 2.0f) {
       const uint32_t v = tile[r * tpitch + lane];
       const uint32_t a = kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
       const bool has = a != kUninit;
@@ -392,7 +405,11 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
       float i2 = 0.f;
       bool deep = false;
       if (has) {
-        cur = make_col(a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u), a0f, c0f);
+        cur.e = a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u);
+        cur.r2 = row2f;
+        const float da = biased(a) - A0;
+        const float dc = biased(v >> 20) - C0;
+        cur.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));
         if (n >= 1) i2 = bisect(top, cur);
         for (int p = 0; n >= 2 && !(top_i < i2); ++p) {  // top is dominated by (second, current): pop
           if (kSoloPops > 0 && p == kSoloPops) {
@@ -405,11 +422,11 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           if (n >= 2) {
             const int d = n - 2;
             if (d >= lo) {
-              sec = make_col(ringE[(d % Cfg::kRing) * 32], a0f, c0f);
+              sec = make_col(ringE[(d % Cfg::kRing) * 32], A0, C0);
               sec_i = ringI[(d % Cfg::kRing) * 32];
             } else {  // below the ring: the workspace has the entries
               const uint2 p = gstk[d * 32];
-              sec = make_col(p.x, a0f, c0f);
+              sec = make_col(p.x, A0, C0);
               sec_i = __uint_as_float(p.y);
             }
           }
@@ -423,7 +440,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
         while (deep_lanes) {
           const int o = __ffs(deep_lanes) - 1;
           deep_lanes &= deep_lanes - 1;
-          coop_pops<Cfg>(o, s.a0_base, c0f, wbase + 2 * Cfg::kTileWords, gstk - lane, n, lo, cur, top, top_i, sec,
+          coop_pops<Cfg>(o, s.a0_base, C0, wbase + 2 * Cfg::kTileWords, gstk - lane, n, lo, cur, top, top_i, sec,
                          sec_i, i2);
         }
       }
@@ -450,19 +467,22 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   // ---- phase 3: rows downward, popping sites that fall behind ----
   // Each stack entry carries its bisector with the entry below, so a pop is
   // one read.  The stack streams back from the workspace through a kWin-entry
-  // window per lane (slot = depth mod kWin, in the ring's memory).  At each
-  // chunk start every lane requests the entries down to kWin below its top
-  // (cp.async), so the pops of the next chunk find them on chip; a lane that
-  // pops past its window waits for the request or reads the workspace.
+  // window per lane (slot = depth mod kWin).  At each chunk start every lane
+  // requests the entries down to kWin below its top (cp.async), so the pops
+  // of the following chunks find them on chip; a lane that pops past what
+  // has landed waits for its request or reads the workspace directly.
   constexpr int kWin = Cfg::kWin;
-  uint2* win = reinterpret_cast<uint2*>(wbase + 2 * Cfg::kTileWords) + lane;  // depth d: win[(d % kWin) * 32]
+  constexpr int kP3Rows = kXPass ? Cfg::kStageRows : kRows;
+  uint32_t* xstage = wbase;  // pass X: kStageRows x kStagePitch
+  uint2* win = reinterpret_cast<uint2*>(wbase + (kXPass ? Cfg::kStageWords : 0)) + lane;  // depth d: win[(d % kWin) * 32]
   int k = n - 1;    // index of the current top
   int flo = n;      // lowest depth requested into the window
   int safe_lo = n;  // depths >= safe_lo have landed
   // Copy depths [new_lo, hi) into the window.  hi never exceeds the lowest
   // depth already requested nor, after the first request, the top (depths
-  // at or above it are dead), so one request spans at most kWin depths and
-  // no two copies in flight target the same slot.
+  // at or above it are dead); requests are waited for before the next one,
+  // so one request spans at most kWin depths and no two copies in flight
+  // target the same slot.
   auto request = [&](int hi, int new_lo) {
     for (int d = hi - 1; d >= new_lo; --d) cp_async8(win + (d & (kWin - 1)) * 32, gstk + d * 32);
     cp_async_commit();
@@ -476,20 +496,26 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     }
     return win[(d & (kWin - 1)) * 32];
   };
-  uint32_t top_e = 0u;
+  // The voxel value a top entry gives, in map order (pass X swaps the
+  // entry's first two fields back).
+  auto out_of = [](uint32_t te) -> uint32_t {
+    return kXPass ? (((te >> 10) & 0x3ffu) | ((te & 0x3ffu) << 10) | (te & 0xFFF00000u)) : te;
+  };
+  uint32_t out = kDvUninit;
   float top_b = 0.f;  // bisector of the top with the entry below
   if (n > 0) {
     request(n, max(0, n - kWin));
     cp_async_wait_all();
     safe_lo = flo;
     const uint2 t = entry(k);
-    top_e = t.x;
+    out = out_of(t.x);
     top_b = __uint_as_float(t.y);
   }
-  uint32_t* stage = tile0;
-  for (int c = nchunks - 1; c >= 0; --c) {
-    const int r0 = c * kRows;
-    const int rows = min(kRows, L - r0);
+  uint32_t* col_out = s.slice + s.a0_base + lane;  // pass Y: this lane's column, row stride X
+  const bool live = lane < s.valid;
+  for (int c = (L + kP3Rows - 1) / kP3Rows - 1; c >= 0; --c) {
+    const int r0 = c * kP3Rows;
+    const int rows = min(kP3Rows, L - r0);
     cp_async_wait_all();  // the previous chunk's request
     safe_lo = flo;
     if (k >= 1) request(min(flo, k), max(0, k - kWin));
@@ -498,26 +524,20 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
       while (k >= 1 && tyf <= top_b) {  // pop
         --k;
         const uint2 t = entry(k);
-        top_e = t.x;
+        out = out_of(t.x);
         top_b = __uint_as_float(t.y);
       }
-      uint32_t out = kDvUninit;
-      if (n > 0) {
-        const uint32_t a = top_e & 0x3ffu, row = (top_e >> 10) & 0x3ffu, cc = top_e >> 20;
-        out = kXPass ? dv_pack(row, a, cc) : dv_pack(a, row, cc);
-      }
-      stage[r * tpitch + lane] = out;
+      if (kXPass) xstage[r * Cfg::kStagePitch + lane] = out;
+      else if (live) col_out[(uint64_t)(r0 + r) * X] = out;
     }
-    __syncwarp();
-    if (!kXPass) {
-      if (lane < s.valid)
-        for (int rr = 0; rr < rows; ++rr) s.slice[(uint64_t)(r0 + rr) * X + s.a0_base + lane] = stage[rr * 32 + lane];
-    } else {
-      const int xl = lane % kRows, t0 = lane / kRows;
+    if (kXPass) {  // transposed flush: 4 rows of the map x 8 consecutive x per store
+      __syncwarp();
+      const int xl = lane >> 2, t0 = lane & 3;
       if (xl < rows)
-        for (int t = t0; t < s.valid; t += 32 / kRows) s.slice[(uint64_t)(s.a0_base + t) * X + r0 + xl] = stage[xl * 33 + t];
+        for (int t = t0; t < s.valid; t += 4)
+          s.slice[(uint64_t)(s.a0_base + t) * X + r0 + xl] = xstage[xl * Cfg::kStagePitch + t];
+      __syncwarp();
     }
-    __syncwarp();
   }
   cp_async_wait_all();
 }
