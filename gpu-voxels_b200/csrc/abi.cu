@@ -93,7 +93,7 @@ gvx_status gvx_dvm_create(const gvx_dims* dims, float voxel_side, gvx_dvm** out)
   gvx_status st = check_dims(dims);
   if (st != GVX_OK) return st;
   if (!(voxel_side > 0.0f)) return fail(GVX_ERR_INVALID_ARG, "voxel side must be > 0");
-  gvx_dvm* m = new (std::nothrow) gvx_dvm{*dims, voxel_side, nullptr, true, nullptr, edt_scratch_words(*dims)};
+  gvx_dvm* m = new (std::nothrow) gvx_dvm{*dims, voxel_side, nullptr, true, nullptr, edt_scratch_words(*dims), 0, 1};
   if (m == nullptr) return fail(GVX_ERR_OOM, "host allocation failed");
   const uint64_t n = num_voxels(*dims);
   cudaError_t e = cudaMalloc(&m->d_vox, n * sizeof(uint32_t) + 16);
@@ -122,7 +122,7 @@ gvx_status gvx_dvm_wrap(const gvx_dims* dims, float voxel_side, uint32_t* d_voxe
   if (st != GVX_OK) return st;
   if (!(voxel_side > 0.0f)) return fail(GVX_ERR_INVALID_ARG, "voxel side must be > 0");
   if (reinterpret_cast<uintptr_t>(d_voxels) % 16 != 0) return fail(GVX_ERR_INVALID_ARG, "voxel buffer must be 16-byte aligned");
-  gvx_dvm* m = new (std::nothrow) gvx_dvm{*dims, voxel_side, d_voxels, false, nullptr, edt_scratch_words(*dims)};
+  gvx_dvm* m = new (std::nothrow) gvx_dvm{*dims, voxel_side, d_voxels, false, nullptr, edt_scratch_words(*dims), 0, 1};
   if (m == nullptr) return fail(GVX_ERR_OOM, "host allocation failed");
   cudaError_t e = cudaMalloc(&m->d_scratch, m->scratch_words * sizeof(uint32_t));
   if (e != cudaSuccess) {
@@ -167,12 +167,12 @@ gvx_status gvx_dvm_insert_points(gvx_dvm* m, const float* d_xyz, uint64_t n, uin
 gvx_status gvx_dvm_edt(gvx_dvm* m, uint32_t m1, uint32_t m2, uint32_t m3, gvx_stream stream) {
   (void)m1; (void)m2; (void)m3;
   if (m == nullptr) return fail(GVX_ERR_INVALID_ARG, "map is null");
-  return cuda_status(launch_edt(m->d_vox, m->d_scratch, m->scratch_words, m->dims, as_stream(stream)), "parallelBanding3D");
+  return cuda_status(launch_edt(m->d_vox, m->d_scratch, m->scratch_words, m->dims, as_stream(stream), EdtConfig{m->edt_rows, m->edt_fused}), "parallelBanding3D");
 }
 
 gvx_status gvx_dvm_edt_pass(gvx_dvm* m, int pass, gvx_stream stream) {
   if (m == nullptr || pass < 0 || pass > 3) return fail(GVX_ERR_INVALID_ARG, "map is null or pass not in {0,1,2,3}");
-  return cuda_status(launch_edt_pass(m->d_vox, m->d_scratch, m->scratch_words, m->dims, pass, as_stream(stream)), "EDT pass");
+  return cuda_status(launch_edt_pass(m->d_vox, m->d_scratch, m->scratch_words, m->dims, pass, as_stream(stream), m->edt_rows), "EDT pass");
 }
 
 gvx_status gvx_dvm_edt_check(gvx_dvm* m, uint32_t* flags) {

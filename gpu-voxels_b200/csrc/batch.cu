@@ -102,6 +102,7 @@ struct gvx_batch {
   unsigned* d_sync = nullptr;     // slice counters of all maps, queue head, error word
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  int edt_rows = 0;  // sweep rows per staging chunk (0 = library default), set by the autotuner
 };
 
 using namespace gvx;
@@ -189,7 +190,7 @@ gvx_status gvx_batch_insert_points(gvx_batch* b, const float* d_xyz, const uint6
 
 gvx_status gvx_batch_edt(gvx_batch* b, gvx_stream stream) {
   if (b == nullptr) return fail(GVX_ERR_INVALID_ARG, "batch is null");
-  return cuda_status(launch_edt_batch(b->d_table, b->items, as_stream(stream)), "batch EDT");
+  return cuda_status(launch_edt_batch(b->d_table, b->items, as_stream(stream), b->edt_rows), "batch EDT");
 }
 
 gvx_status gvx_batch_edt_check(gvx_batch* b, uint32_t* flags) {
@@ -198,6 +199,72 @@ gvx_status gvx_batch_edt_check(gvx_batch* b, uint32_t* flags) {
   if (e == cudaSuccess) e = cudaMemcpy(flags, b->d_sync + b->items.sync_words + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_status(e, "batch EDT check");
   if (*flags != 0) return fail(GVX_ERR_TIMEOUT, "batched EDT: a slice wait gave up (results invalid)");
+  return GVX_OK;
+}
+
+gvx_status gvx_batch_autotune(gvx_batch* b, int force, gvx_edt_config* out, gvx_stream stream) {
+  if (b == nullptr) return fail(GVX_ERR_INVALID_ARG, "batch is null");
+  std::string key = tune_device_name() + "|batch|" + std::to_string(b->maps.size());
+  uint64_t h = 1469598103934665603ull;  // FNV-1a over the dims of all maps
+  for (const gvx_dvm* m : b->maps)
+    for (uint32_t v : {m->dims.x, m->dims.y, m->dims.z}) h = (h ^ v) * 1099511628211ull;
+  key += "|" + std::to_string(h);
+  EdtConfig best;
+  float best_ms = 0.f;
+  if (force || !tune_lookup(key, &best, &best_ms)) {
+    cudaStream_t s = as_stream(stream);
+    uint64_t total = 0;
+    for (const gvx_dvm* m : b->maps) total += num_voxels(m->dims);
+    uint32_t* save = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&save, total * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    auto copy_all = [&](bool to_save) {
+      uint64_t off = 0;
+      cudaError_t r = cudaSuccess;
+      for (const gvx_dvm* m : b->maps) {
+        const uint64_t n = num_voxels(m->dims);
+        if (r == cudaSuccess)
+          r = cudaMemcpyAsync(to_save ? save + off : m->d_vox, to_save ? m->d_vox : save + off, n * sizeof(uint32_t),
+                              cudaMemcpyDeviceToDevice, s);
+        off += n;
+      }
+      return r;
+    };
+    if (e == cudaSuccess) e = copy_all(true);
+    best_ms = 1e30f;
+    for (int rows : {16, 32}) {
+      float t_min = 1e30f;
+      for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {  // first run warms up
+        e = copy_all(false);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+        if (e == cudaSuccess) e = launch_edt_batch(b->d_table, b->items, s, rows);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess && rep > 0) t_min = std::min(t_min, ms);
+      }
+      if (e == cudaSuccess && t_min < best_ms) {
+        best_ms = t_min;
+        best = EdtConfig{rows, 1};
+      }
+    }
+    if (e == cudaSuccess) e = copy_all(false);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (save) cudaFree(save);
+    if (e != cudaSuccess) return cuda_status(e, "batch autotune");
+    uint32_t flag = 0;
+    e = cudaMemcpy(&flag, b->d_sync + b->items.sync_words + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "batch autotune");
+    if (flag) return fail(GVX_ERR_TIMEOUT, "batch autotune: a bounded wait gave up");
+    tune_store(key, best, best_ms);
+  }
+  b->edt_rows = best.rows;
+  if (out) *out = gvx_edt_config{(uint32_t)best.rows, 1u, best_ms};
   return GVX_OK;
 }
 

@@ -878,9 +878,9 @@ uint64_t edt_scratch_words(gvx_dims d) {
 }
 
 cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, int pass,
-                            cudaStream_t s) {
+                            cudaStream_t s, int rows) {
   if (pass != 0 && scratch_words < edt_scratch_words_min(d)) return cudaErrorInvalidValue;
-  const bool big = sweep_rows() == 32;
+  const bool big = (rows == 0 ? sweep_rows() : rows) == 32;
   switch (pass) {
     case 0: return launch_pass_z(d_vox, d, s);
     case 1:
@@ -896,9 +896,12 @@ cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scrat
   }
 }
 
-cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s) {
-  cudaError_t e = launch_edt_pass(d_vox, d_scratch, scratch_words, d, 0, s);
-  return e == cudaSuccess ? launch_edt_pass(d_vox, d_scratch, scratch_words, d, 3, s) : e;
+cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s,
+                       const EdtConfig& cfg) {
+  cudaError_t e = launch_edt_pass(d_vox, d_scratch, scratch_words, d, 0, s, cfg.rows);
+  if (e != cudaSuccess || cfg.fused) return e == cudaSuccess ? launch_edt_pass(d_vox, d_scratch, scratch_words, d, 3, s, cfg.rows) : e;
+  e = launch_edt_pass(d_vox, d_scratch, scratch_words, d, 1, s, cfg.rows);
+  return e == cudaSuccess ? launch_edt_pass(d_vox, d_scratch, scratch_words, d, 2, s, cfg.rows) : e;
 }
 
 cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag) {
@@ -917,7 +920,7 @@ long long edt_batch_stack_warps() {
   return std::max(batch_stack_warps<16>(), batch_stack_warps<32>());
 }
 
-cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s) {
+cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s, int rows) {
   const int smem = kZWarps * kZWarpWords * 4;
   long long blocks = 0;
   cudaError_t e = kernel_setup<edt_pass_z_batch>(kZWarps * 32, smem, &blocks);
@@ -926,7 +929,8 @@ cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cuda
   edt_pass_z_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0]);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return sweep_rows() == 32 ? launch_yx_batch<32>(d_table, it, s) : launch_yx_batch<16>(d_table, it, s);
+  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32>(d_table, it, s)
+                                                 : launch_yx_batch<16>(d_table, it, s);
 }
 
 }  // namespace gvx

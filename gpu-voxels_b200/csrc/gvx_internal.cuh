@@ -46,6 +46,8 @@ struct gvx_dvm {
   bool owns;
   uint32_t* d_scratch;  // EDT workspace (proximate-site stacks, slice counters), owned
   uint64_t scratch_words;
+  int edt_rows;   // EDT sweep configuration (0 = library default), set by the autotuner
+  int edt_fused;
 };
 
 struct gvx_bvm {
@@ -110,10 +112,17 @@ cudaError_t launch_bvm_insert(uint8_t* d_vox, gvx_dims d, float side, const floa
 // edt_scratch_words_min the least any launch needs.
 uint64_t edt_scratch_words(gvx_dims d);
 uint64_t edt_scratch_words_min(gvx_dims d);
-cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s);
+// EDT launch configuration: rows per staging chunk of the sweeps (16 or 32;
+// 0 = library default) and whether the y and x sweeps run as one fused launch.
+struct EdtConfig {
+  int rows = 0;
+  int fused = 1;
+};
+cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s,
+                       const EdtConfig& cfg = EdtConfig{});
 // pass 0 = Z, 1 = Y, 2 = X (one launch each), 3 = fused Y -> X
 cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, int pass,
-                            cudaStream_t s);
+                            cudaStream_t s, int rows = 0);
 // Synchronous read of the error word the last fused launch left (0 = ok).
 cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag);
 // Resident warps of the fused batch launch (size of the batch stack pool).
@@ -123,7 +132,12 @@ void set_edt_sweep_rows(int rows);
 // Warp work items of one EDT pass for a map of dims d.
 long long edt_pass_items(gvx_dims d, int pass);
 // All maps of a batch, one persistent launch per pass.
-cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& items, cudaStream_t s);
+cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& items, cudaStream_t s, int rows = 0);
+// Autotuner cache (tune.cu): the best configuration recorded for `key` on the
+// current device, from memory or the file named by GVX_TUNE_CACHE.
+bool tune_lookup(const std::string& key, EdtConfig* cfg, float* ms);
+void tune_store(const std::string& key, const EdtConfig& cfg, float ms);
+std::string tune_device_name();
 cudaError_t launch_dvm_sqdist(const uint32_t* d_vox, gvx_dims d, const uint32_t* d_ids, uint64_t n, int32_t* d_out,
                               int mode, cudaStream_t s);
 cudaError_t launch_dvm_sqdist_map(const uint32_t* d_vox, gvx_dims d, int32_t* d_out, cudaStream_t s);

@@ -33,6 +33,10 @@ class GvxError(RuntimeError):
         self.status = status
 
 
+class EdtConfig(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_uint32), ("fused", ctypes.c_uint32), ("ms", ctypes.c_float)]
+
+
 class Dims(ctypes.Structure):
     _fields_ = [("x", ctypes.c_uint32), ("y", ctypes.c_uint32), ("z", ctypes.c_uint32)]
 
@@ -73,6 +77,8 @@ PROTOTYPES = {
     "gvx_dvm_edt": [_vp, _u32, _u32, _u32, _vp],
     "gvx_dvm_edt_pass": [_vp, ctypes.c_int, _vp],
     "gvx_dvm_edt_check": [_vp, ctypes.POINTER(_u32)],
+    "gvx_dvm_autotune": [_vp, ctypes.c_int, ctypes.POINTER(EdtConfig), _vp],
+    "gvx_dvm_set_edt_config": [_vp, ctypes.POINTER(EdtConfig)],
     "gvx_dvm_edt_static_workspace": [_vp, ctypes.POINTER(Dims), _vp],
     "gvx_dvm_sqdist": [_vp, _vp, _u64, _vp, _vp],
     "gvx_dvm_dist": [_vp, _vp, _u64, _vp, _vp],
@@ -89,6 +95,7 @@ PROTOTYPES = {
     "gvx_batch_insert_points": [_vp, _vp, _vp, _u64, _vp],
     "gvx_batch_edt": [_vp, _vp],
     "gvx_batch_edt_check": [_vp, ctypes.POINTER(_u32)],
+    "gvx_batch_autotune": [_vp, ctypes.c_int, ctypes.POINTER(EdtConfig), _vp],
     "gvx_batch_query_trilinear": [_vp, _vp, _vp, _u64, _vp, _vp, _vp],
     "gvx_batch_graph_capture": [_vp, _vp, _vp, _u64, _vp, _vp, _u64, _vp, _vp, _vp],
     "gvx_batch_graph_launch": [_vp, _vp],

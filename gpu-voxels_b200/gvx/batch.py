@@ -42,6 +42,14 @@ class Batch:
     def edt(self) -> None:
         call("gvx_batch_edt", self._h, _stream())
 
+    def autotune(self, force: bool = False) -> dict:
+        """Pick the fastest sweep configuration of the batched EDT (the maps'
+        content is saved and restored around the timing runs)."""
+        from ._abi import EdtConfig
+        c = EdtConfig()
+        call("gvx_batch_autotune", self._h, int(bool(force)), ctypes.byref(c), _stream())
+        return {"rows": c.rows, "fused": c.fused, "ms": c.ms}
+
     def edt_check(self) -> int:
         """Synchronise and return the error word of the last batched EDT (0 = ok)."""
         flags = ctypes.c_uint32(0)

@@ -106,6 +106,19 @@ class DistanceVoxelMap:
         sweeps as the one fused launch parallelBanding3D uses."""
         call("gvx_dvm_edt_pass", self._h, int(pass_index), _stream())
 
+    def autotune(self, force: bool = False) -> dict:
+        """Pick the fastest EDT sweep configuration for this map (timed on a
+        copy of its current content; cached per device and dims, and across
+        processes through the file named by GVX_TUNE_CACHE)."""
+        c = _abi.EdtConfig()
+        call("gvx_dvm_autotune", self._h, int(bool(force)), ctypes.byref(c), _stream())
+        return {"rows": c.rows, "fused": c.fused, "ms": c.ms}
+
+    def set_edt_config(self, rows: int = 0, fused: int = 1) -> None:
+        """Fix the EDT sweep configuration (rows 16 or 32, 0 = default; fused 0/1)."""
+        c = _abi.EdtConfig(rows, fused, 0.0)
+        call("gvx_dvm_set_edt_config", self._h, ctypes.byref(c))
+
     def edt_check(self) -> int:
         """Synchronise and return the error word of the last EDT (0 = ok);
         raises GvxError (GVX_ERR_TIMEOUT) when a bounded wait gave up."""

@@ -94,6 +94,24 @@ GVX_API gvx_status gvx_dvm_edt(gvx_dvm *m, uint32_t m1, uint32_t m2, uint32_t m3
  * 0, 1, 2 gives the same result).  Pass 0 alone equals the reference's
  * phase 1 (kernelPBAphase1FloodZ, GV/voxelmap/kernels/VoxelMapOperationsPBA.hpp:63-124). */
 GVX_API gvx_status gvx_dvm_edt_pass(gvx_dvm *m, int pass, gvx_stream stream);
+/* EDT launch configuration chosen by the autotuner: rows per staging chunk of
+ * the sweeps (16 or 32; 0 = library default), whether the y and x sweeps run
+ * as one fused launch (1) or two (0), and the time measured for it. */
+typedef struct {
+  uint32_t rows;
+  uint32_t fused;
+  float ms;
+} gvx_edt_config;
+/* Project-written autotuner (no counterpart in the reference, whose PBA band
+ * counts are fixed by the caller): times every configuration on a copy of
+ * the map's current content (allocated for the call and freed; the map is
+ * not modified), keeps the fastest for this map's later EDTs and returns it.
+ * Choices are cached per device and dims in memory and, if the environment
+ * variable GVX_TUNE_CACHE names a file, across processes; force = 1 re-times.
+ * Synchronises the stream.  Every configuration gives bit-identical results. */
+GVX_API gvx_status gvx_dvm_autotune(gvx_dvm *m, int force, gvx_edt_config *out, gvx_stream stream);
+/* Sets the configuration explicitly (ms is ignored). */
+GVX_API gvx_status gvx_dvm_set_edt_config(gvx_dvm *m, const gvx_edt_config *cfg);
 /* Synchronises the device and reads the error word of the last EDT on this
  * map: *flags = 0 when every bounded wait of the fused y -> x sweep ended in
  * time, else non-zero with GVX_ERR_TIMEOUT (the map's content is then
@@ -191,6 +209,10 @@ GVX_API gvx_status gvx_batch_insert_points(gvx_batch *b, const float *d_xyz, con
 GVX_API gvx_status gvx_batch_edt(gvx_batch *b, gvx_stream stream);
 /* As gvx_dvm_edt_check, for the last gvx_batch_edt. */
 GVX_API gvx_status gvx_batch_edt_check(gvx_batch *b, uint32_t *flags);
+/* As gvx_dvm_autotune for the batched EDT (rows per staging chunk; the batch
+ * always fuses).  The maps' content is saved to a temporary buffer before the
+ * timing runs and restored after them.  Re-capture a graph after tuning. */
+GVX_API gvx_status gvx_batch_autotune(gvx_batch *b, int force, gvx_edt_config *out, gvx_stream stream);
 /* Query i is answered on map d_map[i]; d_grad optional. */
 GVX_API gvx_status gvx_batch_query_trilinear(gvx_batch *b, const float *d_xyz, const uint32_t *d_map, uint64_t n,
                                              float *d_dist, float *d_grad, gvx_stream stream);
