@@ -60,20 +60,31 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // pass Z: phase 1 per (x, y) column, m1 = 1.
 // The forward flood only changes value at rows whose input holds a site, so
 // the forward scan records those (value, row) pairs -- the column's site list
-// -- in an on-chip ring, and the backward flood walks the list downward.  A
-// column with more sites than the ring holds finds the older ones again by
-// scanning its (still unmodified) input below the current row.  Reads and
-// writes stream once; each row is a fixed, lockstep step.
+// -- in an on-chip ring, and the backward flood walks the list downward.
+// Each lane also stores its forward-flood value at the end of every chunk
+// (the chunk's carry) to the workspace.  A warp in which some column has more
+// sites than the ring holds walks back chunk by chunk instead: it restages
+// the (still unmodified) input of each chunk, rebuilds the chunk's forward
+// flood from the carry of the chunk below, and floods backward from that.
+// Every row is a fixed, lockstep step.
 // ---------------------------------------------------------------------------
 constexpr int kZChunk = 16;
 constexpr int kZRing = 16;
 constexpr int kZWarps = 8;
 constexpr int kZWarpWords = 2 * kZChunk * 32 + 2 * kZRing * 32;
 
+// Words of the EDT workspace's counter area (Z slice counters, queue head,
+// error word, padded to 32).
+__host__ __device__ __forceinline__ uint64_t edt_sync_words(int Z) { return ((uint64_t)Z + 2 + 31) / 32 * 32; }
+
+// Workspace words of pass Z's chunk carries for a map: per warp item
+// (32 columns) one word per lane and chunk.
+__host__ __device__ __forceinline__ uint64_t zcarry_item_words(int Z) { return (uint64_t)((Z + kZChunk - 1) / kZChunk) * 32; }
+
 // One warp item of pass Z: 32 adjacent (x, y) columns; wbase = the warp's
-// kZWarpWords of shared memory.
+// kZWarpWords of shared memory; carry = the item's zcarry_item_words(Z) words.
 __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, int Y, int Z, long long item,
-                                            uint32_t* wbase) {
+                                            uint32_t* wbase, uint32_t* __restrict__ carry) {
   const int lane = threadIdx.x & 31;
   const int nxb = (X + 31) >> 5;
   const int xb = (int)(item % nxb), y = (int)(item / nxb);
@@ -99,12 +110,13 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
     }
   };
 
-  // forward: record the sites of the column
+  // forward: record the sites of the column and each chunk's carry
   stage(tile0, 0);
   cp_async_commit();
   if (nchunks > 1) stage(tile1, 1);
   cp_async_commit();
-  int m = 0;  // sites seen
+  int m = 0;                 // sites seen
+  uint32_t flood = kDvUninit;  // forward-flood value
   for (int c = 0; c < nchunks; ++c) {
     cp_async_wait1();
     __syncwarp();
@@ -116,56 +128,79 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
         ringV[(m % kZRing) * 32] = v;
         ringR[(m % kZRing) * 32] = (uint32_t)(r0 + r);
         ++m;
+        flood = v;
       }
     }
+    carry[c * 32 + lane] = flood;
     __syncwarp();
     if (c + 2 < nchunks) stage((c & 1) ? tile1 : tile0, c + 2);
     cp_async_commit();
   }
   cp_async_wait_all();
+  __syncwarp();
 
   // backward: obstacle(z) from the forward value fwd(z) = last site at or below z;
   // ties keep the lower z (<=, VoxelMapOperationsPBA.hpp:112-122)
-  const uint32_t* col = src + lane;  // this lane's column (input rows <= z are still unmodified)
-  int j = m - 1;                     // index of the site fwd(z)
-  uint32_t fwdV = kDvUninit;
-  int fwdRow = -1;
-  if (j >= 0) {
-    fwdV = ringV[(j % kZRing) * 32];
-    fwdRow = (int)ringR[(j % kZRing) * 32];
-  }
   uint32_t obstacle = kDvUninit;
   uint32_t* dst = map + (uint64_t)y * X + x0 + lane;
   const bool live = lane < valid_cols;
-  for (int z = Z - 1; z >= 0; --z) {
-    while (fwdRow > z) {  // step to the previous site
-      --j;
-      if (j < 0) {
-        fwdV = kDvUninit;
-        fwdRow = -1;
-      } else if (j >= m - kZRing) {
-        fwdV = ringV[(j % kZRing) * 32];
-        fwdRow = (int)ringR[(j % kZRing) * 32];
-      } else if (live) {  // older than the ring: scan the input downward
-        int rr = z;
-        uint32_t v = kDvUninit;
-        for (; rr >= 0; --rr) {
-          v = col[(uint64_t)rr * layer];
-          if ((v >> 20) != kUninit) break;
-        }
-        fwdRow = rr;
-        fwdV = rr >= 0 ? v : kDvUninit;
-        if (rr < 0) j = -1;
-      } else {
-        fwdV = kDvUninit;
-        fwdRow = -1;
-      }
+  if (!__any_sync(kFullMask, m > kZRing)) {
+    int j = m - 1;  // index of the site fwd(z)
+    uint32_t fwdV = kDvUninit;
+    int fwdRow = -1;
+    if (j >= 0) {
+      fwdV = ringV[(j % kZRing) * 32];
+      fwdRow = (int)ringR[(j % kZRing) * 32];
     }
-    const int dist_prev = abs((int)(obstacle >> 20) - z);
-    const int dist_next = abs(z - (int)(fwdV >> 20));
-    if (dist_next <= dist_prev) obstacle = fwdV;
-    if (live) dst[(uint64_t)z * layer] = obstacle;
+    for (int z = Z - 1; z >= 0; --z) {
+      while (fwdRow > z) {  // step to the previous site (all in the ring)
+        --j;
+        if (j < 0) {
+          fwdV = kDvUninit;
+          fwdRow = -1;
+        } else {
+          fwdV = ringV[(j % kZRing) * 32];
+          fwdRow = (int)ringR[(j % kZRing) * 32];
+        }
+      }
+      const int dist_prev = abs((int)(obstacle >> 20) - z);
+      const int dist_next = abs(z - (int)(fwdV >> 20));
+      if (dist_next <= dist_prev) obstacle = fwdV;
+      if (live) dst[(uint64_t)z * layer] = obstacle;
+    }
+    return;
   }
+  // chunk by chunk: restage the input (descending, double buffered), rebuild
+  // the chunk's forward flood in place from the carry below, flood backward
+  __syncwarp();  // the carries of all lanes
+  stage(tile0, nchunks - 1);
+  cp_async_commit();
+  if (nchunks > 1) stage(tile1, nchunks - 2);
+  cp_async_commit();
+  for (int c = nchunks - 1, k = 0; c >= 0; --c, ++k) {
+    cp_async_wait1();
+    __syncwarp();
+    uint32_t* tile = (k & 1) ? tile1 : tile0;
+    const int r0 = c * kZChunk, rows = min(kZChunk, Z - r0);
+    uint32_t f = c > 0 ? carry[(c - 1) * 32 + lane] : kDvUninit;
+    for (int r = 0; r < rows; ++r) {
+      const uint32_t v = tile[r * 32 + lane];
+      if ((v >> 20) != kUninit) f = v;
+      tile[r * 32 + lane] = f;
+    }
+    for (int r = rows - 1; r >= 0; --r) {
+      const int z = r0 + r;
+      const uint32_t fwdV = tile[r * 32 + lane];
+      const int dist_prev = abs((int)(obstacle >> 20) - z);
+      const int dist_next = abs(z - (int)(fwdV >> 20));
+      if (dist_next <= dist_prev) obstacle = fwdV;
+      if (live) dst[(uint64_t)z * layer] = obstacle;
+    }
+    __syncwarp();
+    if (c - 2 >= 0) stage(tile, c - 2);
+    cp_async_commit();
+  }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -575,12 +610,14 @@ __device__ __forceinline__ uint32_t batch_owner(const long long* __restrict__ pr
   return lo;
 }
 
-__global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z(uint32_t* __restrict__ map, int X, int Y, int Z) {
+// carries: the map's workspace past its counters (zcarry_item_words per item)
+__global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z(uint32_t* __restrict__ map, uint32_t* __restrict__ carries,
+                                                               int X, int Y, int Z) {
   extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][kZWarpWords]
   const int warp = threadIdx.x >> 5;
   const long long item = (long long)blockIdx.x * kZWarps + warp;
   if (item >= (long long)((X + 31) >> 5) * Y) return;
-  pass_z_item(map, X, Y, Z, item, s_z + (size_t)warp * kZWarpWords);
+  pass_z_item(map, X, Y, Z, item, s_z + (size_t)warp * kZWarpWords, carries + (uint64_t)item * zcarry_item_words(Z));
 }
 
 // Pass Z over every map of a batch: persistent warps stride over the items of
@@ -593,7 +630,9 @@ __global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z_batch(const BatchM
   for (long long g = (long long)blockIdx.x * kZWarps + warp; g < total; g += (long long)gridDim.x * kZWarps) {
     const uint32_t k = batch_owner(prefix, n_maps, g);
     const BatchMap m = maps[k];
-    pass_z_item(m.vox, m.X, m.Y, m.Z, g - __ldg(prefix + k), s_z + (size_t)warp * kZWarpWords);
+    const long long item = g - __ldg(prefix + k);
+    pass_z_item(m.vox, m.X, m.Y, m.Z, item, s_z + (size_t)warp * kZWarpWords,
+                m.scratch + edt_sync_words(m.Z) + (uint64_t)item * zcarry_item_words(m.Z));
     __syncwarp();
   }
 }
@@ -784,18 +823,21 @@ cudaError_t kernel_setup(int threads, int smem, long long* resident) {
   return st.err[dev];
 }
 
-cudaError_t launch_pass_z(uint32_t* map, gvx_dims d, cudaStream_t s) {
+cudaError_t launch_pass_z(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStream_t s) {
   const int smem = kZWarps * kZWarpWords * 4;
   cudaError_t e = kernel_setup<edt_pass_z>(kZWarps * 32, smem, nullptr);
   if (e != cudaSuccess) return e;
   const long long items = (long long)((d.x + 31) / 32) * d.y;
-  edt_pass_z<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(map, (int)d.x, (int)d.y, (int)d.z);
+  edt_pass_z<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(
+      map, scratch + edt_sync_words((int)d.z), (int)d.x, (int)d.y, (int)d.z);
   return cudaGetLastError();
 }
 
 // Workspace layout: [slice counters, queue head, error word: sync_words(d)]
-// [stack area: one stack of warp_stack_words per launched warp].
-uint64_t sync_words(gvx_dims d) { return ((uint64_t)d.z + 2 + 31) / 32 * 32; }
+// [stack area: one stack of warp_stack_words per launched warp; before the
+// sweeps, pass Z keeps its chunk carries there].
+uint64_t sync_words(gvx_dims d) { return edt_sync_words((int)d.z); }
+uint64_t zcarry_words(gvx_dims d) { return (uint64_t)((d.x + 31) / 32) * d.y * zcarry_item_words((int)d.z); }
 
 // Blocks for a persistent sweep launch: resident, fitting the stack area, and
 // no more than the items need (0 when the area holds no block's stacks).
@@ -894,7 +936,7 @@ long long batch_stack_warps() {
 void set_edt_sweep_rows(int rows) { g_sweep_rows = rows == 32 ? 32 : 16; }
 
 uint64_t edt_scratch_words_min(gvx_dims d) {
-  return sync_words(d) + (uint64_t)SweepCfg<32>::kWarps * warp_stack_words((int)d.x, (int)d.y);
+  return sync_words(d) + std::max<uint64_t>(SweepCfg<32>::kWarps * warp_stack_words((int)d.x, (int)d.y), zcarry_words(d));
 }
 uint64_t edt_scratch_words(gvx_dims d) {
   return std::max(sync_words(d) + fused_stack_words(d), edt_scratch_words_min(d));
@@ -902,10 +944,10 @@ uint64_t edt_scratch_words(gvx_dims d) {
 
 cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, int pass,
                             cudaStream_t s, int rows) {
-  if (pass != 0 && scratch_words < edt_scratch_words_min(d)) return cudaErrorInvalidValue;
+  if (scratch_words < edt_scratch_words_min(d)) return cudaErrorInvalidValue;
   const bool big = (rows == 0 ? sweep_rows() : rows) == 32;
   switch (pass) {
-    case 0: return launch_pass_z(d_vox, d, s);
+    case 0: return launch_pass_z(d_vox, d_scratch, d, s);
     case 1:
       return big ? launch_sweep<false, 32>(d_vox, d_scratch, scratch_words, d, s)
                  : launch_sweep<false, 16>(d_vox, d_scratch, scratch_words, d, s);
