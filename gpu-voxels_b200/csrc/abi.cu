@@ -170,6 +170,13 @@ gvx_status gvx_dvm_edt(gvx_dvm* m, uint32_t m1, uint32_t m2, uint32_t m3, gvx_st
   return cuda_status(launch_edt(m->d_vox, m->d_scratch, m->scratch_words, m->dims, as_stream(stream), EdtConfig{m->edt_rows, m->edt_fused}), "parallelBanding3D");
 }
 
+gvx_status gvx_dvm_voxelize_edt(gvx_dvm* m, const float* d_xyz, uint64_t n, uint32_t* d_outside, gvx_stream stream) {
+  if (m == nullptr || (n > 0 && d_xyz == nullptr)) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  return cuda_status(launch_voxelize_edt(m->d_vox, m->d_scratch, m->scratch_words, m->dims, m->side, d_xyz, n, d_outside,
+                                         as_stream(stream), EdtConfig{m->edt_rows, m->edt_fused}),
+                     "voxelize + EDT");
+}
+
 gvx_status gvx_dvm_edt_pass(gvx_dvm* m, int pass, gvx_stream stream) {
   if (m == nullptr || pass < 0 || pass > 3) return fail(GVX_ERR_INVALID_ARG, "map is null or pass not in {0,1,2,3}");
   return cuda_status(launch_edt_pass(m->d_vox, m->d_scratch, m->scratch_words, m->dims, pass, as_stream(stream), m->edt_rows), "EDT pass");

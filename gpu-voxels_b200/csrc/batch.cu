@@ -193,6 +193,13 @@ gvx_status gvx_batch_edt(gvx_batch* b, gvx_stream stream) {
   return cuda_status(launch_edt_batch(b->d_table, b->items, as_stream(stream), b->edt_rows), "batch EDT");
 }
 
+gvx_status gvx_batch_voxelize_edt(gvx_batch* b, const float* d_xyz, const uint64_t* d_offsets, uint64_t n_total,
+                                  gvx_stream stream) {
+  if (b == nullptr || d_offsets == nullptr || (n_total > 0 && d_xyz == nullptr)) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  return cuda_status(launch_voxelize_edt_batch(b->d_table, b->items, d_xyz, d_offsets, n_total, as_stream(stream), b->edt_rows),
+                     "batch voxelize + EDT");
+}
+
 gvx_status gvx_batch_edt_check(gvx_batch* b, uint32_t* flags) {
   if (b == nullptr || flags == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
   cudaError_t e = cudaDeviceSynchronize();
@@ -286,9 +293,7 @@ gvx_status gvx_batch_graph_capture(gvx_batch* b, const float* d_xyz, const uint6
   cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e != cudaSuccess) return cuda_status(e, "capture stream");
   // one plain run first: it sets every kernel attribute outside the capture
-  gvx_status st = gvx_batch_clear(b, s);
-  if (st == GVX_OK) st = gvx_batch_insert_points(b, d_xyz, d_offsets, n_total, s);
-  if (st == GVX_OK) st = gvx_batch_edt(b, s);
+  gvx_status st = gvx_batch_voxelize_edt(b, d_xyz, d_offsets, n_total, s);
   if (st == GVX_OK) st = gvx_batch_query_trilinear(b, d_qxyz, d_qmap, n_q, d_dist, d_grad, s);
   if (st == GVX_OK) st = cuda_status(cudaStreamSynchronize(s), "batch warm-up");
   if (st != GVX_OK) {
@@ -299,9 +304,7 @@ gvx_status gvx_batch_graph_capture(gvx_batch* b, const float* d_xyz, const uint6
   if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
   e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    st = gvx_batch_clear(b, s);
-    if (st == GVX_OK) st = gvx_batch_insert_points(b, d_xyz, d_offsets, n_total, s);
-    if (st == GVX_OK) st = gvx_batch_edt(b, s);
+    st = gvx_batch_voxelize_edt(b, d_xyz, d_offsets, n_total, s);
     if (st == GVX_OK) st = gvx_batch_query_trilinear(b, d_qxyz, d_qmap, n_q, d_dist, d_grad, s);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(s, &g);

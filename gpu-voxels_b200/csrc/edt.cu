@@ -204,6 +204,92 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
 }
 
 // ---------------------------------------------------------------------------
+// Voxelisation fused with pass Z.  After clearMap + insertPointCloud a
+// DistanceVoxelMap holds each occupied voxel's own coordinate and UNINIT
+// elsewhere, so it is fully described by one occupancy bit per voxel.  The
+// fused path records those bits (word ((y * nxb + xb) * Z + z), bit x & 31)
+// in the workspace instead of clearing and scattering the map, and pass Z
+// reads the bits: the map is written once, by pass Z.  The flood arithmetic
+// is phase 1's (the same values, the same ties, UNINIT's z read as 1023).
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint64_t occ_words(int X, int Y, int Z) {
+  return (uint64_t)((X + 31) >> 5) * Y * Z;
+}
+
+__device__ __forceinline__ void occ_set(uint32_t* bits, int X, int Z, uint32_t x, uint32_t y, uint32_t z) {
+  const uint32_t nxb = ((uint32_t)X + 31) >> 5;
+  atomicOr(bits + ((uint64_t)y * nxb + (x >> 5)) * Z + z, 1u << (x & 31));
+}
+
+// insertPointCloud into the occupancy bits (coordinates as
+// kernelInsertGlobalPointCloud, GV/voxelmap/kernels/VoxelMapOperations.hpp:266-300).
+__global__ void occ_insert_kernel(uint32_t* __restrict__ bits, int X, int Y, int Z, float side,
+                                  const float* __restrict__ xyz, uint64_t n, uint32_t* __restrict__ outside) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  bool out = false;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t x = coord_to_voxel(__ldg(xyz + 3 * i), side), y = coord_to_voxel(__ldg(xyz + 3 * i + 1), side),
+                   z = coord_to_voxel(__ldg(xyz + 3 * i + 2), side);
+    if (x < (uint32_t)X && y < (uint32_t)Y && z < (uint32_t)Z) occ_set(bits, X, Z, x, y, z);
+    else out = true;
+  }
+  if (outside != nullptr && __any_sync(kFullMask, out) && (threadIdx.x & 31) == 0) *outside = 1u;
+}
+
+// Pass Z of one warp item (32 adjacent (x, y) columns) from occupancy bits.
+// The item's Z words are read 32 at a time and transposed by ballots into one
+// 32-row mask per lane; an ascending pass keeps, per 32-row chunk, each lane's
+// mask and the last occupied z below the chunk (smem), and the backward flood
+// reads the forward value of every row from them.  wbase: 2048 words.
+__device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, const uint32_t* __restrict__ bits, int X,
+                                                 int Y, int Z, long long item, uint32_t* wbase) {
+  const int lane = threadIdx.x & 31;
+  const int nxb = (X + 31) >> 5;
+  const int xb = (int)(item % nxb), y = (int)(item / nxb);
+  const int x = xb * 32 + lane;
+  const uint32_t* wcol = bits + (uint64_t)item * Z;
+  uint32_t* mk = wbase + lane;         // chunk c: mk[c * 32]
+  uint32_t* lb = wbase + 1024 + lane;  // chunk c: lb[c * 32], 1023 = none
+  const int nch = (Z + 31) >> 5;
+  uint32_t last = 1023u;
+  for (int c = 0; c < nch; ++c) {
+    const int z = c * 32 + lane;
+    const uint32_t w = z < Z ? __ldg(wcol + z) : 0u;
+    uint32_t mine = 0u;
+#pragma unroll
+    for (int l = 0; l < 32; ++l) {
+      const uint32_t b = __ballot_sync(kFullMask, (w >> l) & 1u);
+      if (l == lane) mine = b;
+    }
+    mk[c * 32] = mine;
+    lb[c * 32] = last;
+    if (mine) last = (uint32_t)(c * 32 + 31 - __clz(mine));
+  }
+  __syncwarp();
+  const uint64_t layer = (uint64_t)X * Y;
+  uint32_t* dst = map + (uint64_t)y * X + x;
+  const bool live = x < X;
+  const uint32_t base = (uint32_t)x | ((uint32_t)y << 10);
+  int obst = 1023;  // z of the backward-flood obstacle (1023: UNINIT)
+  for (int z = Z - 1; z >= 0; --z) {
+    const int c = z >> 5;
+    const uint32_t mm = mk[c * 32] & ((2u << (z & 31)) - 1u);
+    const int fz = mm ? c * 32 + 31 - __clz(mm) : (int)lb[c * 32];
+    if (abs(z - fz) <= abs(obst - z)) obst = fz;
+    if (live) dst[(uint64_t)z * layer] = obst == 1023 ? kDvUninit : base | ((uint32_t)obst << 20);
+  }
+}
+
+__global__ void __launch_bounds__(kZWarps * 32) edt_pass_z_bits(uint32_t* __restrict__ map,
+                                                                 const uint32_t* __restrict__ bits, int X, int Y, int Z) {
+  extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][2048]
+  const int warp = threadIdx.x >> 5;
+  const long long item = (long long)blockIdx.x * kZWarps + warp;
+  if (item >= (long long)((X + 31) >> 5) * Y) return;
+  pass_z_bits_item(map, bits, X, Y, Z, item, s_z + (size_t)warp * 2048);
+}
+
+// ---------------------------------------------------------------------------
 // passes Y and X
 // ---------------------------------------------------------------------------
 
@@ -640,6 +726,48 @@ __global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z_batch(const BatchM
 // Words of stack one warp needs for a map (a pair per row per lane).
 __host__ __device__ __forceinline__ uint64_t warp_stack_words(int X, int Y) { return (uint64_t)max(X, Y) * 64; }
 
+// The fused voxelisation for every map of a batch: each map's occupancy
+// bits sit in its own workspace past the counters.
+__device__ __forceinline__ uint32_t* batch_occ(const BatchMap& m) { return m.scratch + edt_sync_words(m.Z); }
+
+__global__ void occ_clear_batch_kernel(const BatchMap* __restrict__ maps) {
+  const BatchMap m = maps[blockIdx.y];
+  uint32_t* bits = batch_occ(m);
+  const uint64_t n = occ_words(m.X, m.Y, m.Z);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    bits[i] = 0u;
+}
+
+// point i belongs to map k with offsets[k] <= i < offsets[k + 1]
+__global__ void occ_insert_batch_kernel(const BatchMap* __restrict__ maps, uint32_t n_maps, const float* __restrict__ xyz,
+                                        const uint64_t* __restrict__ offsets, uint64_t n) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t lo = 0, hi = n_maps;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(offsets + mid) <= i) lo = mid; else hi = mid;
+    }
+    const BatchMap m = maps[lo];
+    const uint32_t x = coord_to_voxel(__ldg(xyz + 3 * i), m.side), y = coord_to_voxel(__ldg(xyz + 3 * i + 1), m.side),
+                   z = coord_to_voxel(__ldg(xyz + 3 * i + 2), m.side);
+    if (x < (uint32_t)m.X && y < (uint32_t)m.Y && z < (uint32_t)m.Z) occ_set(batch_occ(m), m.X, m.Z, x, y, z);
+  }
+}
+
+__global__ void __launch_bounds__(kZWarps * 32) edt_pass_z_bits_batch(const BatchMap* __restrict__ maps,
+                                                                       const long long* __restrict__ prefix,
+                                                                       uint32_t n_maps, long long total) {
+  extern __shared__ __align__(16) uint32_t s_z[];
+  const int warp = threadIdx.x >> 5;
+  for (long long g = (long long)blockIdx.x * kZWarps + warp; g < total; g += (long long)gridDim.x * kZWarps) {
+    const uint32_t k = batch_owner(prefix, n_maps, g);
+    const BatchMap m = maps[k];
+    pass_z_bits_item(m.vox, batch_occ(m), m.X, m.Y, m.Z, g - __ldg(prefix + k), s_z + (size_t)warp * 2048);
+    __syncwarp();
+  }
+}
+
 // One pass (Y or X) on its own (per-pass timing and the fallback of the fused
 // schedule below): persistent warps stride over the items, one stack each.
 template <bool kXPass, int kRows>
@@ -936,7 +1064,8 @@ long long batch_stack_warps() {
 void set_edt_sweep_rows(int rows) { g_sweep_rows = rows == 32 ? 32 : 16; }
 
 uint64_t edt_scratch_words_min(gvx_dims d) {
-  return sync_words(d) + std::max<uint64_t>(SweepCfg<32>::kWarps * warp_stack_words((int)d.x, (int)d.y), zcarry_words(d));
+  return sync_words(d) + std::max<uint64_t>({SweepCfg<32>::kWarps * warp_stack_words((int)d.x, (int)d.y),
+                                             zcarry_words(d), occ_words((int)d.x, (int)d.y, (int)d.z)});
 }
 uint64_t edt_scratch_words(gvx_dims d) {
   return std::max(sync_words(d) + fused_stack_words(d), edt_scratch_words_min(d));
@@ -983,6 +1112,51 @@ long long edt_pass_items(gvx_dims d, int pass) {
 
 long long edt_batch_stack_warps() {
   return std::max(batch_stack_warps<16>(), batch_stack_warps<32>());
+}
+
+cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, float side,
+                                const float* d_xyz, uint64_t n, uint32_t* d_outside, cudaStream_t s,
+                                const EdtConfig& cfg) {
+  if (scratch_words < edt_scratch_words_min(d)) return cudaErrorInvalidValue;
+  uint32_t* bits = d_scratch + edt_sync_words((int)d.z);
+  cudaError_t e = cudaMemsetAsync(bits, 0, occ_words((int)d.x, (int)d.y, (int)d.z) * sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  if (n > 0) {
+    const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
+    occ_insert_kernel<<<blocks, 256, 0, s>>>(bits, (int)d.x, (int)d.y, (int)d.z, side, d_xyz, n, d_outside);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  const int smem = kZWarps * 2048 * 4;
+  e = kernel_setup<edt_pass_z_bits>(kZWarps * 32, smem, nullptr);
+  if (e != cudaSuccess) return e;
+  const long long items = (long long)((d.x + 31) / 32) * d.y;
+  edt_pass_z_bits<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(d_vox, bits, (int)d.x,
+                                                                                         (int)d.y, (int)d.z);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (cfg.fused) return launch_edt_pass(d_vox, d_scratch, scratch_words, d, 3, s, cfg.rows);
+  e = launch_edt_pass(d_vox, d_scratch, scratch_words, d, 1, s, cfg.rows);
+  return e == cudaSuccess ? launch_edt_pass(d_vox, d_scratch, scratch_words, d, 2, s, cfg.rows) : e;
+}
+
+cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems& it, const float* d_xyz,
+                                      const uint64_t* d_offsets, uint64_t n_total, cudaStream_t s, int rows) {
+  occ_clear_batch_kernel<<<dim3(64, it.n_maps), 256, 0, s>>>(d_table);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (n_total > 0) {
+    const unsigned blocks = (unsigned)std::min<uint64_t>((n_total + 255) / 256, 148ull * 16);
+    occ_insert_batch_kernel<<<blocks, 256, 0, s>>>(d_table, it.n_maps, d_xyz, d_offsets, n_total);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  const int smem = kZWarps * 2048 * 4;
+  long long blocks = 0;
+  e = kernel_setup<edt_pass_z_bits_batch>(kZWarps * 32, smem, &blocks);
+  if (e != cudaSuccess) return e;
+  blocks = std::max<long long>(1, std::min<long long>(blocks, (it.total[0] + kZWarps - 1) / kZWarps));
+  edt_pass_z_bits_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0]);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32>(d_table, it, s)
+                                                 : launch_yx_batch<16>(d_table, it, s);
 }
 
 cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s, int rows) {

@@ -133,6 +133,13 @@ void set_edt_sweep_rows(int rows);
 long long edt_pass_items(gvx_dims d, int pass);
 // All maps of a batch, one persistent launch per pass.
 cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& items, cudaStream_t s, int rows = 0);
+// clearMap + insertPointCloud + EDT in one pass: occupancy bits in the
+// workspace, pass Z reads them (the map is written once).
+cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, float side,
+                                const float* d_xyz, uint64_t n, uint32_t* d_outside, cudaStream_t s,
+                                const EdtConfig& cfg = EdtConfig{});
+cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems& items, const float* d_xyz,
+                                      const uint64_t* d_offsets, uint64_t n_total, cudaStream_t s, int rows = 0);
 // Autotuner cache (tune.cu): the best configuration recorded for `key` on the
 // current device, from memory or the file named by GVX_TUNE_CACHE.
 bool tune_lookup(const std::string& key, EdtConfig* cfg, float* ms);

@@ -77,6 +77,7 @@ PROTOTYPES = {
     "gvx_dvm_edt": [_vp, _u32, _u32, _u32, _vp],
     "gvx_dvm_edt_pass": [_vp, ctypes.c_int, _vp],
     "gvx_dvm_edt_check": [_vp, ctypes.POINTER(_u32)],
+    "gvx_dvm_voxelize_edt": [_vp, _vp, _u64, _vp, _vp],
     "gvx_dvm_autotune": [_vp, ctypes.c_int, ctypes.POINTER(EdtConfig), _vp],
     "gvx_dvm_set_edt_config": [_vp, ctypes.POINTER(EdtConfig)],
     "gvx_dvm_edt_static_workspace": [_vp, ctypes.POINTER(Dims), _vp],
@@ -95,6 +96,7 @@ PROTOTYPES = {
     "gvx_batch_insert_points": [_vp, _vp, _vp, _u64, _vp],
     "gvx_batch_edt": [_vp, _vp],
     "gvx_batch_edt_check": [_vp, ctypes.POINTER(_u32)],
+    "gvx_batch_voxelize_edt": [_vp, _vp, _vp, _u64, _vp],
     "gvx_batch_autotune": [_vp, ctypes.c_int, ctypes.POINTER(EdtConfig), _vp],
     "gvx_batch_query_trilinear": [_vp, _vp, _vp, _u64, _vp, _vp, _vp],
     "gvx_batch_graph_capture": [_vp, _vp, _vp, _u64, _vp, _vp, _u64, _vp, _vp, _vp],

@@ -42,6 +42,10 @@ class Batch:
     def edt(self) -> None:
         call("gvx_batch_edt", self._h, _stream())
 
+    def voxelize_edt(self, xyz: torch.Tensor, offsets: torch.Tensor) -> None:
+        """clear + insert + edt in one call (same result)."""
+        call("gvx_batch_voxelize_edt", self._h, _ptr(xyz), _ptr(offsets), xyz.shape[0], _stream())
+
     def autotune(self, force: bool = False) -> dict:
         """Pick the fastest sweep configuration of the batched EDT (the maps'
         content is saved and restored around the timing runs)."""

@@ -98,6 +98,11 @@ class DistanceVoxelMap:
         p = _dev_points(points)
         call("gvx_dvm_insert_points", self._h, _ptr(p), p.shape[0], _ptr(outside), _stream())
 
+    def voxelize_edt(self, points, outside: Optional[torch.Tensor] = None) -> None:
+        """clearMap + insertPointCloud + parallelBanding3D in one call (same result)."""
+        p = _dev_points(points)
+        call("gvx_dvm_voxelize_edt", self._h, _ptr(p), p.shape[0], _ptr(outside), _stream())
+
     def parallelBanding3D(self, m1: int = 1, m2: int = 1, m3: int = 1, *unused) -> None:
         call("gvx_dvm_edt", self._h, m1, m2, m3, _stream())
 

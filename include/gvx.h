@@ -88,6 +88,14 @@ GVX_API gvx_status gvx_dvm_insert_points(gvx_dvm *m, const float *d_xyz, uint64_
  * reference with band counts (1,1,1).  The band counts are accepted for
  * API compatibility; results never depend on them. */
 GVX_API gvx_status gvx_dvm_edt(gvx_dvm *m, uint32_t m1, uint32_t m2, uint32_t m3, gvx_stream stream);
+/* clearMap + insertPointCloud + parallelBanding3D in one call, with the same
+ * result (and the same outside flag) as the three calls in a row
+ * (TemplateVoxelMap.hpp:244-271, :665-709; DistanceVoxelMap.hpp:284-645).
+ * The points are recorded as occupancy bits in the map's workspace and the
+ * z sweep builds the map from them, so the map is written once instead of
+ * cleared, scattered and re-read.  No counterpart in the reference. */
+GVX_API gvx_status gvx_dvm_voxelize_edt(gvx_dvm *m, const float *d_xyz, uint64_t n, uint32_t *d_outside,
+                                        gvx_stream stream);
 /* One stage of the EDT, for per-pass timing and tests: 0 = the z sweep,
  * 1 = the y sweep, 2 = the x sweep (one launch each), 3 = the y and x sweeps
  * as the single fused launch gvx_dvm_edt uses (0 then 3 == gvx_dvm_edt;
@@ -207,6 +215,10 @@ GVX_API gvx_status gvx_batch_insert_points(gvx_batch *b, const float *d_xyz, con
 /* EDT of every map, bit-identical to gvx_dvm_edt per map: one launch for the
  * z sweeps of all maps, one fused launch for their y and x sweeps. */
 GVX_API gvx_status gvx_batch_edt(gvx_batch *b, gvx_stream stream);
+/* gvx_batch_clear + gvx_batch_insert_points + gvx_batch_edt in one call, as
+ * gvx_dvm_voxelize_edt per map (this is what a captured graph records). */
+GVX_API gvx_status gvx_batch_voxelize_edt(gvx_batch *b, const float *d_xyz, const uint64_t *d_offsets,
+                                          uint64_t n_total, gvx_stream stream);
 /* As gvx_dvm_edt_check, for the last gvx_batch_edt. */
 GVX_API gvx_status gvx_batch_edt_check(gvx_batch *b, uint32_t *flags);
 /* As gvx_dvm_autotune for the batched EDT (rows per staging chunk; the batch

@@ -79,3 +79,16 @@ def test_batch_graph_replay_matches_eager():
     for k in range(len(maps)):
         assert np.array_equal(to_u32(maps[k].data()), eager_maps[k])
     assert torch.equal(dist, d_eager) and torch.equal(grad, g_eager)
+
+
+def test_batch_voxelize_edt_equals_clear_insert_edt():
+    scenes = _scenes(6, seed=11)
+    maps_a = [gvx.DistanceVoxelMap(d, s) for d, s, _ in scenes]
+    maps_b = [gvx.DistanceVoxelMap(d, s) for d, s, _ in scenes]
+    pts, offs = _cat(scenes)
+    a, b = Batch(maps_a), Batch(maps_b)
+    a.clear(); a.insert(pts, offs); a.edt()
+    b.voxelize_edt(pts, offs)
+    assert b.edt_check() == 0
+    for ma, mb in zip(maps_a, maps_b):
+        assert torch.equal(ma.data(), mb.data())

@@ -138,3 +138,58 @@ def test_sqdist_out_of_range_ids_are_guarded():
     ids = torch.tensor([0, 16 ** 3 - 1, 16 ** 3, 2 ** 31], dtype=torch.int64)
     out = dvm.getSquaredDistances(ids).cpu().numpy()
     assert out[0] == 3 and out[2] == 2147483647 and out[3] == 2147483647
+
+
+def _walls(dims, seed):
+    """Points on planes parallel to z: many columns hold more sites than pass
+    Z's on-chip ring, plus scattered points."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z = dims
+    pts = [np.stack([np.full(Z, 3.5), np.full(Z, 5.5), np.arange(Z) + 0.5], 1)]
+    for _ in range(4):
+        x = rng.integers(0, X)
+        ys, zs = np.meshgrid(np.arange(rng.integers(0, Y // 2), Y), np.arange(Z // 3, Z), indexing="ij")
+        pts.append(np.stack([np.full(ys.size, x + 0.5), ys.ravel() + 0.5, zs.ravel() + 0.5], 1))
+    pts.append(rng.random((500, 3)) * np.asarray(dims))
+    return np.concatenate(pts).astype(np.float32)
+
+
+@pytest.mark.parametrize("dims", [(70, 40, 90), (64, 64, 200), (33, 17, 1023)])
+def test_edt_dense_columns(dims):
+    _check(dims, 1.0, _walls(dims, sum(dims)))
+
+
+@pytest.mark.parametrize("case", ["random", "walls", "c1", "outside"])
+def test_voxelize_edt_equals_clear_insert_edt(case):
+    dims = {"random": (96, 40, 70), "walls": (70, 40, 90), "c1": (128, 128, 128), "outside": (40, 44, 48)}[case]
+    if case == "random":
+        pts = (np.random.default_rng(1).random((3000, 3)) * np.asarray(dims)).astype(np.float32)
+        side = 1.0
+    elif case == "walls":
+        pts, side = _walls(dims, 3), 1.0
+    elif case == "c1":
+        sc = workloads.c1_scene()
+        pts, side = sc.points, sc.side
+    else:  # negative, NaN and beyond-the-map coordinates: the outside flag and voxel 0
+        rng = np.random.default_rng(2)
+        pts = (rng.random((400, 3)) * 1.4 - 0.2) * np.asarray(dims)
+        pts[:5] = np.nan
+        pts = pts.astype(np.float32)
+        side = 1.0
+    _, want = oracle_edt(dims, side, pts)
+    p = torch.as_tensor(pts).cuda()
+    a = gvx.DistanceVoxelMap(dims, side)
+    b = gvx.DistanceVoxelMap(dims, side)
+    fa = torch.zeros(1, dtype=torch.int32, device="cuda")
+    fb = torch.zeros(1, dtype=torch.int32, device="cuda")
+    a.clearMap()
+    a.insertPointCloud(p, outside=fa)
+    a.parallelBanding3D()
+    b.insertPointCloud(torch.as_tensor(np.random.default_rng(9).random((100, 3)) * np.asarray(dims) * side,
+                                       dtype=torch.float32).cuda())
+    b.parallelBanding3D()  # stale content that the fused call must not depend on
+    b.voxelize_edt(p, outside=fb)
+    assert b.edt_check() == 0
+    assert torch.equal(a.data(), b.data())
+    assert int(fa.item()) == int(fb.item())
+    assert np.array_equal(to_u32(b.data()), want)
