@@ -322,6 +322,66 @@ gvx_status gvx_bvm_collide(gvx_bvm* self, const gvx_bvm* other, const int32_t of
                      "collideWith(BitVectorVoxelMap)");
 }
 
+/* ---- ProbVoxelMap ------------------------------------------------------ */
+
+gvx_status gvx_pvm_create(const gvx_dims* dims, float voxel_side, gvx_pvm** out) {
+  if (out == nullptr) return fail(GVX_ERR_INVALID_ARG, "out is null");
+  *out = nullptr;
+  gvx_status st = check_dims(dims);
+  if (st != GVX_OK) return st;
+  if (!(voxel_side > 0.0f)) return fail(GVX_ERR_INVALID_ARG, "voxel side must be > 0");
+  gvx_pvm* m = new (std::nothrow) gvx_pvm{*dims, voxel_side, nullptr};
+  if (m == nullptr) return fail(GVX_ERR_OOM, "host allocation failed");
+  const uint64_t bytes = (num_voxels(*dims) + 15) / 16 * 16;
+  cudaError_t e = cudaMalloc(&m->d_vox, bytes);
+  if (e == cudaSuccess) e = cudaMemset(m->d_vox, 0x80, bytes);  // UNKNOWN_PROBABILITY
+  if (e != cudaSuccess) {
+    if (m->d_vox) cudaFree(m->d_vox);
+    delete m;
+    return cuda_status(e, "cudaMalloc(ProbVoxelMap)");
+  }
+  *out = m;
+  return GVX_OK;
+}
+
+gvx_status gvx_pvm_destroy(gvx_pvm* m) {
+  if (m == nullptr) return GVX_OK;
+  cudaError_t e = m->d_vox ? cudaFree(m->d_vox) : cudaSuccess;
+  delete m;
+  return cuda_status(e, "cudaFree(ProbVoxelMap)");
+}
+
+gvx_status gvx_pvm_info(const gvx_pvm* m, gvx_dims* dims, float* voxel_side, int8_t** d_voxels) {
+  if (m == nullptr) return fail(GVX_ERR_INVALID_ARG, "map is null");
+  if (dims) *dims = m->dims;
+  if (voxel_side) *voxel_side = m->side;
+  if (d_voxels) *d_voxels = m->d_vox;
+  return GVX_OK;
+}
+
+gvx_status gvx_pvm_clear(gvx_pvm* m, gvx_stream stream) {
+  if (m == nullptr) return fail(GVX_ERR_INVALID_ARG, "map is null");
+  return cuda_status(cudaMemsetAsync(m->d_vox, 0x80, num_voxels(m->dims), as_stream(stream)), "clearMap(ProbVoxelMap)");
+}
+
+gvx_status gvx_pvm_insert_points(gvx_pvm* m, const float* d_xyz, uint64_t n, uint32_t meaning, uint32_t* d_outside,
+                                 gvx_stream stream) {
+  if (m == nullptr || (n > 0 && d_xyz == nullptr)) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (meaning > 255) return fail(GVX_ERR_INVALID_ARG, "meaning must be in [0, 255]");
+  return cuda_status(launch_pvm_insert(m->d_vox, m->dims, m->side, d_xyz, n, meaning, d_outside, as_stream(stream)),
+                     "insertPointCloud(ProbVoxelMap)");
+}
+
+gvx_status gvx_dvm_merge_occupied(gvx_dvm* m, const gvx_pvm* other, const uint32_t offset[3], float occupancy_threshold,
+                                  gvx_stream stream) {
+  if (m == nullptr || other == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(m->dims, other->dims)) return fail(GVX_ERR_INVALID_ARG, "maps differ in dimensions");
+  const uint32_t zero[3] = {0, 0, 0};
+  return cuda_status(launch_merge_occupied(m->d_vox, other->d_vox, m->dims, offset ? offset : zero, occupancy_threshold,
+                                           as_stream(stream)),
+                     "mergeOccupied");
+}
+
 /* ---- BitVectorVoxelList ------------------------------------------------ */
 
 gvx_status gvx_blist_create(const gvx_dims* ref_dims, float voxel_side, gvx_blist** out) {

@@ -56,6 +56,12 @@ struct gvx_bvm {
   uint8_t* d_vox;
 };
 
+struct gvx_pvm {
+  gvx_dims dims;
+  float side;
+  int8_t* d_vox;  // one occupancy byte per voxel, allocation rounded up to 16 bytes
+};
+
 struct gvx_blist {
   gvx_dims ref;
   float side;
@@ -145,6 +151,11 @@ cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems&
 bool tune_lookup(const std::string& key, EdtConfig* cfg, float* ms);
 void tune_store(const std::string& key, const EdtConfig& cfg, float ms);
 std::string tune_device_name();
+cudaError_t launch_pvm_insert(int8_t* d_vox, gvx_dims d, float side, const float* d_xyz, uint64_t n, uint32_t meaning,
+                              uint32_t* d_outside, cudaStream_t s);
+cudaError_t launch_merge_occupied(uint32_t* d_dvm, const int8_t* d_pvm, gvx_dims d, const uint32_t off[3], float threshold,
+                                  cudaStream_t s);
+int prob_threshold(float val);
 cudaError_t launch_dvm_sqdist(const uint32_t* d_vox, gvx_dims d, const uint32_t* d_ids, uint64_t n, int32_t* d_out,
                               int mode, cudaStream_t s);
 cudaError_t launch_dvm_sqdist_map(const uint32_t* d_vox, gvx_dims d, int32_t* d_out, cudaStream_t s);

@@ -11,6 +11,7 @@ from .maps import (  # noqa: F401
     BitVectorVoxelList,
     BitVectorVoxelMap,
     DistanceVoxelMap,
+    ProbVoxelMap,
     eBVM_COLLISION,
     eBVM_FREE,
     eBVM_OCCUPIED,
@@ -25,6 +26,7 @@ __all__ = [
     "DistanceVoxelMap",
     "BitVectorVoxelMap",
     "BitVectorVoxelList",
+    "ProbVoxelMap",
     "lists_collide_map",
     "make_arm",
     "BIT_VECTOR_LENGTH",

@@ -98,6 +98,11 @@ class DistanceVoxelMap:
         p = _dev_points(points)
         call("gvx_dvm_insert_points", self._h, _ptr(p), p.shape[0], _ptr(outside), _stream())
 
+    def mergeOccupied(self, other: "ProbVoxelMap", voxel_offset=(0, 0, 0), occupancy_threshold: float = 0.5) -> None:
+        """Voxels of `other` above the threshold become sites (own coordinates + offset)."""
+        off = (ctypes.c_uint32 * 3)(*[int(v) & 0xFFFFFFFF for v in voxel_offset])
+        call("gvx_dvm_merge_occupied", self._h, other.handle, off, float(occupancy_threshold), _stream())
+
     def voxelize_edt(self, points, outside: Optional[torch.Tensor] = None) -> None:
         """clearMap + insertPointCloud + parallelBanding3D in one call (same result)."""
         p = _dev_points(points)
@@ -215,6 +220,53 @@ def _device_view_u8(ptr: int, n: int) -> torch.Tensor:
         __cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3}
 
     return torch.as_tensor(_CAI(), device="cuda")
+
+
+def _device_view_i8(ptr: int, n: int) -> torch.Tensor:
+    class _CAI:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "|i1", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_CAI(), device="cuda")
+
+
+class ProbVoxelMap:
+    """ProbVoxelMap (GV/voxelmap/ProbVoxelMap.h): one int8 occupancy per voxel
+    (-128 unknown, -127..127 log-odds-like probability)."""
+
+    def __init__(self, dims: Sequence[int], voxel_side_length: float):
+        self.dims = tuple(int(d) for d in dims)
+        self.voxel_side_length = float(voxel_side_length)
+        h = ctypes.c_void_p()
+        call("gvx_pvm_create", ctypes.byref(Dims(*self.dims)), self.voxel_side_length, ctypes.byref(h))
+        self._h = h
+        self._destroy = _abi.lib().gvx_pvm_destroy
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            getattr(self, "_destroy", None) and self._destroy(h)
+            self._h = None
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    @property
+    def size(self) -> int:
+        return self.dims[0] * self.dims[1] * self.dims[2]
+
+    def data(self) -> torch.Tensor:
+        """Borrowed int8 CUDA view of the occupancies."""
+        d, s, p = Dims(), ctypes.c_float(), ctypes.c_void_p()
+        call("gvx_pvm_info", self._h, ctypes.byref(d), ctypes.byref(s), ctypes.byref(p))
+        return _device_view_i8(p.value, self.size)
+
+    def clearMap(self) -> None:
+        call("gvx_pvm_clear", self._h, _stream())
+
+    def insertPointCloud(self, points, meaning: int = eBVM_OCCUPIED, outside: Optional[torch.Tensor] = None) -> None:
+        p = _dev_points(points)
+        call("gvx_pvm_insert_points", self._h, _ptr(p), p.shape[0], int(meaning), _ptr(outside), _stream())
 
 
 class BitVectorVoxelMap:

@@ -61,6 +61,42 @@ struct DeviceArray {
 // ---------------------------------------------------------------------------
 namespace voxelmap {
 
+ProbVoxelMap::ProbVoxelMap(const Vector3ui dim, const float voxel_side_length, const MapType map_type)
+    : GpuVoxelsMap(map_type, dim, voxel_side_length) {
+  gvx_dims d = to_dims(dim);
+  require(gvx_pvm_create(&d, voxel_side_length, &m_handle), "ProbVoxelMap");
+}
+
+ProbVoxelMap::~ProbVoxelMap() { gvx_pvm_destroy(m_handle); }
+
+void ProbVoxelMap::clearMap() {
+  lock_guard g(m_mutex);
+  ok(gvx_pvm_clear(m_handle, nullptr), "clearMap");
+  cudaDeviceSynchronize();
+}
+
+void ProbVoxelMap::insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  DevicePoints d(points);
+  insertPointCloud(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size(), voxel_meaning);
+  cudaDeviceSynchronize();
+}
+
+void ProbVoxelMap::insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  ok(gvx_pvm_insert_points(m_handle, reinterpret_cast<const float*>(d_points), size, (uint32_t)voxel_meaning, nullptr,
+                           nullptr),
+     "insertPointCloud");
+}
+
+size_t ProbVoxelMap::getMemoryUsage() const { return getVoxelMapSize(); }
+
+Probability* ProbVoxelMap::getDeviceDataPtr() {
+  int8_t* p = nullptr;
+  gvx_pvm_info(m_handle, nullptr, nullptr, &p);
+  return p;
+}
+
 DistanceVoxelMap::DistanceVoxelMap(const Vector3ui dim, const float voxel_side_length, const MapType map_type)
     : GpuVoxelsMap(map_type, dim, voxel_side_length) {
   gvx_dims d = to_dims(dim);
@@ -104,6 +140,18 @@ void DistanceVoxelMap::parallelBanding3D(uint32_t m1, uint32_t m2, uint32_t m3, 
   lock_guard g(m_mutex);
   ok(gvx_dvm_edt(m_handle, m1, m2, m3, nullptr), "parallelBanding3D");
   cudaDeviceSynchronize();  // the reference returns with the EDT complete
+}
+
+bool DistanceVoxelMap::mergeOccupied(const std::shared_ptr<ProbVoxelMap> other, const Vector3ui& voxel_offset,
+                                     float occupancy_threshold) {
+  if (!other) return false;
+  std::lock(m_mutex, other->mutexRef());
+  lock_guard g1(m_mutex, std::adopt_lock);
+  std::lock_guard<std::recursive_timed_mutex> g2(other->mutexRef(), std::adopt_lock);
+  const uint32_t off[3] = {voxel_offset.x, voxel_offset.y, voxel_offset.z};
+  const bool r = ok(gvx_dvm_merge_occupied(m_handle, other->handle(), off, occupancy_threshold, nullptr), "mergeOccupied");
+  cudaDeviceSynchronize();
+  return r;
 }
 
 void DistanceVoxelMap::getSquaredDistances(const uint32_t* b, const uint32_t* e, int32_t* out) {
@@ -386,6 +434,7 @@ bool GpuVoxels::addMap(const MapType map_type, const std::string& map_name) {
       case MT_DISTANCE_VOXELMAP: map.reset(new voxelmap::DistanceVoxelMap(m_dim, m_voxel_side_length, map_type)); break;
       case MT_BITVECTOR_VOXELMAP: map.reset(new BitVectorVoxelMap(m_dim, m_voxel_side_length, map_type)); break;
       case MT_BITVECTOR_VOXELLIST: map.reset(new BitVectorVoxelList(m_dim, m_voxel_side_length, map_type)); break;
+      case MT_PROBAB_VOXELMAP: map.reset(new voxelmap::ProbVoxelMap(m_dim, m_voxel_side_length, map_type)); break;
       default:
         std::fprintf(stderr, "gpu_voxels: map type %d is outside the distance-field collision path\n", (int)map_type);
         return false;

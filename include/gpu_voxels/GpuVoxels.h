@@ -16,6 +16,7 @@
 #include "voxellist/BitVoxelList.h"
 #include "voxelmap/BitVoxelMap.h"
 #include "voxelmap/DistanceVoxelMap.h"
+#include "voxelmap/ProbVoxelMap.h"
 
 namespace gpu_voxels {
 

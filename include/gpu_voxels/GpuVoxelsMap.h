@@ -39,6 +39,8 @@ class GpuVoxelsMap {
   virtual void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) = 0;
   // Number of bytes of device memory held by the map.
   virtual size_t getMemoryUsage() const = 0;
+  // The map's lock, for operations that lock two maps together.
+  std::recursive_timed_mutex& mutexRef() const { return m_mutex; }
 
  protected:
   typedef std::lock_guard<std::recursive_timed_mutex> lock_guard;

@@ -17,6 +17,10 @@ enum BitVoxelMeaning {
   eBVM_UNKNOWN = 3,
   eBVM_SWEPT_VOLUME_START = 4,
   eBVM_SWEPT_VOLUME_END = 254,
+  // the swept-volume range read as occupancy probabilities by ProbVoxelMap
+  eBVM_MAX_FREE_PROB = 4,
+  eBVM_UNCERTAIN_OCC_PROB = 129,
+  eBVM_MAX_OCC_PROB = 254,
   eBVM_UNDEFINED = 255
 };
 

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../GpuVoxelsMap.h"
+#include "ProbVoxelMap.h"
 
 struct gvx_dvm;
 
@@ -64,6 +65,12 @@ class DistanceVoxelMap : public GpuVoxelsMap {
                          uint32_t m1_blocksize = PBA_DEFAULT_M1_BLOCK_SIZE,
                          uint32_t m2_blocksize = PBA_DEFAULT_M2_BLOCK_SIZE,
                          uint32_t m3_blocksize = PBA_DEFAULT_M3_BLOCK_SIZE, bool detailtimer = false);
+
+  // mergeOccupied (GV/voxelmap/DistanceVoxelMap.hpp:109-136): voxels of `other`
+  // whose occupancy exceeds the threshold become sites (own coordinates +
+  // voxel_offset).  Returns false when the maps' dims differ.
+  bool mergeOccupied(const std::shared_ptr<ProbVoxelMap> other, const Vector3ui& voxel_offset = Vector3ui(),
+                     float occupancy_threshold = 0.5f);
 
   // Queries at linear voxel ids (device pointers; [begin, end) ids -> out).
   void getSquaredDistances(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, int32_t* dev_output);

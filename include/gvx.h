@@ -49,6 +49,7 @@ typedef struct gvx_dims { uint32_t x, y, z; } gvx_dims;
 /* Opaque handles. */
 typedef struct gvx_dvm gvx_dvm;   /* DistanceVoxelMap */
 typedef struct gvx_bvm gvx_bvm;   /* BitVectorVoxelMap (BitVoxelMap<256>) */
+typedef struct gvx_pvm gvx_pvm;   /* ProbVoxelMap (int8 occupancy per voxel) */
 typedef struct gvx_blist gvx_blist; /* BitVectorVoxelList */
 
 typedef void *gvx_stream; /* cudaStream_t */
@@ -259,6 +260,33 @@ GVX_API gvx_status gvx_bvm_insert_points(gvx_bvm *m, const float *d_xyz, uint64_
  * uint64) receives the count. */
 GVX_API gvx_status gvx_bvm_collide(gvx_bvm *self, const gvx_bvm *other, const int32_t offset[3], int mark, uint64_t *d_count,
                            gvx_stream stream);
+
+/* ---- ProbVoxelMap (GV/voxelmap/ProbVoxelMap.h) and mergeOccupied -------- */
+
+/* Replaces ProbVoxelMap(dim, side, MT_PROBAB_VOXELMAP) (GV/voxelmap/ProbVoxelMap.hpp:35-39):
+ * one int8 occupancy per voxel (ProbabilisticVoxel, GV/voxel/ProbabilisticVoxel.h),
+ * created UNKNOWN (-128). */
+GVX_API gvx_status gvx_pvm_create(const gvx_dims *dims, float voxel_side, gvx_pvm **out);
+GVX_API gvx_status gvx_pvm_destroy(gvx_pvm *m);
+GVX_API gvx_status gvx_pvm_info(const gvx_pvm *m, gvx_dims *dims, float *voxel_side, int8_t **d_voxels);
+/* Replaces TemplateVoxelMap<ProbabilisticVoxel>::clearMap (GV/voxelmap/TemplateVoxelMap.hpp:222-238). */
+GVX_API gvx_status gvx_pvm_clear(gvx_pvm *m, gvx_stream stream);
+/* Replaces insertPointCloud -> kernelInsertGlobalPointCloud<ProbabilisticVoxel>
+ * (GV/voxelmap/kernels/VoxelMapOperations.hpp:241-264) with
+ * ProbabilisticVoxel::insert (GV/voxel/ProbabilisticVoxel.hpp:44-100): eBVM_FREE
+ * adds -10, eBVM_OCCUPIED/COLLISION +72, meanings 4..254 add meaning - 129,
+ * UNKNOWN/UNDEFINED reset to -128; an UNKNOWN voxel starts from 0; sums
+ * saturate at [-127, 127].  Every point's update is applied (the reference's
+ * non-atomic update can drop some when points share a voxel). */
+GVX_API gvx_status gvx_pvm_insert_points(gvx_pvm *m, const float *d_xyz, uint64_t n, uint32_t meaning,
+                                         uint32_t *d_outside, gvx_stream stream);
+/* Replaces DistanceVoxelMap::mergeOccupied(prob_map, offset, threshold)
+ * (GV/voxelmap/DistanceVoxelMap.hpp:109-136, GV/voxelmap/DistanceVoxelMap.h:92-134):
+ * every voxel whose occupancy exceeds floatToProbability(threshold) gets the
+ * site of its own coordinates plus `offset` (NULL = 0); other voxels keep
+ * their value.  The maps must have equal dims (the reference does not check). */
+GVX_API gvx_status gvx_dvm_merge_occupied(gvx_dvm *m, const gvx_pvm *other, const uint32_t offset[3],
+                                          float occupancy_threshold, gvx_stream stream);
 
 /* ---- BitVectorVoxelList (GV/voxellist/BitVoxelList.h) ------------------- */
 

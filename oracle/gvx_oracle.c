@@ -558,3 +558,71 @@ void orc_list_insert(uint32_t *ids_io, uint8_t *voxels_io, uint64_t *n_io, const
   free(keys);
   free(vox);
 }
+
+/* ------------------------------------------------------------------------ */
+/* ProbVoxelMap and DistanceVoxelMap::mergeOccupied                          */
+/* ------------------------------------------------------------------------ */
+
+/* ProbabilisticVoxel::insert -> updateOccupancy, GV/voxel/ProbabilisticVoxel.hpp:44-100,
+ * constants GV/helpers/common_defines.h:154-161 (UNKNOWN -128, MIN -127,
+ * MAX 127, sensor model free -10 / occupied 72) and the meaning ranges
+ * GV/helpers/common_defines.h:50-63. */
+static int8_t prob_update(int8_t cur, uint32_t meaning) {
+  int delta;
+  switch (meaning) {
+    case 0: delta = -10; break;          /* eBVM_FREE */
+    case 1: case 2: delta = 72; break;   /* eBVM_OCCUPIED, eBVM_COLLISION */
+    case 3: case 255: return -128;       /* eBVM_UNKNOWN, eBVM_UNDEFINED */
+    default:
+      if (meaning >= 4 && meaning <= 254) { delta = (int)meaning - 129; break; }
+      return -128;
+  }
+  if (cur == -128) return (int8_t)delta;
+  int v = (int)cur + delta;
+  if (v < -127) v = -127;
+  if (v > 127) v = 127;
+  return (int8_t)v;
+}
+
+/* kernelInsertGlobalPointCloud<ProbabilisticVoxel>, GV/voxelmap/kernels/VoxelMapOperations.hpp:241-264:
+ * every point applies its update to its voxel, one after the other (the
+ * reference's device update is not atomic and can lose updates when points
+ * share a voxel; all updates of one call are the same monotone saturating
+ * step, so applying each of them gives one order-independent result). */
+int orc_pvm_insert(int8_t *map, const uint32_t d[3], float side, const float *xyz, uint64_t n, uint32_t meaning) {
+  int outside = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    uint32_t x = orc_coord_to_voxel(xyz[3 * i + 0], side);
+    uint32_t y = orc_coord_to_voxel(xyz[3 * i + 1], side);
+    uint32_t z = orc_coord_to_voxel(xyz[3 * i + 2], side);
+    if (x < d[0] && y < d[1] && z < d[2]) {
+      uint64_t id = (uint64_t)z * d[0] * d[1] + (uint64_t)y * d[0] + x;
+      map[id] = prob_update(map[id], meaning);
+    } else {
+      outside = 1;
+    }
+  }
+  return outside;
+}
+
+/* ProbabilisticVoxel::floatToProbability, GV/voxel/ProbabilisticVoxel.h:40-45 */
+int orc_float_to_probability(float val) {
+  float tmp = val < 1.0f ? val : 1.0f;
+  tmp = tmp > 0.0f ? tmp : 0.0f;
+  tmp = (tmp * (127.0f - (-127.0f))) + (-127.0f);
+  return (int)(int8_t)tmp;
+}
+
+/* DistanceVoxelMap::mergeOccupied, GV/voxelmap/DistanceVoxelMap.hpp:109-136 with
+ * mergeOccupiedOperator / probVoxelOccupied, GV/voxelmap/DistanceVoxelMap.h:92-134:
+ * voxel i whose occupancy exceeds the threshold gets the site of its own
+ * coordinates plus the offset, packed with 32-bit wrap-around. */
+void orc_dvm_merge_occupied(uint32_t *dvm, const int8_t *pvm, const uint32_t d[3], const uint32_t off[3], float thr) {
+  const int t = orc_float_to_probability(thr);
+  const uint64_t n = (uint64_t)d[0] * d[1] * d[2];
+  for (uint64_t i = 0; i < n; ++i) {
+    if ((int)pvm[i] <= t) continue;
+    uint32_t x = (uint32_t)(i % d[0]), y = (uint32_t)((i / d[0]) % d[1]), z = (uint32_t)(i / ((uint64_t)d[0] * d[1]));
+    dvm[i] = (x + off[0]) | ((y + off[1]) << 10) | ((z + off[2]) << 20);
+  }
+}

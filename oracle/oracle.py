@@ -78,6 +78,12 @@ def lib():
         L.orc_list_collide_list.restype = ctypes.c_uint64
         L.orc_list_insert.argtypes = [_u32p, _u8p, ctypes.POINTER(ctypes.c_uint64), _u32p, ctypes.c_float, _f32p,
                                       ctypes.c_uint64, ctypes.c_uint32]
+        _i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+        L.orc_pvm_insert.argtypes = [_i8p, _u32p, ctypes.c_float, _f32p, ctypes.c_uint64, ctypes.c_uint32]
+        L.orc_pvm_insert.restype = ctypes.c_int
+        L.orc_float_to_probability.argtypes = [ctypes.c_float]
+        L.orc_float_to_probability.restype = ctypes.c_int
+        L.orc_dvm_merge_occupied.argtypes = [_u32p, _i8p, _u32p, _u32p, ctypes.c_float]
         L.orc_num_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -240,6 +246,24 @@ def list_insert(ids, vox, dims, side, xyz, meaning):
 
 
 # ---- FP64 continuous queries ------------------------------------------------
+
+def pvm_empty(dims) -> np.ndarray:
+    """ProbVoxelMap after clearMap: every voxel UNKNOWN (-128)."""
+    return np.full(int(np.prod(dims)), -128, dtype=np.int8)
+
+
+def pvm_insert(pmap: np.ndarray, dims, side: float, xyz, meaning: int) -> bool:
+    p = _pts(xyz)
+    return bool(lib().orc_pvm_insert(pmap, _dims(dims), np.float32(side), p, p.shape[0], int(meaning)))
+
+
+def float_to_probability(val: float) -> int:
+    return int(lib().orc_float_to_probability(float(val)))
+
+
+def dvm_merge_occupied(vmap: np.ndarray, pmap: np.ndarray, dims, offset=(0, 0, 0), threshold: float = 0.5) -> None:
+    lib().orc_dvm_merge_occupied(vmap, pmap, _dims(dims), np.asarray(offset, dtype=np.uint32), float(threshold))
+
 
 def decode_sites(vmap: np.ndarray):
     v = vmap.astype(np.int64)

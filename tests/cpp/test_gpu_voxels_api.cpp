@@ -156,11 +156,38 @@ static void collisions() {
   gvl->delMap("b");
 }
 
+// The reference's ProbMap2DistMap example (EX/ProbMap2DistMap.cpp:60-95): two
+// overlapping cubes inserted into a ProbVoxelMap with maximal occupied and
+// free probability; voxels above 0.55 merged into a DistanceVoxelMap.
+static void prob_map_to_distance_map() {
+  GpuVoxelsSharedPtr gvl = GpuVoxels::getInstance();
+  gvl->initialize(128, 128, 128, 1.0f);
+  CHECK(gvl->addMap(MT_PROBAB_VOXELMAP, "myProbVoxelMap"), "addMap(MT_PROBAB_VOXELMAP)");
+  gvl->addMap(MT_DISTANCE_VOXELMAP, "myDistanceMap");
+  ProbVoxelMapSharedPtr prob(gvl->getMap("myProbVoxelMap"), gvl->getMap("myProbVoxelMap")->as<voxelmap::ProbVoxelMap>());
+  DistanceVoxelMapSharedPtr dist(gvl->getMap("myDistanceMap"),
+                                 gvl->getMap("myDistanceMap")->as<voxelmap::DistanceVoxelMap>());
+  prob->insertPointCloud(box_of_points(Vector3f(40, 40, 40), Vector3f(60, 60, 60), 0.9f), eBVM_MAX_OCC_PROB);
+  prob->insertPointCloud(box_of_points(Vector3f(50, 50, 50), Vector3f(70, 70, 70), 0.9f), eBVM_MAX_FREE_PROB);
+  CHECK(dist->mergeOccupied(prob, Vector3ui(0, 0, 0), 0.55f), "mergeOccupied");
+  std::vector<DistanceVoxel> host(dist->getVoxelMapSize());
+  cudaMemcpy(host.data(), dist->getDeviceDataPtr(), host.size() * sizeof(DistanceVoxel), cudaMemcpyDeviceToHost);
+  size_t sites = 0;
+  for (const DistanceVoxel& v : host) sites += v.raw() != 0x3FFFFFFFu;
+  CHECK(sites == 20 * 20 * 20 - 10 * 10 * 10, "mergeOccupied: box 1 minus the overlap (7000 sites)");
+  dist->parallelBanding3D();
+  // the voxel at (30,30,30) is nearest to the cube's corner (40,40,40): 3 * 10^2
+  CHECK(dist->getSquaredObstacleDistance(30, 30, 30) == 300, "EDT after mergeOccupied: corner distance 300");
+  gvl->delMap("myProbVoxelMap");
+  gvl->delMap("myDistanceMap");
+}
+
 int main() {
   GpuVoxels::getInstance();
   distance_extraction();
   distance_correctness();
   collisions();
+  prob_map_to_distance_map();
   std::printf("%d failure(s)\n", g_failures);
   return g_failures;
 }
