@@ -596,6 +596,44 @@ gvx_status gvx_blist_set(gvx_blist* l, const uint32_t* d_ids, const uint8_t* d_v
   return GVX_OK;
 }
 
+gvx_status gvx_dvm_extract_distances(const gvx_dvm* m, int8_t* d_out, int robot_radius, gvx_stream stream) {
+  if (m == nullptr || d_out == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  return cuda_status(launch_extract_distances(m->d_vox, m->dims, robot_radius, d_out, as_stream(stream)), "extract_distances");
+}
+
+gvx_status gvx_dvm_init_floodfill(const gvx_dvm* m, const int8_t* d_distances, int16_t* d_manhattan, int robot_radius,
+                                  gvx_stream stream) {
+  if (m == nullptr || d_distances == nullptr || d_manhattan == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  return cuda_status(launch_init_floodfill(d_distances, d_manhattan, num_voxels(m->dims), robot_radius, as_stream(stream)),
+                     "init_floodfill");
+}
+
+gvx_status gvx_extract_given_distances(const gvx_dvm* m, int min_dist, int max_dist, gvx_blist* result, uint64_t* n_out,
+                                       gvx_stream stream) {
+  if (m == nullptr || result == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(m->dims, result->ref)) return fail(GVX_ERR_INVALID_ARG, "the list's reference dims differ from the map's");
+  if (min_dist < -128 || min_dist > 127 || max_dist < -128 || max_dist > 127)
+    return fail(GVX_ERR_OUT_OF_DOMAIN, "distance bounds are free_space_t (int8) values");
+  cudaStream_t s = as_stream(stream);
+  const uint64_t nt = band_tiles(m->dims);
+  uint32_t* tiles = nullptr;
+  cudaError_t e = cudaMalloc(&tiles, (nt + 1) * sizeof(uint32_t));
+  if (e == cudaSuccess) e = launch_band_count(m->d_vox, m->dims, min_dist, max_dist, tiles, s);
+  uint32_t total = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&total, tiles + nt, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  result->n = 0;
+  if (e == cudaSuccess) e = blist_reserve(result, total, s);
+  if (e == cudaSuccess && total > 0) e = launch_band_write(m->d_vox, m->dims, min_dist, max_dist, tiles, result->d_ids,
+                                                           result->d_vox, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (tiles) cudaFree(tiles);
+  if (e != cudaSuccess) return cuda_status(e, "extract_given_distances");
+  result->n = total;
+  if (n_out) *n_out = total;
+  return GVX_OK;
+}
+
 gvx_status gvx_blist_collide_bvm(gvx_blist* l, const gvx_bvm* map, const int32_t offset[3], int mark, uint64_t* d_count,
                                  gvx_stream stream) {
   if (l == nullptr || map == nullptr || d_count == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");

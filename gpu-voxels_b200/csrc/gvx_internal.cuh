@@ -19,6 +19,8 @@ constexpr uint32_t kUninit = 1023u;              // PBA_UNINITIALISED_COORD
 constexpr uint32_t kDvUninit = 0x3FFFFFFFu;      // all three coordinates uninitialised
 constexpr int32_t kMaxObstacleDistance = 2147483647;  // MAX_OBSTACLE_DISTANCE
 constexpr uint32_t kBitVoxelBytes = 32;
+constexpr int16_t kManhattanUninitialized = 32767;  // MANHATTAN_DISTANCE_UNINITIALIZED (common_defines.h:117)
+constexpr int16_t kManhattanTooClose = 32765;       // MANHATTAN_DISTANCE_TOO_CLOSE (:119)
 constexpr uint32_t kBitVoxelWords = 8;
 constexpr uint32_t kCollisionBit = 2;            // eBVM_COLLISION
 constexpr uint32_t kMaxDim = 1023;
@@ -156,6 +158,14 @@ cudaError_t launch_pvm_insert(int8_t* d_vox, gvx_dims d, float side, const float
 cudaError_t launch_merge_occupied(uint32_t* d_dvm, const int8_t* d_pvm, gvx_dims d, const uint32_t off[3], float threshold,
                                   cudaStream_t s);
 int prob_threshold(float val);
+cudaError_t launch_extract_distances(const uint32_t* d_vox, gvx_dims d, int robot_radius, int8_t* d_out, cudaStream_t s);
+cudaError_t launch_init_floodfill(const int8_t* d_in, int16_t* d_out, uint64_t n, int robot_radius, cudaStream_t s);
+// Distance band -> list: per-tile counts, exclusive tile offsets (+ total at
+// [band_tiles]), then ids and voxels written in id order.
+uint64_t band_tiles(gvx_dims d);
+cudaError_t launch_band_count(const uint32_t* d_vox, gvx_dims d, int mn, int mx, uint32_t* d_tiles, cudaStream_t s);
+cudaError_t launch_band_write(const uint32_t* d_vox, gvx_dims d, int mn, int mx, const uint32_t* d_tiles, uint32_t* d_ids,
+                              uint8_t* d_lvox, cudaStream_t s);
 cudaError_t launch_dvm_sqdist(const uint32_t* d_vox, gvx_dims d, const uint32_t* d_ids, uint64_t n, int32_t* d_out,
                               int mode, cudaStream_t s);
 cudaError_t launch_dvm_sqdist_map(const uint32_t* d_vox, gvx_dims d, int32_t* d_out, cudaStream_t s);

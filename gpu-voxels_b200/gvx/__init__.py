@@ -15,6 +15,7 @@ from .maps import (  # noqa: F401
     eBVM_COLLISION,
     eBVM_FREE,
     eBVM_OCCUPIED,
+    extract_given_distances,
     lists_collide_map,
     make_arm,
 )
@@ -28,6 +29,7 @@ __all__ = [
     "BitVectorVoxelList",
     "ProbVoxelMap",
     "lists_collide_map",
+    "extract_given_distances",
     "make_arm",
     "BIT_VECTOR_LENGTH",
     "eBVM_FREE",

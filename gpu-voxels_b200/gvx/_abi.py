@@ -113,6 +113,9 @@ PROTOTYPES = {
     "gvx_pvm_clear": [_vp, _vp],
     "gvx_pvm_insert_points": [_vp, _vp, _u64, _u32, _vp, _vp],
     "gvx_dvm_merge_occupied": [_vp, _vp, _vp, _f, _vp],
+    "gvx_dvm_extract_distances": [_vp, _vp, ctypes.c_int, _vp],
+    "gvx_dvm_init_floodfill": [_vp, _vp, _vp, ctypes.c_int, _vp],
+    "gvx_extract_given_distances": [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_u64), _vp],
     "gvx_blist_create": [ctypes.POINTER(Dims), _f, ctypes.POINTER(_vp)],
     "gvx_blist_destroy": [_vp],
     "gvx_blist_size": [_vp, ctypes.POINTER(_u64)],

@@ -98,6 +98,18 @@ class DistanceVoxelMap:
         p = _dev_points(points)
         call("gvx_dvm_insert_points", self._h, _ptr(p), p.shape[0], _ptr(outside), _stream())
 
+    def extract_distances(self, robot_radius: int = 0, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """int8 free-space byte per voxel (DistanceVoxelMap::extract_distances)."""
+        out = torch.empty(self.size, dtype=torch.int8, device="cuda") if out is None else out
+        call("gvx_dvm_extract_distances", self._h, _ptr(out), int(robot_radius), _stream())
+        return out
+
+    def init_floodfill(self, distances: torch.Tensor, robot_radius: int) -> torch.Tensor:
+        """int16 per voxel: 32765 where distances <= robot_radius, else 32767."""
+        out = torch.empty(self.size, dtype=torch.int16, device="cuda")
+        call("gvx_dvm_init_floodfill", self._h, _ptr(distances), _ptr(out), int(robot_radius), _stream())
+        return out
+
     def mergeOccupied(self, other: "ProbVoxelMap", voxel_offset=(0, 0, 0), occupancy_threshold: float = 0.5) -> None:
         """Voxels of `other` above the threshold become sites (own coordinates + offset)."""
         off = (ctypes.c_uint32 * 3)(*[int(v) & 0xFFFFFFFF for v in voxel_offset])
@@ -227,6 +239,16 @@ def _device_view_i8(ptr: int, n: int) -> torch.Tensor:
         __cuda_array_interface__ = {"shape": (n,), "typestr": "|i1", "data": (ptr, False), "version": 3}
 
     return torch.as_tensor(_CAI(), device="cuda")
+
+
+def extract_given_distances(dist_map: "DistanceVoxelMap", min_dist: int, max_dist: int,
+                            result: "BitVectorVoxelList") -> int:
+    """distance_map_converter::extract_given_distances: voxels whose free-space
+    byte lies in [min_dist, max_dist] become `result` (blocking; returns the count)."""
+    n = ctypes.c_uint64(0)
+    call("gvx_extract_given_distances", dist_map.handle, int(min_dist), int(max_dist), result.handle, ctypes.byref(n),
+         _stream())
+    return int(n.value)
 
 
 class ProbVoxelMap:

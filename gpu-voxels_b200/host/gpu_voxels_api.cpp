@@ -14,6 +14,7 @@
 #include <string>
 
 #include "../../include/gpu_voxels/GpuVoxels.h"
+#include "../../include/gpu_voxels/helpers_highlevel/DistanceMapConverter.h"
 #include "../../include/gvx.h"
 
 namespace gpu_voxels {
@@ -140,6 +141,20 @@ void DistanceVoxelMap::parallelBanding3D(uint32_t m1, uint32_t m2, uint32_t m3, 
   lock_guard g(m_mutex);
   ok(gvx_dvm_edt(m_handle, m1, m2, m3, nullptr), "parallelBanding3D");
   cudaDeviceSynchronize();  // the reference returns with the EDT complete
+}
+
+void DistanceVoxelMap::extract_distances(free_space_t* dev_distances, int robot_radius) const {
+  lock_guard g(m_mutex);
+  ok(gvx_dvm_extract_distances(m_handle, dev_distances, robot_radius, nullptr), "extract_distances");
+  cudaDeviceSynchronize();
+}
+
+void DistanceVoxelMap::init_floodfill(free_space_t* dev_distances, manhattan_dist_t* dev_manhattan_distances,
+                                      uint32_t robot_radius) {
+  lock_guard g(m_mutex);
+  ok(gvx_dvm_init_floodfill(m_handle, dev_distances, dev_manhattan_distances, (int)robot_radius, nullptr),
+     "init_floodfill");
+  cudaDeviceSynchronize();
 }
 
 bool DistanceVoxelMap::mergeOccupied(const std::shared_ptr<ProbVoxelMap> other, const Vector3ui& voxel_offset,
@@ -483,4 +498,21 @@ void GpuVoxels::getDimensions(Vector3ui& dim) const { dim = m_dim; }
 
 void GpuVoxels::getVoxelSideLength(float& voxel_side_length) const { voxel_side_length = m_voxel_side_length; }
 
+}  // namespace gpu_voxels
+
+// ---------------------------------------------------------------------------
+// distance_map_converter
+// ---------------------------------------------------------------------------
+namespace gpu_voxels {
+namespace distance_map_converter {
+
+size_t extract_given_distances(const voxelmap::DistanceVoxelMap& dist_map, free_space_t min_dist, free_space_t max_dist,
+                               BitVectorVoxelList& result) {
+  uint64_t n = 0;
+  ok(gvx_extract_given_distances(dist_map.handle(), min_dist, max_dist, result.handle(), &n, nullptr),
+     "extract_given_distances");
+  return (size_t)n;
+}
+
+}  // namespace distance_map_converter
 }  // namespace gpu_voxels

@@ -44,6 +44,12 @@ static const uint32_t PBA_DEFAULT_M2_BLOCK_SIZE = 64;
 static const uint32_t PBA_DEFAULT_M3_BLOCK_SIZE = 16;
 
 typedef uint32_t MapVoxelID;
+// free-space byte and flood-fill distance types (GV/voxel/DistanceVoxel.h:149,203)
+typedef int8_t free_space_t;
+typedef int16_t manhattan_dist_t;
+static const int MANHATTAN_DISTANCE_UNINITIALIZED = 32767;  // SHRT_MAX
+static const int MANHATTAN_DISTANCE_START = MANHATTAN_DISTANCE_UNINITIALIZED - 1;
+static const int MANHATTAN_DISTANCE_TOO_CLOSE = MANHATTAN_DISTANCE_UNINITIALIZED - 2;
 
 namespace voxelmap {
 class DistanceVoxelMap;

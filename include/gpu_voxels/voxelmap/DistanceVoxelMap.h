@@ -72,6 +72,14 @@ class DistanceVoxelMap : public GpuVoxelsMap {
   bool mergeOccupied(const std::shared_ptr<ProbVoxelMap> other, const Vector3ui& voxel_offset = Vector3ui(),
                      float occupancy_threshold = 0.5f);
 
+  // extract_distances (GV/voxelmap/DistanceVoxelMap.hpp:676-688): one
+  // free-space byte per voxel into dev_distances (device, getVoxelMapSize()).
+  void extract_distances(free_space_t* dev_distances, int robot_radius) const;
+  // init_floodfill (DistanceVoxelMap.hpp:658-674): dev_manhattan_distances[i] =
+  // MANHATTAN_DISTANCE_TOO_CLOSE where dev_distances[i] <= robot_radius, else
+  // MANHATTAN_DISTANCE_UNINITIALIZED.
+  void init_floodfill(free_space_t* dev_distances, manhattan_dist_t* dev_manhattan_distances, uint32_t robot_radius);
+
   // Queries at linear voxel ids (device pointers; [begin, end) ids -> out).
   void getSquaredDistances(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, int32_t* dev_output);
   void getDistances(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, int32_t* dev_output);

@@ -288,6 +288,20 @@ GVX_API gvx_status gvx_pvm_insert_points(gvx_pvm *m, const float *d_xyz, uint64_
 GVX_API gvx_status gvx_dvm_merge_occupied(gvx_dvm *m, const gvx_pvm *other, const uint32_t offset[3],
                                           float occupancy_threshold, gvx_stream stream);
 
+/* ---- Consumers of the distance field ------------------------------------- */
+
+/* Replaces DistanceVoxelMap::extract_distances(free_space_t*, robot_radius)
+ * (GV/voxelmap/DistanceVoxelMap.hpp:676-688, DistanceVoxel::extract_byte_distance
+ * GV/voxel/DistanceVoxel.h:144-199): one int8 per voxel -- the distance to the
+ * map border for voxels within robot_radius of it, else int(sqrtf(squared
+ * obstacle distance)) capped at 127. */
+GVX_API gvx_status gvx_dvm_extract_distances(const gvx_dvm *m, int8_t *d_out, int robot_radius, gvx_stream stream);
+/* Replaces DistanceVoxelMap::init_floodfill (DistanceVoxelMap.hpp:658-674,
+ * DistanceVoxel::init_floodfill_distance DistanceVoxel.h:201-215): int16 per
+ * voxel, 32765 (too close) where the byte <= robot_radius, else 32767. */
+GVX_API gvx_status gvx_dvm_init_floodfill(const gvx_dvm *m, const int8_t *d_distances, int16_t *d_manhattan,
+                                          int robot_radius, gvx_stream stream);
+
 /* ---- BitVectorVoxelList (GV/voxellist/BitVoxelList.h) ------------------- */
 
 /* Replaces BitVoxelList<256,uint32>(dim, side, MT_BITVECTOR_VOXELLIST). */
@@ -301,6 +315,15 @@ GVX_API gvx_status gvx_blist_clear(gvx_blist *l);
  * voxelise, drop out-of-bounds, sort and merge duplicates (make_unique, :143-212).
  * Blocking. */
 GVX_API gvx_status gvx_blist_insert_points(gvx_blist *l, const float *d_xyz, uint64_t n, uint32_t meaning, gvx_stream stream);
+/* Replaces distance_map_converter::extract_given_distances
+ * (GV/helpers_highlevel/DistanceMapConverter.cu:156-196): the voxels whose
+ * free-space byte (extract_distances at robot radius 0) lies in
+ * [min_dist, max_dist] become the list `result` (its reference dims must be
+ * the map's), in id order, each voxel with eBVM_OCCUPIED and swept-volume
+ * bits 4 .. 4 + byte - 1 (transform_to_bitvoxel, :103-154).  Blocking;
+ * *n_out = the number of entries. */
+GVX_API gvx_status gvx_extract_given_distances(const gvx_dvm *m, int min_dist, int max_dist, gvx_blist *result,
+                                               uint64_t *n_out, gvx_stream stream);
 /* Set the list to already-sorted unique ids with their voxels (device
  * arrays, copied).  n_voxels == 0 means every voxel gets bit `meaning`. */
 GVX_API gvx_status gvx_blist_set(gvx_blist *l, const uint32_t *d_ids, const uint8_t *d_voxels, uint64_t n, uint32_t meaning,

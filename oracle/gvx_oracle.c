@@ -626,3 +626,64 @@ void orc_dvm_merge_occupied(uint32_t *dvm, const int8_t *pvm, const uint32_t d[3
     dvm[i] = (x + off[0]) | ((y + off[1]) << 10) | ((z + off[2]) << 20);
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Distance-map consumers                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* DistanceVoxel::extract_byte_distance, GV/voxel/DistanceVoxel.h:144-199, as
+ * applied by DistanceVoxelMap::extract_distances (GV/voxelmap/DistanceVoxelMap.hpp:676-688):
+ * voxels within robot_radius of the map border get their border distance;
+ * the rest int(sqrtf(squared distance)) capped at SCHAR_MAX; int8 result. */
+static int8_t free_space_byte(uint32_t v, int x, int y, int z, int X, int Y, int Z, int r) {
+  if (x > X - r) return (int8_t)(X - x < 0 ? 0 : X - x);
+  if (y > Y - r) return (int8_t)(Y - y < 0 ? 0 : Y - y);
+  if (z > Z - r) return (int8_t)(Z - z < 0 ? 0 : Z - z);
+  if (x < r) return (int8_t)(x < 0 ? 0 : x);
+  if (y < r) return (int8_t)(y < 0 ? 0 : y);
+  if (z < r) return (int8_t)(z < 0 ? 0 : z);
+  int fs = (int)sqrtf((float)dv_sqdist(v, x, y, z));
+  return (int8_t)(fs > 127 ? 127 : fs);
+}
+
+void orc_extract_distances(const uint32_t *map, const uint32_t d[3], int r, int8_t *out) {
+  const uint64_t layer = (uint64_t)d[0] * d[1], n = layer * d[2];
+  for (uint64_t i = 0; i < n; ++i) {
+    int z = (int)(i / layer), y = (int)((i % layer) / d[0]), x = (int)(i % d[0]);
+    out[i] = free_space_byte(map[i], x, y, z, (int)d[0], (int)d[1], (int)d[2], r);
+  }
+}
+
+/* DistanceVoxel::init_floodfill_distance, GV/voxel/DistanceVoxel.h:201-215
+ * (MANHATTAN_DISTANCE_* constants, GV/helpers/common_defines.h:117-119). */
+void orc_init_floodfill(const int8_t *in, int16_t *out, uint64_t n, int r) {
+  for (uint64_t i = 0; i < n; ++i) out[i] = (int16_t)((int)in[i] <= r ? 32765 : 32767);
+}
+
+/* distance_map_converter::extract_given_distances,
+ * GV/helpers_highlevel/DistanceMapConverter.cu:156-196 with transform_to_bitvoxel (:103-154):
+ * free-space bytes at robot radius 0; voxels with min <= byte <= max, in id
+ * order, become list entries whose voxel has eBVM_OCCUPIED and the
+ * swept-volume bits 4 .. 4 + byte - 1 set (UNDEFINED and a cap above 255).
+ * Returns the count; ids / voxels (32 B each) may be NULL to count only. */
+uint64_t orc_extract_given_distances(const uint32_t *map, const uint32_t d[3], int mn, int mx, uint32_t *ids,
+                                     uint8_t *vox) {
+  const uint64_t layer = (uint64_t)d[0] * d[1], n = layer * d[2];
+  uint64_t k = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    int z = (int)(i / layer), y = (int)((i % layer) / d[0]), x = (int)(i % d[0]);
+    int8_t b = free_space_byte(map[i], x, y, z, (int)d[0], (int)d[1], (int)d[2], 0);
+    if (b < mn || b > mx) continue;
+    if (ids) ids[k] = (uint32_t)i;
+    if (vox) {
+      uint8_t *v = vox + k * BITVOXEL_BYTES;
+      memset(v, 0, BITVOXEL_BYTES);
+      v[0] |= 1u << 1; /* eBVM_OCCUPIED */
+      unsigned fs = (uint16_t)(int)b + 4u;
+      if (fs > 255u) { v[31] |= 0x80u; fs = 255u; }
+      for (unsigned s = 4; s < fs; ++s) v[s >> 3] |= (uint8_t)(1u << (s & 7));
+    }
+    ++k;
+  }
+  return k;
+}

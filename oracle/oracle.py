@@ -84,6 +84,12 @@ def lib():
         L.orc_float_to_probability.argtypes = [ctypes.c_float]
         L.orc_float_to_probability.restype = ctypes.c_int
         L.orc_dvm_merge_occupied.argtypes = [_u32p, _i8p, _u32p, _u32p, ctypes.c_float]
+        _i16p = np.ctypeslib.ndpointer(dtype=np.int16, flags="C_CONTIGUOUS")
+        L.orc_extract_distances.argtypes = [_u32p, _u32p, ctypes.c_int, _i8p]
+        L.orc_init_floodfill.argtypes = [_i8p, _i16p, ctypes.c_uint64, ctypes.c_int]
+        L.orc_extract_given_distances.argtypes = [_u32p, _u32p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                  ctypes.c_void_p]
+        L.orc_extract_given_distances.restype = ctypes.c_uint64
         L.orc_num_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -263,6 +269,27 @@ def float_to_probability(val: float) -> int:
 
 def dvm_merge_occupied(vmap: np.ndarray, pmap: np.ndarray, dims, offset=(0, 0, 0), threshold: float = 0.5) -> None:
     lib().orc_dvm_merge_occupied(vmap, pmap, _dims(dims), np.asarray(offset, dtype=np.uint32), float(threshold))
+
+
+def extract_distances(vmap: np.ndarray, dims, robot_radius: int = 0) -> np.ndarray:
+    out = np.empty(vmap.size, dtype=np.int8)
+    lib().orc_extract_distances(vmap, _dims(dims), int(robot_radius), out)
+    return out
+
+
+def init_floodfill(dist: np.ndarray, robot_radius: int) -> np.ndarray:
+    out = np.empty(dist.size, dtype=np.int16)
+    lib().orc_init_floodfill(np.ascontiguousarray(dist, dtype=np.int8), out, dist.size, int(robot_radius))
+    return out
+
+
+def extract_given_distances(vmap: np.ndarray, dims, min_dist: int, max_dist: int):
+    """-> (ids uint32[k], voxels uint8[k*32])"""
+    k = int(lib().orc_extract_given_distances(vmap, _dims(dims), int(min_dist), int(max_dist), None, None))
+    ids = np.empty(max(k, 1), dtype=np.uint32)
+    vox = np.empty(max(k, 1) * 32, dtype=np.uint8)
+    lib().orc_extract_given_distances(vmap, _dims(dims), int(min_dist), int(max_dist), ids.ctypes.data, vox.ctypes.data)
+    return ids[:k], vox[:k * 32]
 
 
 def decode_sites(vmap: np.ndarray):

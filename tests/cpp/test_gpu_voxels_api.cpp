@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/gpu_voxels/GpuVoxels.h"
+#include "../../include/gpu_voxels/helpers_highlevel/DistanceMapConverter.h"
 
 using namespace gpu_voxels;
 
@@ -182,8 +183,36 @@ static void prob_map_to_distance_map() {
   gvl->delMap("myDistanceMap");
 }
 
+// Free-space bytes and the distance band -> BitVoxelList conversion
+// (DistanceVoxelMap::extract_distances, distance_map_converter) on one site.
+static void distance_consumers() {
+  voxelmap::DistanceVoxelMap dist(Vector3ui(8, 8, 8), 1.0f);
+  dist.insertPointCloud(std::vector<Vector3f>{Vector3f(3.5f, 3.5f, 3.5f)}, eBVM_OCCUPIED);
+  dist.parallelBanding3D();
+  free_space_t* d_bytes = nullptr;
+  manhattan_dist_t* d_flood = nullptr;
+  cudaMalloc(&d_bytes, 512);
+  cudaMalloc(&d_flood, 512 * sizeof(manhattan_dist_t));
+  dist.extract_distances(d_bytes, 0);
+  std::vector<free_space_t> bytes(512);
+  cudaMemcpy(bytes.data(), d_bytes, 512, cudaMemcpyDeviceToHost);
+  CHECK(bytes[7 + 8 * 7 + 64 * 7] == 6 && bytes[3 + 8 * 3 + 64 * 3] == 0, "extract_distances: int(sqrt(48)) = 6, site 0");
+  dist.init_floodfill(d_bytes, d_flood, 2);
+  std::vector<manhattan_dist_t> flood(512);
+  cudaMemcpy(flood.data(), d_flood, 512 * sizeof(manhattan_dist_t), cudaMemcpyDeviceToHost);
+  bool flood_ok = true;
+  for (int i = 0; i < 512; ++i)
+    flood_ok &= flood[i] == (bytes[i] <= 2 ? MANHATTAN_DISTANCE_TOO_CLOSE : MANHATTAN_DISTANCE_UNINITIALIZED);
+  CHECK(flood_ok, "init_floodfill");
+  BitVectorVoxelList band(Vector3ui(8, 8, 8), 1.0f);
+  CHECK(distance_map_converter::extract_given_distances(dist, 1, 1, band) == 26, "extract_given_distances(1,1): 26 voxels");
+  cudaFree(d_bytes);
+  cudaFree(d_flood);
+}
+
 int main() {
   GpuVoxels::getInstance();
+  distance_consumers();
   distance_extraction();
   distance_correctness();
   collisions();
