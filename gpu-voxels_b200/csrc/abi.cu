@@ -322,6 +322,28 @@ gvx_status gvx_bvm_collide(gvx_bvm* self, const gvx_bvm* other, const int32_t of
                      "collideWith(BitVectorVoxelMap)");
 }
 
+/* ---- typed collisions ---------------------------------------------------- */
+
+gvx_status gvx_bvm_collide_types(gvx_bvm* self, const gvx_bvm* other, uint64_t* d_count, uint8_t* d_types,
+                                 gvx_stream stream) {
+  if (self == nullptr || other == nullptr || d_count == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(self->dims, other->dims)) return fail(GVX_ERR_INVALID_ARG, "maps differ in dimensions");
+  return cuda_status(launch_bvm_collide_types(self->d_vox, other->d_vox, num_voxels(self->dims), 0, 0.f,
+                                              reinterpret_cast<unsigned long long*>(d_count),
+                                              reinterpret_cast<uint32_t*>(d_types), as_stream(stream)),
+                     "collideWithTypes(BitVectorVoxelMap)");
+}
+
+gvx_status gvx_bvm_collide_types_pvm(gvx_bvm* self, const gvx_pvm* other, float coll_threshold, uint64_t* d_count,
+                                     uint8_t* d_types, gvx_stream stream) {
+  if (self == nullptr || other == nullptr || d_count == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(self->dims, other->dims)) return fail(GVX_ERR_INVALID_ARG, "maps differ in dimensions");
+  return cuda_status(launch_bvm_collide_types(self->d_vox, other->d_vox, num_voxels(self->dims), 1, coll_threshold,
+                                              reinterpret_cast<unsigned long long*>(d_count),
+                                              reinterpret_cast<uint32_t*>(d_types), as_stream(stream)),
+                     "collideWithTypes(ProbVoxelMap)");
+}
+
 /* ---- ProbVoxelMap ------------------------------------------------------ */
 
 gvx_status gvx_pvm_create(const gvx_dims* dims, float voxel_side, gvx_pvm** out) {
@@ -594,6 +616,49 @@ gvx_status gvx_blist_set(gvx_blist* l, const uint32_t* d_ids, const uint8_t* d_v
   if (e != cudaSuccess) return cuda_status(e, "list set");
   l->n = n;
   return GVX_OK;
+}
+
+gvx_status gvx_blist_collide_types_bvm(gvx_blist* l, const gvx_bvm* map, const int32_t offset[3], uint64_t* d_count,
+                                       uint8_t* d_types, gvx_stream stream) {
+  if (l == nullptr || map == nullptr || d_count == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(l->ref, map->dims)) return fail(GVX_ERR_INVALID_ARG, "the list's reference dims differ from the map's");
+  return cuda_status(launch_list_collide_types(l->d_ids, l->d_vox, l->n, map->d_vox, num_voxels(map->dims), 0, 0.f,
+                                               linear_offset(map->dims, offset), nullptr,
+                                               reinterpret_cast<unsigned long long*>(d_count),
+                                               reinterpret_cast<uint32_t*>(d_types), as_stream(stream)),
+                     "collideWithTypes(list, BitVectorVoxelMap)");
+}
+
+gvx_status gvx_blist_collide_types_pvm(gvx_blist* l, const gvx_pvm* map, float coll_threshold, const int32_t offset[3],
+                                       uint64_t* d_count, uint8_t* d_types, gvx_stream stream) {
+  if (l == nullptr || map == nullptr || d_count == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(l->ref, map->dims)) return fail(GVX_ERR_INVALID_ARG, "the list's reference dims differ from the map's");
+  return cuda_status(launch_list_collide_types(l->d_ids, l->d_vox, l->n, map->d_vox, num_voxels(map->dims), 1,
+                                               coll_threshold, linear_offset(map->dims, offset), nullptr,
+                                               reinterpret_cast<unsigned long long*>(d_count),
+                                               reinterpret_cast<uint32_t*>(d_types), as_stream(stream)),
+                     "collideWithTypes(list, ProbVoxelMap)");
+}
+
+gvx_status gvx_blist_collide_type_mask_bvm(gvx_blist* l, const gvx_bvm* map, const uint8_t* d_mask, const int32_t offset[3],
+                                           uint64_t* d_count, gvx_stream stream) {
+  if (l == nullptr || map == nullptr || d_mask == nullptr || d_count == nullptr)
+    return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(l->ref, map->dims)) return fail(GVX_ERR_INVALID_ARG, "the list's reference dims differ from the map's");
+  return cuda_status(launch_list_collide_types(l->d_ids, l->d_vox, l->n, map->d_vox, num_voxels(map->dims), 0, 0.f,
+                                               linear_offset(map->dims, offset), d_mask,
+                                               reinterpret_cast<unsigned long long*>(d_count), nullptr,
+                                               as_stream(stream)),
+                     "collideWithTypeMask");
+}
+
+gvx_status gvx_blist_collide_types_blist(const gvx_blist* l, const gvx_blist* other, uint64_t* d_count, uint8_t* d_types,
+                                         gvx_stream stream) {
+  if (l == nullptr || other == nullptr || d_count == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  return cuda_status(launch_list_list_types(l->d_ids, l->d_vox, l->n, other->d_ids, other->d_vox, other->n,
+                                            reinterpret_cast<unsigned long long*>(d_count),
+                                            reinterpret_cast<uint32_t*>(d_types), as_stream(stream)),
+                     "collideWithTypes(list, list)");
 }
 
 gvx_status gvx_dvm_extract_distances(const gvx_dvm* m, int8_t* d_out, int robot_radius, gvx_stream stream) {

@@ -22,6 +22,7 @@ constexpr uint32_t kBitVoxelBytes = 32;
 constexpr int16_t kManhattanUninitialized = 32767;  // MANHATTAN_DISTANCE_UNINITIALIZED (common_defines.h:117)
 constexpr int16_t kManhattanTooClose = 32765;       // MANHATTAN_DISTANCE_TOO_CLOSE (:119)
 constexpr uint32_t kBitVoxelWords = 8;
+constexpr uint32_t kEbvmCollision = 2;  // eBVM_COLLISION (GV/helpers/common_defines.h:55)
 constexpr uint32_t kCollisionBit = 2;            // eBVM_COLLISION
 constexpr uint32_t kMaxDim = 1023;
 
@@ -158,6 +159,17 @@ cudaError_t launch_pvm_insert(int8_t* d_vox, gvx_dims d, float side, const float
 cudaError_t launch_merge_occupied(uint32_t* d_dvm, const int8_t* d_pvm, gvx_dims d, const uint32_t off[3], float threshold,
                                   cudaStream_t s);
 int prob_threshold(float val);
+// Typed collisions (collide_types.cu).  mode / kind 0: the other map is a
+// BitVoxel map; 1: an int8 ProbVoxelMap.  d_count (uint64) and d_types (32 B)
+// are overwritten with this call's count and OR of colliding types.
+cudaError_t launch_bvm_collide_types(uint8_t* d_self, const void* d_other, uint64_t n, int mode, float threshold,
+                                     unsigned long long* d_count, uint32_t* d_types, cudaStream_t s);
+cudaError_t launch_list_collide_types(const uint32_t* d_ids, uint8_t* d_lvox, uint64_t n, const void* d_map,
+                                      uint64_t map_n, int kind, float threshold, int64_t off, const uint8_t* d_mask,
+                                      unsigned long long* d_count, uint32_t* d_types, cudaStream_t s);
+cudaError_t launch_list_list_types(const uint32_t* d_ids_a, const uint8_t* d_vox_a, uint64_t na, const uint32_t* d_ids_b,
+                                   const uint8_t* d_vox_b, uint64_t nb, unsigned long long* d_count, uint32_t* d_types,
+                                   cudaStream_t s);
 cudaError_t launch_extract_distances(const uint32_t* d_vox, gvx_dims d, int robot_radius, int8_t* d_out, cudaStream_t s);
 cudaError_t launch_init_floodfill(const int8_t* d_in, int16_t* d_out, uint64_t n, int robot_radius, cudaStream_t s);
 // Distance band -> list: per-tile counts, exclusive tile offsets (+ total at

@@ -116,6 +116,12 @@ PROTOTYPES = {
     "gvx_dvm_extract_distances": [_vp, _vp, ctypes.c_int, _vp],
     "gvx_dvm_init_floodfill": [_vp, _vp, _vp, ctypes.c_int, _vp],
     "gvx_extract_given_distances": [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_u64), _vp],
+    "gvx_bvm_collide_types": [_vp, _vp, _vp, _vp, _vp],
+    "gvx_bvm_collide_types_pvm": [_vp, _vp, _f, _vp, _vp, _vp],
+    "gvx_blist_collide_types_bvm": [_vp, _vp, _i32p, _vp, _vp, _vp],
+    "gvx_blist_collide_types_pvm": [_vp, _vp, _f, _i32p, _vp, _vp, _vp],
+    "gvx_blist_collide_type_mask_bvm": [_vp, _vp, _vp, _i32p, _vp, _vp],
+    "gvx_blist_collide_types_blist": [_vp, _vp, _vp, _vp, _vp],
     "gvx_blist_create": [ctypes.POINTER(Dims), _f, ctypes.POINTER(_vp)],
     "gvx_blist_destroy": [_vp],
     "gvx_blist_size": [_vp, ctypes.POINTER(_u64)],

@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes
 from typing import Iterable, Optional, Sequence
 
+import numpy as np
 import torch
 
 from . import _abi
@@ -340,6 +341,21 @@ class BitVectorVoxelMap:
     def collideWith(self, other: "BitVectorVoxelMap", coll_threshold: float = 1.0, offset=(0, 0, 0)) -> int:
         return int(self.collideWithAsync(other, offset).item())
 
+    def collideWithTypes(self, other, coll_threshold: float = 1.0, offset=(0, 0, 0)):
+        """-> (count, types uint8[32]): swept-volume types colliding with a
+        BitVectorVoxelMap, or this map's types where a ProbVoxelMap is
+        occupied; colliding voxels get eBVM_COLLISION.  `offset` is ignored,
+        as in the reference."""
+        types = torch.zeros(32, dtype=torch.uint8, device="cuda")
+        if isinstance(other, BitVectorVoxelMap):
+            call("gvx_bvm_collide_types", self._h, other.handle, _ptr(self._count), _ptr(types), _stream())
+        elif isinstance(other, ProbVoxelMap):
+            call("gvx_bvm_collide_types_pvm", self._h, other.handle, float(coll_threshold), _ptr(self._count),
+                 _ptr(types), _stream())
+        else:
+            raise TypeError("collideWithTypes expects a BitVectorVoxelMap or ProbVoxelMap")
+        return int(self._count.item()), types.cpu().numpy()
+
 
 class BitVectorVoxelList:
     """BitVoxelList<256, uint32> (GV/voxellist/BitVoxelList.h): sorted unique
@@ -401,6 +417,31 @@ class BitVectorVoxelList:
             call("gvx_blist_collide_blist", self._h, other.handle, _offset(offset), _ptr(self._count), _stream())
         else:
             raise TypeError("collideWith expects a BitVectorVoxelMap or BitVectorVoxelList")
+        return int(self._count.item())
+
+    def collideWithTypes(self, other, coll_threshold: float = 1.0, offset=(0, 0, 0)):
+        """-> (count, types uint8[32]) against a BitVectorVoxelMap, a ProbVoxelMap
+        or another BitVectorVoxelList; colliding entries get eBVM_COLLISION
+        (not for list vs list)."""
+        types = torch.zeros(32, dtype=torch.uint8, device="cuda")
+        if isinstance(other, BitVectorVoxelMap):
+            call("gvx_blist_collide_types_bvm", self._h, other.handle, _offset(offset), _ptr(self._count), _ptr(types),
+                 _stream())
+        elif isinstance(other, ProbVoxelMap):
+            call("gvx_blist_collide_types_pvm", self._h, other.handle, float(coll_threshold), _offset(offset),
+                 _ptr(self._count), _ptr(types), _stream())
+        elif isinstance(other, BitVectorVoxelList):
+            call("gvx_blist_collide_types_blist", self._h, other.handle, _ptr(self._count), _ptr(types), _stream())
+        else:
+            raise TypeError("collideWithTypes expects a BitVectorVoxelMap, ProbVoxelMap or BitVectorVoxelList")
+        return int(self._count.item()), types.cpu().numpy()
+
+    def collideWithTypeMask(self, other: "BitVectorVoxelMap", types_to_check, coll_threshold: float = 1.0,
+                            offset=(0, 0, 0)) -> int:
+        """Collisions of entries whose bits meet the 32-byte mask."""
+        mask = torch.as_tensor(np.asarray(types_to_check, dtype=np.uint8)).cuda()
+        call("gvx_blist_collide_type_mask_bvm", self._h, other.handle, _ptr(mask), _offset(offset), _ptr(self._count),
+             _stream())
         return int(self._count.item())
 
 

@@ -261,6 +261,26 @@ GVX_API gvx_status gvx_bvm_insert_points(gvx_bvm *m, const float *d_xyz, uint64_
 GVX_API gvx_status gvx_bvm_collide(gvx_bvm *self, const gvx_bvm *other, const int32_t offset[3], int mark, uint64_t *d_count,
                            gvx_stream stream);
 
+/* ---- Typed collisions ------------------------------------------------------ */
+/* Every call overwrites *d_count (device uint64) with the number of colliding
+ * voxels / entries and, where given, d_types (device, 32 bytes = one
+ * BitVector<256>) with the OR of the colliding types; colliding voxels of
+ * `self` / entries of the list get eBVM_COLLISION. */
+
+/* Replaces BitVoxelMap::collideWithTypes(const BitVectorVoxelMap*, BitVectorVoxel&, thr, offset)
+ * (GV/voxelmap/BitVoxelMap.hpp:212-217 -> kernelCollideVoxelMapsBitvector,
+ * GV/voxelmap/kernels/VoxelMapOperations.hpp:187-239, SVCollider window 0,
+ * GV/voxel/SVCollider.hpp:90-96, GV/helpers/BitVector.h:415-470): the types of
+ * voxel i are self[i] & other[i] on the swept-volume bits (4..255).  The
+ * reference ignores the offset and threshold here; so does this entry. */
+GVX_API gvx_status gvx_bvm_collide_types(gvx_bvm *self, const gvx_bvm *other, uint64_t *d_count, uint8_t *d_types,
+                                         gvx_stream stream);
+/* Replaces collideWithTypes(const ProbVoxelMap*, ...) (BitVoxelMap.hpp:219-224,
+ * SVCollider.hpp:98-108): occupancy >= SVCollider's threshold (thr*254-127,
+ * not clamped) and self not empty; the types are all of self's bits. */
+GVX_API gvx_status gvx_bvm_collide_types_pvm(gvx_bvm *self, const gvx_pvm *other, float coll_threshold,
+                                             uint64_t *d_count, uint8_t *d_types, gvx_stream stream);
+
 /* ---- ProbVoxelMap (GV/voxelmap/ProbVoxelMap.h) and mergeOccupied -------- */
 
 /* Replaces ProbVoxelMap(dim, side, MT_PROBAB_VOXELMAP) (GV/voxelmap/ProbVoxelMap.hpp:35-39):
@@ -315,6 +335,29 @@ GVX_API gvx_status gvx_blist_clear(gvx_blist *l);
  * voxelise, drop out-of-bounds, sort and merge duplicates (make_unique, :143-212).
  * Blocking. */
 GVX_API gvx_status gvx_blist_insert_points(gvx_blist *l, const float *d_xyz, uint64_t n, uint32_t meaning, gvx_stream stream);
+/* Replaces BitVoxelList::collideWithTypes(const BitVectorVoxelMap*, ...) and
+ * (const ProbVoxelMap*, ...) (GV/voxellist/BitVoxelList.hpp:120-201 ->
+ * kernelCollideWithVoxelMap, GV/voxellist/kernels/VoxelListOperations.hpp:204-260):
+ * entry i meets map voxel ids[i] + offset (skipped outside the map) and
+ * collides when that voxel is occupied (BitVoxel: not noneButEmpty;
+ * ProbVoxelMap: occupancy >= coll_threshold compared as float); its bits
+ * (before the mark) are the types. */
+GVX_API gvx_status gvx_blist_collide_types_bvm(gvx_blist *l, const gvx_bvm *map, const int32_t offset[3],
+                                               uint64_t *d_count, uint8_t *d_types, gvx_stream stream);
+GVX_API gvx_status gvx_blist_collide_types_pvm(gvx_blist *l, const gvx_pvm *map, float coll_threshold,
+                                               const int32_t offset[3], uint64_t *d_count, uint8_t *d_types,
+                                               gvx_stream stream);
+/* Replaces BitVoxelList::collideWithTypeMask(map, types_to_check, ...)
+ * (BitVoxelList.hpp:203-246, kernelCollideWithVoxelMapBitMask
+ * VoxelListOperations.hpp:282-325): as above, counting only entries whose
+ * bits meet the mask (d_mask: device, 32 bytes). */
+GVX_API gvx_status gvx_blist_collide_type_mask_bvm(gvx_blist *l, const gvx_bvm *map, const uint8_t *d_mask,
+                                                   const int32_t offset[3], uint64_t *d_count, gvx_stream stream);
+/* Replaces BitVoxelList::collideWithTypes(const BitVectorVoxelList*, ...)
+ * (BitVoxelList.hpp:94-118): ids present in both lists; types = OR of both
+ * entries' bits.  Offsets are unsupported there and not taken here. */
+GVX_API gvx_status gvx_blist_collide_types_blist(const gvx_blist *l, const gvx_blist *other, uint64_t *d_count,
+                                                 uint8_t *d_types, gvx_stream stream);
 /* Replaces distance_map_converter::extract_given_distances
  * (GV/helpers_highlevel/DistanceMapConverter.cu:156-196): the voxels whose
  * free-space byte (extract_distances at robot radius 0) lies in

@@ -687,3 +687,100 @@ uint64_t orc_extract_given_distances(const uint32_t *map, const uint32_t d[3], i
   }
   return k;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Typed collisions                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* BitVoxelMap::collideWithTypes(BitVectorVoxelMap*) (GV/voxelmap/BitVoxelMap.hpp:212-217)
+ * -> collisionCheckBitvector (:91-143) -> kernelCollideVoxelMapsBitvector
+ * (GV/voxelmap/kernels/VoxelMapOperations.hpp:187-239) with SVCollider
+ * (GV/voxel/SVCollider.hpp:90-96) and bitMarginCollisionCheck at window 0
+ * and bit offset 0 (GV/helpers/BitVector.h:415-470): the colliding types of
+ * voxel i are self[i] & other[i] restricted to the swept-volume bits (bits
+ * 0..3 of `other` masked out); a voxel with any collides, is counted, marks
+ * self with eBVM_COLLISION and adds its types to `types` (32 bytes, OR). */
+uint64_t orc_bvm_collide_types(uint8_t *self, const uint8_t *other, uint64_t n, uint8_t *types) {
+  uint64_t count = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    uint8_t *a = self + i * BITVOXEL_BYTES;
+    const uint8_t *b = other + i * BITVOXEL_BYTES;
+    uint8_t t[BITVOXEL_BYTES];
+    int any = 0;
+    for (int k = 0; k < BITVOXEL_BYTES; ++k) {
+      t[k] = (uint8_t)(a[k] & (k == 0 ? (b[k] & 0xF0) : b[k]));
+      any |= t[k];
+    }
+    if (!any) continue;
+    ++count;
+    for (int k = 0; k < BITVOXEL_BYTES; ++k) types[k] |= t[k];
+    a[EBVM_COLLISION >> 3] |= (uint8_t)(1u << (EBVM_COLLISION & 7));
+  }
+  return count;
+}
+
+/* SVCollider::floatToProbability (GV/voxel/SVCollider.hpp:144-148): no clamping. */
+static int sv_threshold(float val) { return (int)(int8_t)((val * (127.0f - (-127.0f))) + (-127.0f)); }
+
+/* BitVoxelMap::collideWithTypes(ProbVoxelMap*) (BitVoxelMap.hpp:219-224) with
+ * SVCollider::collide(BitVoxel, ProbabilisticVoxel, ...) (SVCollider.hpp:98-108):
+ * occupancy >= threshold and self not empty -> all of self's bits are types. */
+uint64_t orc_bvm_collide_types_pvm(uint8_t *self, const int8_t *other, uint64_t n, float thr, uint8_t *types) {
+  const int t = sv_threshold(thr);
+  uint64_t count = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    uint8_t *a = self + i * BITVOXEL_BYTES;
+    if (!((int)other[i] >= t && !bv_none_but_empty(a))) continue;
+    ++count;
+    for (int k = 0; k < BITVOXEL_BYTES; ++k) types[k] |= a[k];
+    a[EBVM_COLLISION >> 3] |= (uint8_t)(1u << (EBVM_COLLISION & 7));
+  }
+  return count;
+}
+
+/* BitVoxelList::collideWithTypes(BitVectorVoxelMap*) / (ProbVoxelMap*) and
+ * collideWithTypeMask (GV/voxellist/BitVoxelList.hpp:120-246) ->
+ * kernelCollideWithVoxelMap / kernelCollideWithVoxelMapBitMask
+ * (GV/voxellist/kernels/VoxelListOperations.hpp:204-260,282-325): entry i meets
+ * map voxel ids[i] + offset (skipped outside the map); it collides when that
+ * voxel is occupied -- BitVoxel: not noneButEmpty; ProbabilisticVoxel:
+ * occupancy >= threshold as a float -- and, with a mask, when its own bits
+ * meet the mask.  Colliding entries are counted, add their bits (before the
+ * mark) to `types` and get eBVM_COLLISION.  map_kind 0: BitVoxel map, 1: int8. */
+uint64_t orc_list_collide_types_map(const uint32_t *ids, uint8_t *list_voxels, uint64_t n, const void *map,
+                                    uint64_t map_n, int map_kind, float thr, int64_t offset_linear, const uint8_t *mask,
+                                    uint8_t *types) {
+  uint64_t count = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    int64_t j = (int64_t)ids[i] + offset_linear;
+    if (j < 0 || j >= (int64_t)map_n) continue;
+    int occ = map_kind == 0 ? !bv_none_but_empty((const uint8_t *)map + (uint64_t)j * BITVOXEL_BYTES)
+                            : ((float)((const int8_t *)map)[j] >= thr);
+    if (!occ) continue;
+    uint8_t *a = list_voxels + i * BITVOXEL_BYTES;
+    if (mask) {
+      int meet = 0;
+      for (int k = 0; k < BITVOXEL_BYTES; ++k) meet |= a[k] & mask[k];
+      if (!meet) continue;
+    }
+    ++count;
+    if (types)
+      for (int k = 0; k < BITVOXEL_BYTES; ++k) types[k] |= a[k];
+    a[EBVM_COLLISION >> 3] |= (uint8_t)(1u << (EBVM_COLLISION & 7));
+  }
+  return count;
+}
+
+/* BitVoxelList::collideWithTypes(BitVectorVoxelList*) (BitVoxelList.hpp:94-118):
+ * the ids present in both sorted lists; types = OR over them of both voxels. */
+uint64_t orc_list_collide_types_list(const uint32_t *ids_a, const uint8_t *vox_a, uint64_t na, const uint32_t *ids_b,
+                                     const uint8_t *vox_b, uint64_t nb, uint8_t *types) {
+  uint64_t i = 0, j = 0, count = 0;
+  while (i < na && j < nb) {
+    if (ids_a[i] < ids_b[j]) { ++i; continue; }
+    if (ids_b[j] < ids_a[i]) { ++j; continue; }
+    for (int k = 0; k < BITVOXEL_BYTES; ++k) types[k] |= vox_a[i * BITVOXEL_BYTES + k] | vox_b[j * BITVOXEL_BYTES + k];
+    ++count; ++i; ++j;
+  }
+  return count;
+}

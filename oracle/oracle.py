@@ -90,6 +90,16 @@ def lib():
         L.orc_extract_given_distances.argtypes = [_u32p, _u32p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                   ctypes.c_void_p]
         L.orc_extract_given_distances.restype = ctypes.c_uint64
+        L.orc_bvm_collide_types.argtypes = [_u8p, _u8p, ctypes.c_uint64, _u8p]
+        L.orc_bvm_collide_types.restype = ctypes.c_uint64
+        L.orc_bvm_collide_types_pvm.argtypes = [_u8p, _i8p, ctypes.c_uint64, ctypes.c_float, _u8p]
+        L.orc_bvm_collide_types_pvm.restype = ctypes.c_uint64
+        L.orc_list_collide_types_map.argtypes = [_u32p, _u8p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64,
+                                                 ctypes.c_int, ctypes.c_float, ctypes.c_int64, ctypes.c_void_p,
+                                                 ctypes.c_void_p]
+        L.orc_list_collide_types_map.restype = ctypes.c_uint64
+        L.orc_list_collide_types_list.argtypes = [_u32p, _u8p, ctypes.c_uint64, _u32p, _u8p, ctypes.c_uint64, _u8p]
+        L.orc_list_collide_types_list.restype = ctypes.c_uint64
         L.orc_num_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -290,6 +300,43 @@ def extract_given_distances(vmap: np.ndarray, dims, min_dist: int, max_dist: int
     vox = np.empty(max(k, 1) * 32, dtype=np.uint8)
     lib().orc_extract_given_distances(vmap, _dims(dims), int(min_dist), int(max_dist), ids.ctypes.data, vox.ctypes.data)
     return ids[:k], vox[:k * 32]
+
+
+def bvm_collide_types(self_map: np.ndarray, other: np.ndarray):
+    """-> (count, types uint8[32]); marks self."""
+    types = np.zeros(32, dtype=np.uint8)
+    n = lib().orc_bvm_collide_types(self_map, other, self_map.size // 32, types)
+    return int(n), types
+
+
+def bvm_collide_types_pvm(self_map: np.ndarray, pmap: np.ndarray, threshold: float):
+    types = np.zeros(32, dtype=np.uint8)
+    n = lib().orc_bvm_collide_types_pvm(self_map, pmap, self_map.size // 32, float(threshold), types)
+    return int(n), types
+
+
+def list_collide_types_map(ids, list_vox: np.ndarray, bmap: np.ndarray, offset_linear: int = 0, mask=None,
+                           prob_threshold: float = None):
+    """List vs BitVoxel map (bmap uint8, 32 B voxels) or, with prob_threshold,
+    vs a ProbVoxelMap (bmap int8).  -> (count, types uint8[32]); marks the list."""
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    types = np.zeros(32, dtype=np.uint8)
+    kind = 0 if prob_threshold is None else 1
+    map_n = bmap.size // 32 if kind == 0 else bmap.size
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    n = lib().orc_list_collide_types_map(ids, list_vox, ids.size, bmap.ctypes.data, map_n, kind,
+                                         float(prob_threshold or 0.0), int(offset_linear),
+                                         None if m is None else m.ctypes.data, types.ctypes.data)
+    return int(n), types
+
+
+def list_collide_types_list(ids_a, vox_a, ids_b, vox_b):
+    types = np.zeros(32, dtype=np.uint8)
+    a = np.ascontiguousarray(ids_a, dtype=np.uint32)
+    b = np.ascontiguousarray(ids_b, dtype=np.uint32)
+    n = lib().orc_list_collide_types_list(a, np.ascontiguousarray(vox_a), a.size, b, np.ascontiguousarray(vox_b), b.size,
+                                          types)
+    return int(n), types
 
 
 def decode_sites(vmap: np.ndarray):
