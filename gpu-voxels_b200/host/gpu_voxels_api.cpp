@@ -246,13 +246,15 @@ BitVoxelMap<length>::BitVoxelMap(const Vector3ui dim, const float voxel_side_len
     : GpuVoxelsMap(map_type, dim, voxel_side_length) {
   gvx_dims d = to_dims(dim);
   require(gvx_bvm_create(&d, voxel_side_length, &m_handle), "BitVoxelMap");
-  if (cudaMalloc(&m_dev_count, sizeof(uint64_t)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+  if (cudaMalloc(&m_dev_count, sizeof(uint64_t)) != cudaSuccess || cudaMalloc(&m_dev_types, 32) != cudaSuccess)
+    throw std::runtime_error("cudaMalloc failed");
 }
 
 template <size_t length>
 BitVoxelMap<length>::~BitVoxelMap() {
   gvx_bvm_destroy(m_handle);
   if (m_dev_count) cudaFree(m_dev_count);
+  if (m_dev_types) cudaFree(m_dev_types);
 }
 
 template <size_t length>
@@ -294,6 +296,39 @@ size_t BitVoxelMap<length>::collideWith(const BitVoxelMap<length>* map, float, c
   return (size_t)count;
 }
 
+// The count and types a typed-collision call left on the device.
+static size_t read_types(const uint64_t* d_count, const uint8_t* d_types, BitVectorVoxel* types, bool accumulate) {
+  uint64_t count = 0;
+  BitVectorVoxel t;
+  cudaMemcpy(&count, d_count, sizeof(count), cudaMemcpyDeviceToHost);
+  cudaMemcpy(t.bitVector().data(), d_types, 32, cudaMemcpyDeviceToHost);
+  if (accumulate) types->bitVector() |= t.bitVector();
+  else *types = t;
+  return (size_t)count;
+}
+
+template <size_t length>
+size_t BitVoxelMap<length>::collideWithTypes(const BitVoxelMap<length>* map, BitVectorVoxel& types, float,
+                                             const Vector3i&) {
+  std::lock(m_mutex, map->m_mutex);
+  std::lock_guard<std::recursive_timed_mutex> g1(m_mutex, std::adopt_lock);
+  std::lock_guard<std::recursive_timed_mutex> g2(map->m_mutex, std::adopt_lock);
+  if (!ok(gvx_bvm_collide_types(m_handle, map->m_handle, m_dev_count, m_dev_types, nullptr), "collideWithTypes")) return 0;
+  return read_types(m_dev_count, m_dev_types, &types, true);  // the reference ORs into the caller's set
+}
+
+template <size_t length>
+size_t BitVoxelMap<length>::collideWithTypes(const ProbVoxelMap* map, BitVectorVoxel& types, float coll_threshold,
+                                             const Vector3i&) {
+  std::lock(m_mutex, map->mutexRef());
+  std::lock_guard<std::recursive_timed_mutex> g1(m_mutex, std::adopt_lock);
+  std::lock_guard<std::recursive_timed_mutex> g2(map->mutexRef(), std::adopt_lock);
+  if (!ok(gvx_bvm_collide_types_pvm(m_handle, map->handle(), coll_threshold, m_dev_count, m_dev_types, nullptr),
+          "collideWithTypes"))
+    return 0;
+  return read_types(m_dev_count, m_dev_types, &types, true);
+}
+
 template <size_t length>
 uint8_t* BitVoxelMap<length>::getDeviceDataPtr() {
   uint8_t* p = nullptr;
@@ -315,13 +350,15 @@ BitVoxelList<length, ID>::BitVoxelList(const Vector3ui ref_map_dim, const float 
     : GpuVoxelsMap(map_type, ref_map_dim, voxel_side_length) {
   gvx_dims d = to_dims(ref_map_dim);
   require(gvx_blist_create(&d, voxel_side_length, &m_handle), "BitVoxelList");
-  if (cudaMalloc(&m_dev_count, sizeof(uint64_t)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+  if (cudaMalloc(&m_dev_count, sizeof(uint64_t)) != cudaSuccess || cudaMalloc(&m_dev_types, 64) != cudaSuccess)
+    throw std::runtime_error("cudaMalloc failed");
 }
 
 template <size_t length, class ID>
 BitVoxelList<length, ID>::~BitVoxelList() {
   gvx_blist_destroy(m_handle);
   if (m_dev_count) cudaFree(m_dev_count);
+  if (m_dev_types) cudaFree(m_dev_types);
 }
 
 template <size_t length, class ID>
@@ -381,6 +418,67 @@ size_t BitVoxelList<length, ID>::collideWith(const BitVoxelList<length, ID>* oth
   lock_guard g(m_mutex);
   const int32_t off[3] = {0, 0, 0};
   if (!ok(gvx_blist_collide_blist(m_handle, other->m_handle, off, m_dev_count, nullptr), "collideWith")) return 0;
+  uint64_t count = 0;
+  cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
+  return (size_t)count;
+}
+
+template <size_t length, class ID>
+size_t BitVoxelList<length, ID>::collideWithTypes(const voxelmap::BitVoxelMap<length>* map, BitVectorVoxel& types, float,
+                                                  const Vector3i& offset) {
+  if (map->getDimensions() != m_dim) {
+    std::fprintf(stderr, "gpu_voxels: list reference dims differ from the map's; not checking collisions\n");
+    return SSIZE_MAX;
+  }
+  lock_guard g(m_mutex);
+  const int32_t off[3] = {offset.x, offset.y, offset.z};
+  if (!ok(gvx_blist_collide_types_bvm(m_handle, map->handle(), off, m_dev_count, m_dev_types, nullptr), "collideWithTypes"))
+    return 0;
+  return voxelmap::read_types(m_dev_count, m_dev_types, &types, false);  // the reference clears the set first
+}
+
+template <size_t length, class ID>
+size_t BitVoxelList<length, ID>::collideWithTypes(const voxelmap::ProbVoxelMap* map, BitVectorVoxel& types,
+                                                  float coll_threshold, const Vector3i& offset) {
+  if (map->getDimensions() != m_dim) {
+    std::fprintf(stderr, "gpu_voxels: list reference dims differ from the map's; not checking collisions\n");
+    return SSIZE_MAX;
+  }
+  lock_guard g(m_mutex);
+  const int32_t off[3] = {offset.x, offset.y, offset.z};
+  if (!ok(gvx_blist_collide_types_pvm(m_handle, map->handle(), coll_threshold, off, m_dev_count, m_dev_types, nullptr),
+          "collideWithTypes"))
+    return 0;
+  return voxelmap::read_types(m_dev_count, m_dev_types, &types, false);
+}
+
+template <size_t length, class ID>
+size_t BitVoxelList<length, ID>::collideWithTypes(const BitVoxelList<length, ID>* other, BitVectorVoxel& types, float,
+                                                  const Vector3i& offset) {
+  if (offset != Vector3i()) {
+    std::fprintf(stderr, "gpu_voxels: offset for voxel-list collision not supported\n");
+    types = BitVectorVoxel();
+    return 0;
+  }
+  lock_guard g(m_mutex);
+  if (!ok(gvx_blist_collide_types_blist(m_handle, other->m_handle, m_dev_count, m_dev_types, nullptr), "collideWithTypes"))
+    return 0;
+  return voxelmap::read_types(m_dev_count, m_dev_types, &types, false);
+}
+
+template <size_t length, class ID>
+size_t BitVoxelList<length, ID>::collideWithTypeMask(const voxelmap::BitVoxelMap<length>* map,
+                                                     const BitVectorVoxel& types_to_check, float, const Vector3i& offset) {
+  if (map->getDimensions() != m_dim) {
+    std::fprintf(stderr, "gpu_voxels: list reference dims differ from the map's; not checking collisions\n");
+    return SSIZE_MAX;
+  }
+  lock_guard g(m_mutex);
+  cudaMemcpy(m_dev_types + 32, types_to_check.bitVector().data(), 32, cudaMemcpyHostToDevice);
+  const int32_t off[3] = {offset.x, offset.y, offset.z};
+  if (!ok(gvx_blist_collide_type_mask_bvm(m_handle, map->handle(), m_dev_types + 32, off, m_dev_count, nullptr),
+          "collideWithTypeMask"))
+    return 0;
   uint64_t count = 0;
   cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
   return (size_t)count;

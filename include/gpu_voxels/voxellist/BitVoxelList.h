@@ -39,6 +39,20 @@ class BitVoxelList : public GpuVoxelsMap {
   size_t collideWith(const BitVoxelList<length, VoxelIDType>* other, float coll_threshold = 1.0,
                      const Vector3i& offset = Vector3i());
 
+  // collideWithTypes / collideWithTypeMask (GV/voxellist/BitVoxelList.hpp:94-246):
+  // types_in_collision receives the OR of the colliding entries' types (for a
+  // list: of both lists' entries at the common ids); against maps colliding
+  // entries get eBVM_COLLISION.  SSIZE_MAX when a map's dims differ from the
+  // list's reference dims; list vs list with an offset returns 0.
+  size_t collideWithTypes(const voxelmap::BitVoxelMap<length>* map, BitVectorVoxel& types_in_collision,
+                          float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
+  size_t collideWithTypes(const voxelmap::ProbVoxelMap* map, BitVectorVoxel& types_in_collision,
+                          float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
+  size_t collideWithTypes(const BitVoxelList<length, VoxelIDType>* other, BitVectorVoxel& types_in_collision,
+                          float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
+  size_t collideWithTypeMask(const voxelmap::BitVoxelMap<length>* map, const BitVectorVoxel& types_to_check,
+                             float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
+
   // Host copies of the ids and the 32-byte voxels.
   void copyIdsToHost(std::vector<VoxelIDType>& ids) const;
   void copyVoxelsToHost(std::vector<uint8_t>& voxels) const;
@@ -47,6 +61,7 @@ class BitVoxelList : public GpuVoxelsMap {
  private:
   gvx_blist* m_handle = nullptr;
   uint64_t* m_dev_count = nullptr;
+  uint8_t* m_dev_types = nullptr;  // 32 B result + 32 B mask
 };
 
 extern template class BitVoxelList<BIT_VECTOR_LENGTH, MapVoxelID>;

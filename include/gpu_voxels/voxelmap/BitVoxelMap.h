@@ -8,6 +8,8 @@
 #include <vector>
 
 #include "../GpuVoxelsMap.h"
+#include "../voxel/BitVoxel.h"
+#include "ProbVoxelMap.h"
 
 struct gvx_bvm;
 
@@ -32,6 +34,15 @@ class BitVoxelMap : public GpuVoxelsMap {
   // shifted by `offset`; colliding voxels of this map get eBVM_COLLISION.
   size_t collideWith(const BitVoxelMap<length>* map, float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
 
+  // collideWithTypes (GV/voxelmap/BitVoxelMap.hpp:212-224): the swept-volume
+  // types colliding with `map` (with a ProbVoxelMap: this map's types where
+  // its occupancy reaches the threshold) are OR-ed into types_in_collision;
+  // colliding voxels get eBVM_COLLISION.  `offset` is ignored, as in the reference.
+  size_t collideWithTypes(const BitVoxelMap<length>* map, BitVectorVoxel& types_in_collision,
+                          float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
+  size_t collideWithTypes(const ProbVoxelMap* map, BitVectorVoxel& types_in_collision, float coll_threshold = 1.0,
+                          const Vector3i& offset = Vector3i());
+
   // Raw 32-byte voxels on the device.
   uint8_t* getDeviceDataPtr();
   size_t getVoxelMapSize() const { return (size_t)m_dim.x * m_dim.y * m_dim.z; }
@@ -40,6 +51,7 @@ class BitVoxelMap : public GpuVoxelsMap {
  private:
   gvx_bvm* m_handle = nullptr;
   uint64_t* m_dev_count = nullptr;
+  uint8_t* m_dev_types = nullptr;
 };
 
 extern template class BitVoxelMap<BIT_VECTOR_LENGTH>;

@@ -210,9 +210,33 @@ static void distance_consumers() {
   cudaFree(d_flood);
 }
 
+// collideWithTypes: two swept volumes (meanings 10 and 20) against a map and a
+// list holding meaning 10 in an overlapping box.
+static void typed_collisions() {
+  const Vector3ui dim(32, 32, 32);
+  BitVectorVoxelMap sv(dim, 1.0f), obstacle(dim, 1.0f);
+  sv.insertPointCloud(box_of_points(Vector3f(2.5f, 2.5f, 2.5f), Vector3f(5.5f, 5.5f, 5.5f), 1.0f), BitVoxelMeaning(10));
+  sv.insertPointCloud(box_of_points(Vector3f(20.5f, 20.5f, 20.5f), Vector3f(22.5f, 22.5f, 22.5f), 1.0f),
+                      BitVoxelMeaning(20));
+  obstacle.insertPointCloud(box_of_points(Vector3f(4.5f, 4.5f, 4.5f), Vector3f(8.5f, 8.5f, 8.5f), 1.0f),
+                            BitVoxelMeaning(10));
+  BitVectorVoxel types;
+  const size_t n = sv.collideWithTypes(&obstacle, types);
+  CHECK(n == 8 && types.bitVector().getBit(10) && !types.bitVector().getBit(20), "collideWithTypes map: 8 voxels of type 10");
+  BitVectorVoxelList list(dim, 1.0f);
+  list.insertPointCloud(box_of_points(Vector3f(4.5f, 4.5f, 4.5f), Vector3f(6.5f, 6.5f, 6.5f), 1.0f), BitVoxelMeaning(30));
+  BitVectorVoxel ltypes;
+  const size_t ln = list.collideWithTypes(&obstacle, ltypes);
+  CHECK(ln == 27 && ltypes.bitVector().getBit(30), "collideWithTypes list vs map: 27 entries of type 30");
+  BitVectorVoxel mask;
+  mask.bitVector().setBit(31);
+  CHECK(list.collideWithTypeMask(&obstacle, mask) == 0, "collideWithTypeMask with a disjoint mask: 0");
+}
+
 int main() {
   GpuVoxels::getInstance();
   distance_consumers();
+  typed_collisions();
   distance_extraction();
   distance_correctness();
   collisions();
