@@ -122,6 +122,12 @@ PROTOTYPES = {
     "gvx_blist_collide_types_pvm": [_vp, _vp, _f, _i32p, _vp, _vp, _vp],
     "gvx_blist_collide_type_mask_bvm": [_vp, _vp, _vp, _i32p, _vp, _vp],
     "gvx_blist_collide_types_blist": [_vp, _vp, _vp, _vp, _vp],
+    "gvx_dvm_write_to_disk": [_vp, ctypes.c_char_p],
+    "gvx_dvm_read_from_disk": [_vp, ctypes.c_char_p],
+    "gvx_bvm_write_to_disk": [_vp, ctypes.c_char_p],
+    "gvx_bvm_read_from_disk": [_vp, ctypes.c_char_p],
+    "gvx_pvm_write_to_disk": [_vp, ctypes.c_char_p],
+    "gvx_pvm_read_from_disk": [_vp, ctypes.c_char_p],
     "gvx_blist_create": [ctypes.POINTER(Dims), _f, ctypes.POINTER(_vp)],
     "gvx_blist_destroy": [_vp],
     "gvx_blist_size": [_vp, ctypes.POINTER(_u64)],

@@ -92,6 +92,14 @@ class DistanceVoxelMap:
         call("gvx_dvm_info", self._h, ctypes.byref(d), ctypes.byref(s), ctypes.byref(p))
         return _device_view(p.value, self.size)
 
+    def writeToDisk(self, path: str) -> None:
+        """TemplateVoxelMap::writeToDisk: the reference's binary map file."""
+        call("gvx_dvm_write_to_disk", self._h, str(path).encode())
+
+    def readFromDisk(self, path: str) -> None:
+        """TemplateVoxelMap::readFromDisk (type and dims must match)."""
+        call("gvx_dvm_read_from_disk", self._h, str(path).encode())
+
     def clearMap(self) -> None:
         call("gvx_dvm_clear", self._h, _stream())
 
@@ -284,6 +292,14 @@ class ProbVoxelMap:
         call("gvx_pvm_info", self._h, ctypes.byref(d), ctypes.byref(s), ctypes.byref(p))
         return _device_view_i8(p.value, self.size)
 
+    def writeToDisk(self, path: str) -> None:
+        """TemplateVoxelMap::writeToDisk: the reference's binary map file."""
+        call("gvx_pvm_write_to_disk", self._h, str(path).encode())
+
+    def readFromDisk(self, path: str) -> None:
+        """TemplateVoxelMap::readFromDisk (type and dims must match)."""
+        call("gvx_pvm_read_from_disk", self._h, str(path).encode())
+
     def clearMap(self) -> None:
         call("gvx_pvm_clear", self._h, _stream())
 
@@ -324,6 +340,14 @@ class BitVectorVoxelMap:
         d, s, p = Dims(), ctypes.c_float(), ctypes.c_void_p()
         call("gvx_bvm_info", self._h, ctypes.byref(d), ctypes.byref(s), ctypes.byref(p))
         return _device_view_u8(p.value, self.size * 32)
+
+    def writeToDisk(self, path: str) -> None:
+        """TemplateVoxelMap::writeToDisk: the reference's binary map file."""
+        call("gvx_bvm_write_to_disk", self._h, str(path).encode())
+
+    def readFromDisk(self, path: str) -> None:
+        """TemplateVoxelMap::readFromDisk (type and dims must match)."""
+        call("gvx_bvm_read_from_disk", self._h, str(path).encode())
 
     def clearMap(self) -> None:
         call("gvx_bvm_clear", self._h, _stream())

@@ -92,6 +92,16 @@ void ProbVoxelMap::insertPointCloud(const Vector3f* d_points, uint32_t size, Bit
 
 size_t ProbVoxelMap::getMemoryUsage() const { return getVoxelMapSize(); }
 
+bool ProbVoxelMap::writeToDisk(const std::string path) {
+  lock_guard g(m_mutex);
+  return ok(gvx_pvm_write_to_disk(m_handle, path.c_str()), "writeToDisk");
+}
+
+bool ProbVoxelMap::readFromDisk(const std::string path) {
+  lock_guard g(m_mutex);
+  return ok(gvx_pvm_read_from_disk(m_handle, path.c_str()), "readFromDisk");
+}
+
 Probability* ProbVoxelMap::getDeviceDataPtr() {
   int8_t* p = nullptr;
   gvx_pvm_info(m_handle, nullptr, nullptr, &p);
@@ -136,6 +146,16 @@ void DistanceVoxelMap::insertPointCloud(const Vector3f* d_points, uint32_t size,
 }
 
 size_t DistanceVoxelMap::getMemoryUsage() const { return getVoxelMapSize() * sizeof(Voxel); }
+
+bool DistanceVoxelMap::writeToDisk(const std::string path) {
+  lock_guard g(m_mutex);
+  return ok(gvx_dvm_write_to_disk(m_handle, path.c_str()), "writeToDisk");
+}
+
+bool DistanceVoxelMap::readFromDisk(const std::string path) {
+  lock_guard g(m_mutex);
+  return ok(gvx_dvm_read_from_disk(m_handle, path.c_str()), "readFromDisk");
+}
 
 void DistanceVoxelMap::parallelBanding3D(uint32_t m1, uint32_t m2, uint32_t m3, uint32_t, uint32_t, uint32_t, bool) {
   lock_guard g(m_mutex);
@@ -327,6 +347,18 @@ size_t BitVoxelMap<length>::collideWithTypes(const ProbVoxelMap* map, BitVectorV
           "collideWithTypes"))
     return 0;
   return read_types(m_dev_count, m_dev_types, &types, true);
+}
+
+template <size_t length>
+bool BitVoxelMap<length>::writeToDisk(const std::string path) {
+  lock_guard g(m_mutex);
+  return ok(gvx_bvm_write_to_disk(m_handle, path.c_str()), "writeToDisk");
+}
+
+template <size_t length>
+bool BitVoxelMap<length>::readFromDisk(const std::string path) {
+  lock_guard g(m_mutex);
+  return ok(gvx_bvm_read_from_disk(m_handle, path.c_str()), "readFromDisk");
 }
 
 template <size_t length>

@@ -39,6 +39,11 @@ class GpuVoxelsMap {
   virtual void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) = 0;
   // Number of bytes of device memory held by the map.
   virtual size_t getMemoryUsage() const = 0;
+  // TemplateVoxelMap::writeToDisk / readFromDisk (GV/voxelmap/TemplateVoxelMap.hpp:906-1039):
+  // the reference's binary map file; false on I/O errors or (reading) another
+  // map type or dims.  Maps without a file form return false.
+  virtual bool writeToDisk(const std::string path) { (void)path; return false; }
+  virtual bool readFromDisk(const std::string path) { (void)path; return false; }
   // The map's lock, for operations that lock two maps together.
   std::recursive_timed_mutex& mutexRef() const { return m_mutex; }
 

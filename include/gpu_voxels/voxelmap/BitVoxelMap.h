@@ -28,6 +28,8 @@ class BitVoxelMap : public GpuVoxelsMap {
   void insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) override;
   void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) override;
   size_t getMemoryUsage() const override;
+  bool writeToDisk(const std::string path) override;
+  bool readFromDisk(const std::string path) override;
 
   // collideWith(const BitVectorVoxelMap*, float, const Vector3i&) (GV/voxelmap/BitVoxelMap.hpp:198-203):
   // voxels where both maps hold a meaning other than eBVM_FREE, this map

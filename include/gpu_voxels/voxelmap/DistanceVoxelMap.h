@@ -57,6 +57,8 @@ class DistanceVoxelMap : public GpuVoxelsMap {
   void insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) override;
   void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) override;
   size_t getMemoryUsage() const override;
+  bool writeToDisk(const std::string path) override;
+  bool readFromDisk(const std::string path) override;
 
   // Exact EDT (GV/voxelmap/DistanceVoxelMap.hpp:284-645).  Band counts and
   // block sizes are accepted for source compatibility; the result is always

@@ -31,6 +31,8 @@ class ProbVoxelMap : public GpuVoxelsMap {
   void insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) override;
   void insertPointCloud(const Vector3f* d_points, uint32_t size, BitVoxelMeaning voxel_meaning) override;
   size_t getMemoryUsage() const override;
+  bool writeToDisk(const std::string path) override;
+  bool readFromDisk(const std::string path) override;
 
   Probability* getDeviceDataPtr();
   size_t getVoxelMapSize() const { return (size_t)m_dim.x * m_dim.y * m_dim.z; }

@@ -308,6 +308,20 @@ GVX_API gvx_status gvx_pvm_insert_points(gvx_pvm *m, const float *d_xyz, uint64_
 GVX_API gvx_status gvx_dvm_merge_occupied(gvx_dvm *m, const gvx_pvm *other, const uint32_t offset[3],
                                           float occupancy_threshold, gvx_stream stream);
 
+/* ---- On-disk format ------------------------------------------------------- */
+/* Replace TemplateVoxelMap::writeToDisk / readFromDisk (GV/voxelmap/TemplateVoxelMap.hpp:906-1039),
+ * binary mode: int32 MapType (BitVectorVoxelMap 0, ProbVoxelMap 4,
+ * DistanceVoxelMap 9), float voxel side, uint32 x, y, z, then the voxels byte
+ * for byte -- files interchange with the reference's.  Blocking (the device
+ * is synchronised first).  Reading fails on a different type or dims and
+ * only warns on a different voxel side, as the reference does. */
+GVX_API gvx_status gvx_dvm_write_to_disk(const gvx_dvm *m, const char *path);
+GVX_API gvx_status gvx_dvm_read_from_disk(gvx_dvm *m, const char *path);
+GVX_API gvx_status gvx_bvm_write_to_disk(const gvx_bvm *m, const char *path);
+GVX_API gvx_status gvx_bvm_read_from_disk(gvx_bvm *m, const char *path);
+GVX_API gvx_status gvx_pvm_write_to_disk(const gvx_pvm *m, const char *path);
+GVX_API gvx_status gvx_pvm_read_from_disk(gvx_pvm *m, const char *path);
+
 /* ---- Consumers of the distance field ------------------------------------- */
 
 /* Replaces DistanceVoxelMap::extract_distances(free_space_t*, robot_radius)

@@ -179,6 +179,13 @@ static void prob_map_to_distance_map() {
   dist->parallelBanding3D();
   // the voxel at (30,30,30) is nearest to the cube's corner (40,40,40): 3 * 10^2
   CHECK(dist->getSquaredObstacleDistance(30, 30, 30) == 300, "EDT after mergeOccupied: corner distance 300");
+  const std::string file = "/tmp/gvx_test_dist_map.gvm";
+  CHECK(dist->writeToDisk(file), "writeToDisk");
+  voxelmap::DistanceVoxelMap loaded(Vector3ui(128, 128, 128), 1.0f);
+  CHECK(loaded.readFromDisk(file) && loaded.getSquaredObstacleDistance(30, 30, 30) == 300, "readFromDisk round trip");
+  voxelmap::DistanceVoxelMap other(Vector3ui(64, 64, 64), 1.0f);
+  CHECK(!other.readFromDisk(file), "readFromDisk rejects other dims");
+  std::remove(file.c_str());
   gvl->delMap("myProbVoxelMap");
   gvl->delMap("myDistanceMap");
 }
