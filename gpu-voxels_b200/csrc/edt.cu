@@ -511,8 +511,14 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   if (nchunks > 1) stage_chunk<kXPass, kRows>(tile1, s, 1, vec16);
   cp_async_commit();
 
-  int n = 0;   // stack depth
-  int lo = 0;  // lowest depth guaranteed to be in the ring
+  // The stack lives in the ring (depths [lo, n)) and in the workspace
+  // (depths [0, spill)); lo <= spill whenever both ranges matter.  An entry
+  // is written to the workspace only when a push evicts it from the ring (and
+  // the ring's remainder once phase 2 ends), so entries pushed and popped
+  // within the ring's reach never leave the chip.
+  int n = 0;      // stack depth
+  int lo = 0;     // lowest depth in the ring
+  int spill = 0;  // depths below it have their workspace copy
   Col top{0u, 0.f, 0.f}, sec{0u, 0.f, 0.f};
   float top_i = 0.f, sec_i = 0.f;  // bisector(second, top), bisector(third, second)
   Col last{0u, 0.f, 0.f};          // the last site seen (the top before the next row)
@@ -588,11 +594,17 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
         }
         if (has) {
           if (n == 0) i2 = 0.f;
+          spill = min(spill, n);  // workspace copies at or above n are stale
+          lo = min(lo, n);
           const int slot = (n % Cfg::kRing) * 32;  // push the current site
+          const int ev = n - Cfg::kRing;             // the depth this slot held
+          if (ev >= lo && ev >= spill) {             // evicted before it reached the workspace
+            gstk[ev * 32] = make_uint2(ringE[slot], __float_as_uint(ringI[slot]));
+            spill = ev + 1;
+          }
           ringE[slot] = cur.e;
           ringI[slot] = i2;
-          gstk[n * 32] = make_uint2(cur.e, __float_as_uint(i2));
-          lo = max(lo, n - Cfg::kRing + 1);
+          lo = max(lo, ev + 1);
           ++n;
           sec = top;
           sec_i = top_i;
@@ -605,6 +617,9 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     if (c + 2 < nchunks) stage_chunk<kXPass, kRows>((c & 1) ? tile1 : tile0, s, c + 2, vec16);
     cp_async_commit();
   }
+  // the ring's entries that never reached the workspace
+  spill = min(spill, n);
+  for (int d = spill; d < n; ++d) gstk[d * 32] = make_uint2(ringE[(d % Cfg::kRing) * 32], __float_as_uint(ringI[(d % Cfg::kRing) * 32]));
   cp_async_wait_all();
   __syncwarp();
 
