@@ -355,10 +355,6 @@ struct SweepCfg {
   static constexpr int kStagePitch = 36;
   static constexpr int kStageWords = kStageRows * kStagePitch;
   static constexpr int kWin = 32;
-  // Phase-2 rows whose first bisectors are computed together (stage A); 1
-  // measured fastest on B200 -- larger groups raise register pressure past
-  // the 3-blocks-per-SM budget (2: +1%, 4: +17%, 8: x2.3 at 512^3).
-  static constexpr int kGroup = 1;
   static constexpr int kPhase3Words = kStageWords + kWin * 64;
   static constexpr int kWarpWords = kPhase2Words > kPhase3Words ? kPhase2Words : kPhase3Words;
   static_assert((kWin & (kWin - 1)) == 0, "window slots are depth mod kWin");
@@ -521,8 +517,6 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   int spill = 0;  // depths below it have their workspace copy
   Col top{0u, 0.f, 0.f}, sec{0u, 0.f, 0.f};
   float top_i = 0.f, sec_i = 0.f;  // bisector(second, top), bisector(third, second)
-  Col last{0u, 0.f, 0.f};          // the last site seen (the top before the next row)
-  constexpr int kGroup = Cfg::kGroup;
   for (int c = 0; c < nchunks; ++c) {
     cp_async_wait1();
     __syncwarp();
@@ -530,33 +524,23 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     const int r0 = c * kRows;
     const int rows = min(kRows, L - r0);
     float row2f = small_to_float(2 * r0);  // 2 * row, exact
-    for (int r = 0; r < rows; r += kGroup) {
-      // Stage A, kGroup rows at once: each row's site and its bisector with
-      // the top it will meet.  Before a row's pops the top is always the site
-      // of the last earlier row that had one, so these bisectors do not
-      // depend on the stack and the divisions of a group run independently.
-      Col gc[kGroup];
-      float gb[kGroup];
-      bool gh[kGroup];
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j, row2f += 2.0f) {
-        const uint32_t v = r + j < rows ? tile[(r + j) * tpitch + lane] : kDvUninit;
-        const uint32_t a = kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
-        gh[j] = a != kUninit;
-        gc[j].e = a | ((uint32_t)(r0 + r + j) << 10) | (v & 0xFFF00000u);
-        gc[j].r2 = row2f;
+    for (int r = 0; r < rows; ++r, row2f += 2.0f) {
+      const uint32_t v = tile[r * tpitch + lane];
+      const uint32_t a = kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
+      const bool has = a != kUninit;
+      Col cur;
+      cur.e = a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u);
+      cur.r2 = row2f;
+      {
         const float da = biased(a) - A0;
         const float dc = biased(v >> 20) - C0;
-        gc[j].d = __fmaf_rn(da, da, __fmul_rn(dc, dc));
-        gb[j] = bisect(last, gc[j]);  // used only when an earlier site exists
-        if (gh[j]) last = gc[j];
+        cur.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));
       }
-      // Stage B: the stack, row by row.
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j) {
-        const bool has = gh[j];
-        const Col& cur = gc[j];
-        float i2 = gb[j];
+      // Before a row's pops the top is the site of the last earlier row that
+      // had one, so this bisector does not wait for the pops of earlier rows;
+      // computed for every lane (used only when the stack is not empty).
+      float i2 = bisect(top, cur);
+      {
         bool deep = false;
         if (has) {
           for (int p = 0; n >= 2 && !(top_i < i2); ++p) {  // top is dominated by (second, current): pop
