@@ -108,6 +108,49 @@ def _traffic_from_profiles():
         return {}
 
 
+class Ranks:
+    """The bench's multi-process plumbing: one process per GPU (torchrun env),
+    replicas with no data-path collective -- only a barrier around the timed
+    region and the max of the per-rank times.  backend "nccl" on GPUs,
+    "gloo" for the CPU tests of this logic."""
+
+    def __init__(self, backend: str = "nccl"):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
+        self.dist = None
+        if self.world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+            dist.init_process_group(backend, timeout=timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def whole_job_rate(units_per_rank: float, world: int, ms: float, scale: float = 1e9) -> float:
+    """Throughput of the whole job: the units every rank processed over the
+    slowest rank's time (ms), in units of `scale` per second."""
+    return units_per_rank * world / (ms / 1e3) / scale
+
+
 # ---------------------------------------------------------------------------
 # reference arm: the CPU restatement (gpu-voxels has no CPU path of its own)
 # ---------------------------------------------------------------------------
@@ -428,26 +471,11 @@ def main():
     import gvx
     from gvx import workloads
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl")
+    world, rank = ranks.world, ranks.rank
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     stream = torch.cuda.current_stream()
     hbm_peak, peak_kind = _peaks()
@@ -489,7 +517,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = nvox * args.steps * world / (ms / 1e3) / 1e9
+    value = whole_job_rate(nvox * args.steps, world, ms)
     for _ in range(args.warmup):
         three_calls()
     torch.cuda.synchronize()
@@ -566,7 +594,7 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    e2e = {"value": round(nvox * args.steps * world / (e2e_ms / 1e3) / 1e9, 3), "unit": "Gvoxel/s",
+    e2e = {"value": round(whole_job_rate(nvox * args.steps, world, e2e_ms), 3), "unit": "Gvoxel/s",
            "h2d_bytes_per_step": int(pinned.numel() * 4 + q_host.numel() * 4),
            "d2h_bytes_per_step": int(out_host.numel() * 4),
            "ms_per_step": round(e2e_ms / args.steps, 4),
@@ -623,9 +651,7 @@ def main():
             line["sections"] = run_sections(args, hbm_peak, pts_host)
         print(json.dumps(line), flush=True)
 
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":
