@@ -56,10 +56,14 @@ __global__ void trilinear_bwd_kernel(MapView m, const float* __restrict__ xyz, u
 // Forward kinematics: frames F_0 = base, F_{j+1} = F_j * A_j(q_j),
 // A_j = Rz(theta_j + q_j) Tz(d_j) Tx(a_j) Rx(alpha_j).  Link j spans origin
 // o_j -> o_{j+1}; joint j turns about z_j (third column of F_j) through o_j.
+// The chain runs once per configuration (one lane) in FP64, and sphere
+// centres are formed in FP64 and rounded once to FP32: an FP32 chain of
+// seven frames alone puts the centres ~1e-6 m off, 1e-4 voxel at 1 cm.  The
+// distance queries themselves stay FP32.
 // ---------------------------------------------------------------------------
 struct Frame {
-  float r[9];  // row-major rotation
-  float o[3];
+  double r[9];  // row-major rotation
+  double o[3];
 };
 
 __device__ __forceinline__ Frame base_frame(const gvx_arm& arm) {
@@ -72,11 +76,11 @@ __device__ __forceinline__ Frame base_frame(const gvx_arm& arm) {
 }
 
 __device__ __forceinline__ Frame dh_step(const Frame& F, const gvx_arm& arm, int j, float q) {
-  float st, ct, sa, ca;
-  sincosf(arm.theta[j] + q, &st, &ct);
-  sincosf(arm.alpha[j], &sa, &ca);
-  const float A[9] = {ct, -st * ca, st * sa, st, ct * ca, -ct * sa, 0.0f, sa, ca};
-  const float t[3] = {arm.a[j] * ct, arm.a[j] * st, arm.d[j]};
+  double st, ct, sa, ca;
+  sincos((double)arm.theta[j] + (double)q, &st, &ct);
+  sincos((double)arm.alpha[j], &sa, &ca);
+  const double A[9] = {ct, -st * ca, st * sa, st, ct * ca, -ct * sa, 0.0, sa, ca};
+  const double t[3] = {(double)arm.a[j] * ct, (double)arm.a[j] * st, (double)arm.d[j]};
   Frame G;
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -90,8 +94,8 @@ __device__ __forceinline__ Frame dh_step(const Frame& F, const gvx_arm& arm, int
 
 // Per-warp FK into shared memory: origins o[0..J] and joint axes z[0..J-1].
 struct WarpFK {
-  float o[GVX_MAX_JOINTS + 1][3];
-  float z[GVX_MAX_JOINTS][3];
+  double o[GVX_MAX_JOINTS + 1][3];
+  double z[GVX_MAX_JOINTS][3];
 };
 
 __device__ __forceinline__ void warp_fk(const gvx_arm& arm, const float* q, WarpFK& fk) {
@@ -110,9 +114,9 @@ __device__ __forceinline__ void warp_fk(const gvx_arm& arm, const float* q, Warp
 
 __device__ __forceinline__ void sphere_centre(const gvx_arm& arm, const WarpFK& fk, int s, float c[3]) {
   const int j = arm.link[s];
-  const float t = arm.t[s];
+  const double t = arm.t[s];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) c[i] = fmaf(t, fk.o[j + 1][i] - fk.o[j][i], fk.o[j][i]);
+  for (int i = 0; i < 3; ++i) c[i] = (float)fma(t, fk.o[j + 1][i] - fk.o[j][i], fk.o[j][i]);
 }
 
 constexpr int kWarpsPerBlock = 8;
@@ -224,12 +228,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapV
       float M[3] = {0.f, 0.f, 0.f}, G[3] = {0.f, 0.f, 0.f};
       for (int k = J - 1; k >= 0; --k) {
         for (int i = 0; i < 3; ++i) { M[i] += s_link[warp][k][i]; G[i] += s_link[warp][k][3 + i]; }
-        const float* o = s_fk[warp].o[k];
-        const float* z = s_fk[warp].z[k];
-        const float v0 = M[0] - (o[1] * G[2] - o[2] * G[1]);
-        const float v1 = M[1] - (o[2] * G[0] - o[0] * G[2]);
-        const float v2 = M[2] - (o[0] * G[1] - o[1] * G[0]);
-        gq[item * J + k] = -g * (z[0] * v0 + z[1] * v1 + z[2] * v2);
+        const double* o = s_fk[warp].o[k];
+        const double* z = s_fk[warp].z[k];
+        const double v0 = M[0] - (o[1] * G[2] - o[2] * G[1]);
+        const double v1 = M[1] - (o[2] * G[0] - o[0] * G[2]);
+        const double v2 = M[2] - (o[0] * G[1] - o[1] * G[0]);
+        gq[item * J + k] = (float)(-g * (z[0] * v0 + z[1] * v1 + z[2] * v2));
       }
     }
     __syncwarp();
