@@ -369,7 +369,7 @@ struct SweepCfg {
 // Lane 31 only supplies the entry below lane 30's, so a round covers 31
 // depths.  All 32 lanes call this; only lane o's state changes.
 template <class Cfg>
-__device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t* ring_base, const uint2* gstk_base,
+__device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t* ring_base, const uint2* gstk_base, int L,
                                           int& n, int& lo, const Col& cur, Col& top, float& top_i, Col& sec,
                                           float& sec_i, float& i2) {
   const int lane = threadIdx.x & 31;
@@ -380,7 +380,7 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t
   const Col oc = make_col(ce, oA0, C0);
   uint32_t* ringE = ring_base + o;
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
-  const uint2* gstk = gstk_base + o;
+  const uint2* gstk = gstk_base + (size_t)o * L;
   for (int start = on - 1;; start -= 31) {
     const int j = start - lane;
     const int jc = max(j, 0);
@@ -392,7 +392,7 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t
       I = ringI[(jc % Cfg::kRing) * 32];
       ec = make_col(e, oA0, C0);
     } else {
-      const uint2 p = gstk[jc * 32];
+      const uint2 p = gstk[jc];
       e = p.x;
       I = __uint_as_float(p.y);
       ec = make_col(e, oA0, C0);
@@ -465,7 +465,8 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
 // One warp item of pass Y (kXPass false) or X: 32 adjacent columns of one
 // z slice; wbase = the warp's kWarpWords of shared memory; stack = L * 64
 // words of workspace: entry d of lane l is the pair (site, bisector with the
-// entry below) at ((uint2*)stack)[d * 32 + l].
+// entry below) at ((uint2*)stack)[l * L + d] -- each lane's stack contiguous,
+// so its spills, refills and window reads fill whole sectors.
 template <bool kXPass, int kRows>
 __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t* __restrict__ stack, int X, int Y,
                                            int Z, long long item, uint32_t* wbase) {
@@ -486,7 +487,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   uint32_t* tile1 = wbase + Cfg::kTileWords;
   uint32_t* ringE = wbase + 2 * Cfg::kTileWords + lane;  // slot k: ringE[k * 32]
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
-  uint2* gstk = reinterpret_cast<uint2*>(stack) + lane;  // depth d: gstk[d * 32]
+  uint2* gstk = reinterpret_cast<uint2*>(stack) + (size_t)lane * L;  // this lane's stack, depth d: gstk[d]
   const float A0 = biased((uint32_t)(s.a0_base + lane));  // this lane's column coordinate, biased
   const float C0 = biased((uint32_t)z);
   const int nchunks = (L + kRows - 1) / kRows;
@@ -557,7 +558,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
                 sec = make_col(ringE[(d % Cfg::kRing) * 32], A0, C0);
                 sec_i = ringI[(d % Cfg::kRing) * 32];
               } else {  // below the ring: the workspace has the entries
-                const uint2 p = gstk[d * 32];
+                const uint2 p = gstk[d];
                 sec = make_col(p.x, A0, C0);
                 sec_i = __uint_as_float(p.y);
               }
@@ -572,7 +573,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           while (deep_lanes) {
             const int o = __ffs(deep_lanes) - 1;
             deep_lanes &= deep_lanes - 1;
-            coop_pops<Cfg>(o, s.a0_base, C0, wbase + 2 * Cfg::kTileWords, gstk - lane, n, lo, cur, top, top_i, sec,
+            coop_pops<Cfg>(o, s.a0_base, C0, wbase + 2 * Cfg::kTileWords, gstk - (size_t)lane * L, L, n, lo, cur, top, top_i, sec,
                            sec_i, i2);
           }
         }
@@ -583,7 +584,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           const int slot = (n % Cfg::kRing) * 32;  // push the current site
           const int ev = n - Cfg::kRing;             // the depth this slot held
           if (ev >= lo && ev >= spill) {             // evicted before it reached the workspace
-            gstk[ev * 32] = make_uint2(ringE[slot], __float_as_uint(ringI[slot]));
+            gstk[ev] = make_uint2(ringE[slot], __float_as_uint(ringI[slot]));
             spill = ev + 1;
           }
           ringE[slot] = cur.e;
@@ -603,7 +604,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   }
   // the ring's entries that never reached the workspace
   spill = min(spill, n);
-  for (int d = spill; d < n; ++d) gstk[d * 32] = make_uint2(ringE[(d % Cfg::kRing) * 32], __float_as_uint(ringI[(d % Cfg::kRing) * 32]));
+  for (int d = spill; d < n; ++d) gstk[d] = make_uint2(ringE[(d % Cfg::kRing) * 32], __float_as_uint(ringI[(d % Cfg::kRing) * 32]));
   cp_async_wait_all();
   __syncwarp();
 
@@ -627,7 +628,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   // so one request spans at most kWin depths and no two copies in flight
   // target the same slot.
   auto request = [&](int hi, int new_lo) {
-    for (int d = hi - 1; d >= new_lo; --d) cp_async8(win + (d & (kWin - 1)) * 32, gstk + d * 32);
+    for (int d = hi - 1; d >= new_lo; --d) cp_async8(win + (d & (kWin - 1)) * 32, gstk + d);
     cp_async_commit();
     flo = min(flo, new_lo);
   };
@@ -635,7 +636,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     if (d < safe_lo) {
       cp_async_wait_all();
       safe_lo = flo;
-      if (d < flo) return gstk[d * 32];
+      if (d < flo) return gstk[d];
     }
     return win[(d & (kWin - 1)) * 32];
   };

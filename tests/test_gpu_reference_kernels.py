@@ -50,10 +50,15 @@ def test_reference_kernels_equal_oracle_and_library(ref, name, dims, gen, side):
     assert ref.ref_dvm_insert(ins_r, np.asarray(dims, np.uint32), np.float32(side), np.ascontiguousarray(pts, np.float32),
                               pts.shape[0], ctypes.byref(flag)) == 0
     assert np.array_equal(ins_r, ins_o)
-    edt_r = _ref_edt(ref, ins_o, dims)
-    assert np.array_equal(edt_r, edt_o), first_mismatch(edt_r, edt_o, dims)
     _, edt_g, _ = gpu_edt(dims, side, pts)
-    assert np.array_equal(edt_g, edt_r), first_mismatch(edt_g, edt_r, dims)
+    assert np.array_equal(edt_g, edt_o), first_mismatch(edt_g, edt_o, dims)
+    edt_r = _ref_edt(ref, ins_o, dims)
+    if not np.array_equal(edt_r, edt_o):
+        # a second run tells a transient result of the reference kernels
+        # apart from a disagreement that reproduces
+        again = _ref_edt(ref, ins_o, dims)
+        raise AssertionError(dict(first_run=first_mismatch(edt_r, edt_o, dims),
+                                  second_run=first_mismatch(again, edt_o, dims)))
 
 
 def test_reference_banded_settings_keep_distances(ref):
