@@ -191,6 +191,20 @@ gvx_status gvx_dvm_edt_check(gvx_dvm* m, uint32_t* flags) {
   return GVX_OK;
 }
 
+gvx_status gvx_check_bisector_quotient(uint64_t* mismatches) {
+  if (mismatches == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  unsigned long long* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(unsigned long long));
+  if (e != cudaSuccess) return cuda_status(e, "bisector check");
+  unsigned long long h = 0;
+  e = check_bisector_quotient(d, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_status(e, "bisector check");
+  *mismatches = h;
+  return GVX_OK;
+}
+
 gvx_status gvx_dvm_sqdist(const gvx_dvm* m, const uint32_t* d_ids, uint64_t n, int32_t* d_out, gvx_stream stream) {
   if (m == nullptr || (n > 0 && (d_ids == nullptr || d_out == nullptr))) return fail(GVX_ERR_INVALID_ARG, "null argument");
   return cuda_status(launch_dvm_sqdist(m->d_vox, m->dims, d_ids, n, d_out, 0, as_stream(stream)), "getSquaredDistances");

@@ -328,8 +328,29 @@ __device__ __forceinline__ Col make_col(uint32_t e, float A0, float C0) {
 // exact: bit for bit the reference's float.  With r2 = 2 * row the divisor is
 // r2' - r2 (never 0: stacked sites have distinct rows) and the midpoint
 // 0.25 * (r2 + r2'), both exact.
+//
+// The quotient is rounded to nearest without the general divide: num is an
+// integer with |num| < 2^21 and den an even integer in [2, 2046] (rows below
+// 1024, the later site second).  Markstein's correction (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Develop. 34(1), 1990): with y the reciprocal of den
+// rounded to nearest and q0 within an ulp of num/den, the residual
+// r = num - q0*den is exact in one fma and fma(r, y, q0) is num/den rounded to
+// nearest.  y comes from the hardware's approximate reciprocal and one Newton
+// step.  No quotient of this domain is a tie (num/den either has at most 21
+// significant bits or is not a finite binary fraction).  gvx_check_bisector_quotient
+// compares every (num, den) of the domain with the IEEE divide on the device.
+__device__ __forceinline__ float quotient_rn(float num, float den) {
+  float y0;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(den));
+  const float y = __fmaf_rn(__fmaf_rn(-den, y0, 1.0f), y0, y0);
+  const float q0 = __fmul_rn(num, y);
+  const float r = __fmaf_rn(-q0, den, num);
+  return __fmaf_rn(r, y, q0);
+}
+
 __device__ __forceinline__ float bisect(const Col& s1, const Col& s2) {
-  const float q = __fdiv_rn(__fsub_rn(s2.d, s1.d), __fsub_rn(s2.r2, s1.r2));
+  const float q = quotient_rn(__fsub_rn(s2.d, s1.d), __fsub_rn(s2.r2, s1.r2));
   return __fadd_rn(__fmul_rn(__fadd_rn(s1.r2, s2.r2), 0.25f), q);
 }
 
@@ -346,7 +367,7 @@ template <int kRows>
 struct SweepCfg {
   static constexpr int kWarps = 8;                       // warps per CTA
   static constexpr int kTileWords = kRows * 33;          // one staging tile
-  static constexpr int kRing = 16;                       // ring slots per lane
+  static constexpr int kRing = 16;                       // ring slots per lane (a power of two)
   static constexpr int kPhase2Words = 2 * kTileWords + 2 * kRing * 32;
   // Phase 3: pass X stages kStageRows output rows (pitch 36) before its
   // transposed flush; pass Y stores rows directly.  The stack window (kWin
@@ -358,6 +379,7 @@ struct SweepCfg {
   static constexpr int kPhase3Words = kStageWords + kWin * 64;
   static constexpr int kWarpWords = kPhase2Words > kPhase3Words ? kPhase2Words : kPhase3Words;
   static_assert((kWin & (kWin - 1)) == 0, "window slots are depth mod kWin");
+  static_assert((kRing & (kRing - 1)) == 0, "ring slots are depth mod kRing");
   static_assert(kStageWords % 2 == 0 && kWarpWords % 2 == 0, "8-byte window entries need even offsets");
 };
 
@@ -388,8 +410,8 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t
     float I = 0.f;
     Col ec;
     if (jc >= olo) {
-      e = ringE[(jc % Cfg::kRing) * 32];
-      I = ringI[(jc % Cfg::kRing) * 32];
+      e = ringE[(jc & (Cfg::kRing - 1)) * 32];
+      I = ringI[(jc & (Cfg::kRing - 1)) * 32];
       ec = make_col(e, oA0, C0);
     } else {
       const uint2 p = gstk[jc];
@@ -408,8 +430,8 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t
       const int u_last = min(t + Cfg::kRing - 2, 31);
       const int new_lo = max(start - u_last, 0);
       if (lane >= t && lane <= u_last && j >= 0 && jc < olo) {
-        ringE[(jc % Cfg::kRing) * 32] = e;
-        ringI[(jc % Cfg::kRing) * 32] = I;
+        ringE[(jc & (Cfg::kRing - 1)) * 32] = e;
+        ringI[(jc & (Cfg::kRing - 1)) * 32] = I;
       }
       const uint32_t e_top = __shfl_sync(kFullMask, e, t);
       const float i_top = __shfl_sync(kFullMask, I, t);
@@ -555,8 +577,8 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
             if (n >= 2) {
               const int d = n - 2;
               if (d >= lo) {
-                sec = make_col(ringE[(d % Cfg::kRing) * 32], A0, C0);
-                sec_i = ringI[(d % Cfg::kRing) * 32];
+                sec = make_col(ringE[(d & (Cfg::kRing - 1)) * 32], A0, C0);
+                sec_i = ringI[(d & (Cfg::kRing - 1)) * 32];
               } else {  // below the ring: the workspace has the entries
                 const uint2 p = gstk[d];
                 sec = make_col(p.x, A0, C0);
@@ -581,7 +603,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           if (n == 0) i2 = 0.f;
           spill = min(spill, n);  // workspace copies at or above n are stale
           lo = min(lo, n);
-          const int slot = (n % Cfg::kRing) * 32;  // push the current site
+          const int slot = (n & (Cfg::kRing - 1)) * 32;  // push the current site
           const int ev = n - Cfg::kRing;             // the depth this slot held
           if (ev >= lo && ev >= spill) {             // evicted before it reached the workspace
             gstk[ev] = make_uint2(ringE[slot], __float_as_uint(ringI[slot]));
@@ -604,7 +626,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   }
   // the ring's entries that never reached the workspace
   spill = min(spill, n);
-  for (int d = spill; d < n; ++d) gstk[d] = make_uint2(ringE[(d % Cfg::kRing) * 32], __float_as_uint(ringI[(d % Cfg::kRing) * 32]));
+  for (int d = spill; d < n; ++d) gstk[d] = make_uint2(ringE[(d & (Cfg::kRing - 1)) * 32], __float_as_uint(ringI[(d & (Cfg::kRing - 1)) * 32]));
   cp_async_wait_all();
   __syncwarp();
 
@@ -1059,7 +1081,27 @@ long long batch_stack_warps() {
   return blocks * Cfg::kWarps;
 }
 
+// Every (num, den) of the bisector domain: den = 2 * (blockIdx.y + 1), num
+// over (-2^21, 2^21); counts quotients whose bits differ from the IEEE divide.
+__global__ void quotient_check_kernel(unsigned long long* __restrict__ mismatches) {
+  const float den = (float)(2 * (blockIdx.y + 1));
+  constexpr int kHalf = (1 << 21) - 1;
+  unsigned long long bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= 2 * kHalf; i += gridDim.x * blockDim.x) {
+    const float num = (float)(i - kHalf);
+    bad += __float_as_uint(quotient_rn(num, den)) != __float_as_uint(__fdiv_rn(num, den));
+  }
+  if (bad) atomicAdd(mismatches, bad);
+}
+
 }  // namespace
+
+cudaError_t check_bisector_quotient(unsigned long long* d_mismatches, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_mismatches, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  quotient_check_kernel<<<dim3(64, 1023), 256, 0, s>>>(d_mismatches);
+  return cudaGetLastError();
+}
 
 void set_edt_sweep_rows(int rows) { g_sweep_rows = rows == 32 ? 32 : 16; }
 

@@ -134,6 +134,9 @@ cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scrat
                             cudaStream_t s, int rows = 0);
 // Synchronous read of the error word the last fused launch left (0 = ok).
 cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag);
+// Counts the quotients of the EDT bisector domain whose bits differ from the
+// IEEE divide (every numerator and divisor the sweeps can meet).
+cudaError_t check_bisector_quotient(unsigned long long* d_mismatches, cudaStream_t s);
 // Resident warps of the fused batch launch (size of the batch stack pool).
 long long edt_batch_stack_warps();
 // Rows per staging chunk of the sweeps (16 or 32).

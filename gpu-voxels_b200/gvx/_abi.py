@@ -77,6 +77,7 @@ PROTOTYPES = {
     "gvx_dvm_edt": [_vp, _u32, _u32, _u32, _vp],
     "gvx_dvm_edt_pass": [_vp, ctypes.c_int, _vp],
     "gvx_dvm_edt_check": [_vp, ctypes.POINTER(_u32)],
+    "gvx_check_bisector_quotient": [ctypes.POINTER(_u64)],
     "gvx_dvm_voxelize_edt": [_vp, _vp, _u64, _vp, _vp],
     "gvx_dvm_autotune": [_vp, ctypes.c_int, ctypes.POINTER(EdtConfig), _vp],
     "gvx_dvm_set_edt_config": [_vp, ctypes.POINTER(EdtConfig)],

@@ -126,6 +126,12 @@ GVX_API gvx_status gvx_dvm_set_edt_config(gvx_dvm *m, const gvx_edt_config *cfg)
  * time, else non-zero with GVX_ERR_TIMEOUT (the map's content is then
  * invalid).  No counterpart in the reference, whose EDT has no waits. */
 GVX_API gvx_status gvx_dvm_edt_check(gvx_dvm *m, uint32_t *flags);
+/* Self-check of the EDT's bisector arithmetic on this device: the sweeps
+ * round the quotient of devicePBAintersection3DY (VoxelMapOperationsPBA.hpp:
+ * 265-276) without the general divide.  Compares it, bit for bit, with the
+ * IEEE divide for every numerator (|num| < 2^21) and divisor (even, 2..2046)
+ * the sweeps can meet; *mismatches = 0 when all agree.  Synchronous. */
+GVX_API gvx_status gvx_check_bisector_quotient(uint64_t *mismatches);
 
 /* No counterpart in the reference.  The same EDT as gvx_dvm_edt, in place on
  * caller-owned device voxels (uint32 DistanceVoxels, x fastest, 16-byte

@@ -193,3 +193,13 @@ def test_voxelize_edt_equals_clear_insert_edt(case):
     assert torch.equal(a.data(), b.data())
     assert int(fa.item()) == int(fb.item())
     assert np.array_equal(to_u32(b.data()), want)
+
+
+def test_bisector_quotient_equals_ieee_divide_over_domain():
+    """The sweeps round the bisector quotient without the general divide; every
+    (numerator, divisor) they can meet gives the IEEE divide's bits."""
+    import ctypes
+    from gvx import _abi
+    bad = ctypes.c_uint64(1)
+    _abi.check(_abi.lib().gvx_check_bisector_quotient(ctypes.byref(bad)))
+    assert bad.value == 0
