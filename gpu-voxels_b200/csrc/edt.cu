@@ -389,10 +389,11 @@ struct SweepCfg {
 // test depends only on e_j, I_j and cur, so lane t tests depth start - t and
 // the first kept depth (lowest t) is exactly where the sequential loop stops.
 // Lane 31 only supplies the entry below lane 30's, so a round covers 31
-// depths.  All 32 lanes call this; only lane o's state changes.
+// depths.  All 32 lanes call this; only lane o's state changes (sec_e: the
+// packed entry below the top, decoded only when it becomes the top).
 template <class Cfg>
 __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t* ring_base, const uint2* gstk_base, int L,
-                                          int& n, int& lo, const Col& cur, Col& top, float& top_i, Col& sec,
+                                          int& n, int& lo, const Col& cur, Col& top, float& top_i, uint32_t& sec_e,
                                           float& sec_i, float& i2) {
   const int lane = threadIdx.x & 31;
   const int on = __shfl_sync(kFullMask, n, o);
@@ -406,19 +407,16 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t
   for (int start = on - 1;; start -= 31) {
     const int j = start - lane;
     const int jc = max(j, 0);
-    uint32_t e;
-    float I = 0.f;
-    Col ec;
-    if (jc >= olo) {
-      e = ringE[(jc & (Cfg::kRing - 1)) * 32];
-      I = ringI[(jc & (Cfg::kRing - 1)) * 32];
-      ec = make_col(e, oA0, C0);
-    } else {
+    // the ring slot, replaced by the workspace entry below the ring (a
+    // predicated load, so one decode and no divergent branch)
+    uint32_t e = ringE[(jc & (Cfg::kRing - 1)) * 32];
+    float I = ringI[(jc & (Cfg::kRing - 1)) * 32];
+    if (jc < olo) {
       const uint2 p = gstk[jc];
       e = p.x;
       I = __uint_as_float(p.y);
-      ec = make_col(e, oA0, C0);
     }
+    const Col ec = make_col(e, oA0, C0);
     const float b = bisect(ec, oc);
     const bool keep = j <= 0 || I < b;
     const unsigned kb = __ballot_sync(kFullMask, keep) & 0x7fffffffu;
@@ -444,7 +442,7 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t
         top = make_col(e_top, oA0, C0);
         top_i = i_top;
         i2 = b_top;
-        sec = make_col(e_sec, oA0, C0);
+        sec_e = e_sec;
         sec_i = i_sec;
       }
       __syncwarp();  // the refill before lane o's next ring access
@@ -538,8 +536,11 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   int n = 0;      // stack depth
   int lo = 0;     // lowest depth in the ring
   int spill = 0;  // depths below it have their workspace copy
-  Col top{0u, 0.f, 0.f}, sec{0u, 0.f, 0.f};
-  float top_i = 0.f, sec_i = 0.f;  // bisector(second, top), bisector(third, second)
+  // The top decoded; the entry below it packed (decoded when a pop makes it
+  // the top).  top_i = bisector(second, top), sec_i = bisector(third, second).
+  Col top{0u, 0.f, 0.f};
+  uint32_t sec_e = 0u;
+  float top_i = 0.f, sec_i = 0.f;
   for (int c = 0; c < nchunks; ++c) {
     cp_async_wait1();
     __syncwarp();
@@ -572,18 +573,18 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
               break;
             }
             --n;
-            top = sec;
+            top = make_col(sec_e, A0, C0);
             top_i = sec_i;
-            if (n >= 2) {
-              const int d = n - 2;
-              if (d >= lo) {
-                sec = make_col(ringE[(d & (Cfg::kRing - 1)) * 32], A0, C0);
-                sec_i = ringI[(d & (Cfg::kRing - 1)) * 32];
-              } else {  // below the ring: the workspace has the entries
-                const uint2 p = gstk[d];
-                sec = make_col(p.x, A0, C0);
-                sec_i = __uint_as_float(p.y);
-              }
+            // The entry below the new top: its ring slot, or below the ring
+            // the workspace (a predicated load; no divergent branch).  With
+            // n < 2 it is never read: the next push replaces it.
+            const int d = n - 2;
+            sec_e = ringE[(d & (Cfg::kRing - 1)) * 32];
+            sec_i = ringI[(d & (Cfg::kRing - 1)) * 32];
+            if (d >= 0 && d < lo) {
+              const uint2 p = gstk[d];
+              sec_e = p.x;
+              sec_i = __uint_as_float(p.y);
             }
             i2 = bisect(top, cur);
           }
@@ -595,12 +596,13 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           while (deep_lanes) {
             const int o = __ffs(deep_lanes) - 1;
             deep_lanes &= deep_lanes - 1;
-            coop_pops<Cfg>(o, s.a0_base, C0, wbase + 2 * Cfg::kTileWords, gstk - (size_t)lane * L, L, n, lo, cur, top, top_i, sec,
-                           sec_i, i2);
+            coop_pops<Cfg>(o, s.a0_base, C0, wbase + 2 * Cfg::kTileWords, gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
+                           sec_e, sec_i, i2);
           }
         }
         if (has) {
-          if (n == 0) i2 = 0.f;
+          // (the bottom entry's bisector is never read: phase 2 pops need two
+          // entries, phase 3 and the warp pops never test depth 0)
           spill = min(spill, n);  // workspace copies at or above n are stale
           lo = min(lo, n);
           const int slot = (n & (Cfg::kRing - 1)) * 32;  // push the current site
@@ -613,7 +615,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           ringI[slot] = i2;
           lo = max(lo, ev + 1);
           ++n;
-          sec = top;
+          sec_e = top.e;
           sec_i = top_i;
           top = cur;
           top_i = i2;
