@@ -267,16 +267,56 @@ __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, con
   }
   __syncwarp();
   const uint64_t layer = (uint64_t)X * Y;
-  uint32_t* dst = map + (uint64_t)y * X + x;
+  uint32_t* const col = map + (uint64_t)y * X + x;  // dereferenced only when live
   const bool live = x < X;
   const uint32_t base = (uint32_t)x | ((uint32_t)y << 10);
+  auto enc = [&](int o) -> uint32_t { return o == 1023 ? kDvUninit : base | ((uint32_t)o << 20); };
   int obst = 1023;  // z of the backward-flood obstacle (1023: UNINIT)
-  for (int z = Z - 1; z >= 0; --z) {
-    const int c = z >> 5;
-    const uint32_t mm = mk[c * 32] & ((2u << (z & 31)) - 1u);
-    const int fz = mm ? c * 32 + 31 - __clz(mm) : (int)lb[c * 32];
+  // The backward flood row by row (kernelPBAphase1FloodZ's second loop):
+  // fz = the forward flood at z, kept when at least as close as obst.
+  auto scan_row = [&](int z, uint32_t mm, int lbc) {
+    const int fz = mm ? (z & ~31) + 31 - __clz(mm) : lbc;
     if (abs(z - fz) <= abs(obst - z)) obst = fz;
-    if (live) dst[(uint64_t)z * layer] = obst == 1023 ? kDvUninit : base | ((uint32_t)obst << 20);
+    if (live) col[(uint64_t)z * layer] = enc(obst);
+  };
+  int c = nch - 1;
+  if (Z & 31) {  // a partial top chunk: row by row
+    const uint32_t mfull = mk[c * 32];
+    const int lbc = (int)lb[c * 32];
+    for (int z = Z - 1; z >= c * 32; --z) scan_row(z, mfull & ((2u << (z & 31)) - 1u), lbc);
+    --c;
+  }
+  for (; c >= 0; --c) {
+    const int zc = c * 32;
+    const uint32_t mfull = mk[c * 32];
+    const int lbc = (int)lb[c * 32];
+    uint32_t* dst = col + (uint64_t)(zc + 31) * layer;
+    if (mfull == 0u) {
+      // No site in this chunk: fz = lbc on every row, and obst is 1023, lbc
+      // or a site above the chunk (obst takes only forward-flood values,
+      // and every such value from above is either above the chunk or lbc).
+      // The test |z - lbc| <= |obst - z| holds exactly for z <= (obst + lbc)/2
+      // (lbc < z <= obst or obst == 1023); with lbc == 1023 it never changes
+      // obst.  So the rows above sw keep obst and the rest take lbc.
+      const int sw = lbc == 1023 ? -1 : (obst + lbc) >> 1;
+      const uint32_t v_hi = enc(obst), v_lo = enc(lbc);
+#pragma unroll
+      for (int l = 31; l >= 0; --l) {
+        if (live) *dst = zc + l <= sw ? v_lo : v_hi;
+        dst -= layer;
+      }
+      if (sw >= zc) obst = lbc;
+    } else {
+#pragma unroll
+      for (int l = 31; l >= 0; --l) {
+        const uint32_t mm = mfull & (0xFFFFFFFFu >> (31 - l));  // sites at or below row l
+        const int fz = mm ? zc + 31 - __clz(mm) : lbc;
+        const int z = zc + l;
+        if (abs(z - fz) <= abs(obst - z)) obst = fz;
+        if (live) *dst = enc(obst);
+        dst -= layer;
+      }
+    }
   }
 }
 

@@ -159,11 +159,15 @@ def test_edt_dense_columns(dims):
     _check(dims, 1.0, _walls(dims, sum(dims)))
 
 
-@pytest.mark.parametrize("case", ["random", "walls", "c1", "outside"])
+@pytest.mark.parametrize("case", ["random", "walls", "c1", "outside", "tall_sparse", "few", "empty"])
 def test_voxelize_edt_equals_clear_insert_edt(case):
-    dims = {"random": (96, 40, 70), "walls": (70, 40, 90), "c1": (128, 128, 128), "outside": (40, 44, 48)}[case]
-    if case == "random":
-        pts = (np.random.default_rng(1).random((3000, 3)) * np.asarray(dims)).astype(np.float32)
+    dims = {"random": (96, 40, 70), "walls": (70, 40, 90), "c1": (128, 128, 128), "outside": (40, 44, 48),
+            "tall_sparse": (40, 36, 700), "few": (33, 40, 320), "empty": (32, 32, 96)}[case]
+    if case in ("random", "tall_sparse", "few", "empty"):
+        # tall_sparse and few: mostly site-free 32-row z chunks, sites below and
+        # above them, and (Z > 512) rows the reference leaves uninitialised
+        n = {"random": 3000, "tall_sparse": 300, "few": 6, "empty": 0}[case]
+        pts = (np.random.default_rng(1).random((n, 3)) * np.asarray(dims)).astype(np.float32).reshape(n, 3)
         side = 1.0
     elif case == "walls":
         pts, side = _walls(dims, 3), 1.0
