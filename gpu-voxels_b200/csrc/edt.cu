@@ -271,51 +271,55 @@ __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, con
   const bool live = x < X;
   const uint32_t base = (uint32_t)x | ((uint32_t)y << 10);
   auto enc = [&](int o) -> uint32_t { return o == 1023 ? kDvUninit : base | ((uint32_t)o << 20); };
-  int obst = 1023;  // z of the backward-flood obstacle (1023: UNINIT)
-  // The backward flood row by row (kernelPBAphase1FloodZ's second loop):
-  // fz = the forward flood at z, kept when at least as close as obst.
-  auto scan_row = [&](int z, uint32_t mm, int lbc) {
-    const int fz = mm ? (z & ~31) + 31 - __clz(mm) : lbc;
-    if (abs(z - fz) <= abs(obst - z)) obst = fz;
-    if (live) col[(uint64_t)z * layer] = enc(obst);
+  // kernelPBAphase1FloodZ's backward loop keeps the forward-flood value fz
+  // (the highest site at or below z) when |z - fz| <= |obst - z|.  Between
+  // consecutive sites s1 < s2 of a column (s2 = 1023 above the highest
+  // site, s1 = 1023 below the lowest) that recurrence gives s1 on the rows
+  // z <= (s1 + s2) / 2 and s2 above (with s1 = 1023: s2 everywhere), the
+  // reference's UNINIT-as-1023 arithmetic included.  So a row is one compare
+  // and select; the pair (s1, s2) moves down only when the scan passes s1.
+  int s2 = 1023, s1, sw;
+  uint32_t v1, v2;
+  auto set_pair = [&]() {
+    sw = s1 == 1023 ? -1 : (s1 + s2) >> 1;
+    v1 = enc(s1);
+    v2 = enc(s2);
   };
-  int c = nch - 1;
-  if (Z & 31) {  // a partial top chunk: row by row
-    const uint32_t mfull = mk[c * 32];
-    const int lbc = (int)lb[c * 32];
-    for (int z = Z - 1; z >= c * 32; --z) scan_row(z, mfull & ((2u << (z & 31)) - 1u), lbc);
-    --c;
+  {
+    const int c = nch - 1;
+    const uint32_t mm = mk[c * 32] & ((2u << ((Z - 1) & 31)) - 1u);
+    s1 = mm ? c * 32 + 31 - __clz(mm) : (int)lb[c * 32];
   }
-  for (; c >= 0; --c) {
+  set_pair();
+  for (int c = nch - 1; c >= 0; --c) {
     const int zc = c * 32;
     const uint32_t mfull = mk[c * 32];
     const int lbc = (int)lb[c * 32];
-    uint32_t* dst = col + (uint64_t)(zc + 31) * layer;
-    if (mfull == 0u) {
-      // No site in this chunk: fz = lbc on every row, and obst is 1023, lbc
-      // or a site above the chunk (obst takes only forward-flood values,
-      // and every such value from above is either above the chunk or lbc).
-      // The test |z - lbc| <= |obst - z| holds exactly for z <= (obst + lbc)/2
-      // (lbc < z <= obst or obst == 1023); with lbc == 1023 it never changes
-      // obst.  So the rows above sw keep obst and the rest take lbc.
-      const int sw = lbc == 1023 ? -1 : (obst + lbc) >> 1;
-      const uint32_t v_hi = enc(obst), v_lo = enc(lbc);
+    const int top = min(31, Z - 1 - zc);
+    uint32_t* dst = col + (uint64_t)(zc + top) * layer;
+    auto row = [&](int l) {
+      const int z = zc + l;
+      if (s1 != 1023 && z < s1) {  // the scan passed s1: the pair moves down
+        s2 = s1;
+        const uint32_t mm = mfull & ((2u << l) - 1u);
+        s1 = mm ? zc + 31 - __clz(mm) : lbc;
+        set_pair();
+      }
+      if (live) *dst = z <= sw ? v1 : v2;
+      dst -= layer;
+    };
+    if (top == 31 && __all_sync(kFullMask, s1 == 1023 || s1 < zc)) {
+      // no lane passes a site in this chunk (none in it, none above s1)
 #pragma unroll
       for (int l = 31; l >= 0; --l) {
-        if (live) *dst = zc + l <= sw ? v_lo : v_hi;
+        if (live) *dst = zc + l <= sw ? v1 : v2;
         dst -= layer;
       }
-      if (sw >= zc) obst = lbc;
+    } else if (top == 31) {
+#pragma unroll
+      for (int l = 31; l >= 0; --l) row(l);
     } else {
-#pragma unroll
-      for (int l = 31; l >= 0; --l) {
-        const uint32_t mm = mfull & (0xFFFFFFFFu >> (31 - l));  // sites at or below row l
-        const int fz = mm ? zc + 31 - __clz(mm) : lbc;
-        const int z = zc + l;
-        if (abs(z - fz) <= abs(obst - z)) obst = fz;
-        if (live) *dst = enc(obst);
-        dst -= layer;
-      }
+      for (int l = top; l >= 0; --l) row(l);
     }
   }
 }
