@@ -251,10 +251,20 @@ __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, con
   uint32_t* mk = wbase + lane;         // chunk c: mk[c * 32]
   uint32_t* lb = wbase + 1024 + lane;  // chunk c: lb[c * 32], 1023 = none
   const int nch = (Z + 31) >> 5;
-  uint32_t last = 1023u;
+  // All of the column's occupancy words in flight at once (word z of chunk c
+  // lands in mk[c * 32] of lane z & 31), then transposed in place: a lane
+  // reads its word before the ballots and writes its mask after them.
   for (int c = 0; c < nch; ++c) {
     const int z = c * 32 + lane;
-    const uint32_t w = z < Z ? __ldg(wcol + z) : 0u;
+    if (z < Z) cp_async4(mk + c * 32, wcol + z);
+    else mk[c * 32] = 0u;
+  }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncwarp();
+  uint32_t last = 1023u;
+  for (int c = 0; c < nch; ++c) {
+    const uint32_t w = mk[c * 32];
     uint32_t mine = 0u;
 #pragma unroll
     for (int l = 0; l < 32; ++l) {
