@@ -113,7 +113,7 @@ gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** o
   if (out == nullptr || maps == nullptr || n_maps == 0) return fail(GVX_ERR_INVALID_ARG, "need at least one map");
   *out = nullptr;
   std::vector<BatchMap> table(n_maps);
-  uint32_t sync_words = 0, stack_len = 1;
+  uint32_t sync_words = 0, stack_len = 1, z_max = 1;
   for (uint32_t k = 0; k < n_maps; ++k) {
     if (maps[k] == nullptr) return fail(GVX_ERR_INVALID_ARG, "null map in batch");
     const gvx_dvm* m = maps[k];
@@ -121,6 +121,7 @@ gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** o
                         (int)m->dims.z, m->side, num_voxels(m->dims), sync_words};
     sync_words += m->dims.z;
     stack_len = std::max(stack_len, std::max(m->dims.x, m->dims.y));
+    z_max = std::max(z_max, m->dims.z);
   }
   const long long stack_warps = edt_batch_stack_warps();
   if (stack_warps <= 0) return fail(GVX_ERR_CUDA, "occupancy query for the batched EDT failed");
@@ -155,6 +156,7 @@ gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** o
   b->items.stack_len = stack_len;
   b->items.d_sync = b->d_sync;
   b->items.sync_words = sync_words;
+  b->items.z_max = z_max;
   *out = b;
   return GVX_OK;
 }

@@ -71,6 +71,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 constexpr int kZChunk = 16;
 constexpr int kZRing = 16;
 constexpr int kZWarps = 8;
+// Pass Z from occupancy bits keeps two words per lane and 32-row chunk (the
+// chunk's mask and the last site below it); up to 32 chunks (Z <= 1024).
+__host__ __device__ constexpr int z_bits_words(int Z) { return 32 * ((Z + 31) >> 5); }
+constexpr int kZBitsSmemMax = kZWarps * 2 * z_bits_words(1024) * 4;
 constexpr int kZWarpWords = 2 * kZChunk * 32 + 2 * kZRing * 32;
 
 // Words of the EDT workspace's counter area (Z slice counters, queue head,
@@ -240,16 +244,17 @@ __global__ void occ_insert_kernel(uint32_t* __restrict__ bits, int X, int Y, int
 // The item's Z words are read 32 at a time and transposed by ballots into one
 // 32-row mask per lane; an ascending pass keeps, per 32-row chunk, each lane's
 // mask and the last occupied z below the chunk (smem), and the backward flood
-// reads the forward value of every row from them.  wbase: 2048 words.
+// reads the forward value of every row from them.  wbase: 2 * zw words, zw =
+// 32 * (chunks of the tallest map of the launch) (z_bits_words).
 __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, const uint32_t* __restrict__ bits, int X,
-                                                 int Y, int Z, long long item, uint32_t* wbase) {
+                                                 int Y, int Z, long long item, uint32_t* wbase, int zw) {
   const int lane = threadIdx.x & 31;
   const int nxb = (X + 31) >> 5;
   const int xb = (int)(item % nxb), y = (int)(item / nxb);
   const int x = xb * 32 + lane;
   const uint32_t* wcol = bits + (uint64_t)item * Z;
   uint32_t* mk = wbase + lane;         // chunk c: mk[c * 32]
-  uint32_t* lb = wbase + 1024 + lane;  // chunk c: lb[c * 32], 1023 = none
+  uint32_t* lb = wbase + zw + lane;  // chunk c: lb[c * 32], 1023 = none
   const int nch = (Z + 31) >> 5;
   // All of the column's occupancy words in flight at once (word z of chunk c
   // lands in mk[c * 32] of lane z & 31), then transposed in place: a lane
@@ -336,11 +341,12 @@ __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, con
 
 __global__ void __launch_bounds__(kZWarps * 32) edt_pass_z_bits(uint32_t* __restrict__ map,
                                                                  const uint32_t* __restrict__ bits, int X, int Y, int Z) {
-  extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][2048]
+  extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][2 * zw]
   const int warp = threadIdx.x >> 5;
   const long long item = (long long)blockIdx.x * kZWarps + warp;
   if (item >= (long long)((X + 31) >> 5) * Y) return;
-  pass_z_bits_item(map, bits, X, Y, Z, item, s_z + (size_t)warp * 2048);
+  const int zw = z_bits_words(Z);
+  pass_z_bits_item(map, bits, X, Y, Z, item, s_z + (size_t)warp * 2 * zw, zw);
 }
 
 // ---------------------------------------------------------------------------
@@ -835,13 +841,13 @@ __global__ void occ_insert_batch_kernel(const BatchMap* __restrict__ maps, uint3
 
 __global__ void __launch_bounds__(kZWarps * 32) edt_pass_z_bits_batch(const BatchMap* __restrict__ maps,
                                                                        const long long* __restrict__ prefix,
-                                                                       uint32_t n_maps, long long total) {
-  extern __shared__ __align__(16) uint32_t s_z[];
+                                                                       uint32_t n_maps, long long total, int zw) {
+  extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][2 * zw]
   const int warp = threadIdx.x >> 5;
   for (long long g = (long long)blockIdx.x * kZWarps + warp; g < total; g += (long long)gridDim.x * kZWarps) {
     const uint32_t k = batch_owner(prefix, n_maps, g);
     const BatchMap m = maps[k];
-    pass_z_bits_item(m.vox, batch_occ(m), m.X, m.Y, m.Z, g - __ldg(prefix + k), s_z + (size_t)warp * 2048);
+    pass_z_bits_item(m.vox, batch_occ(m), m.X, m.Y, m.Z, g - __ldg(prefix + k), s_z + (size_t)warp * 2 * zw, zw);
     __syncwarp();
   }
 }
@@ -1224,9 +1230,9 @@ cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t s
     occ_insert_kernel<<<blocks, 256, 0, s>>>(bits, (int)d.x, (int)d.y, (int)d.z, side, d_xyz, n, d_outside);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  const int smem = kZWarps * 2048 * 4;
-  e = kernel_setup<edt_pass_z_bits>(kZWarps * 32, smem, nullptr);
+  e = kernel_setup<edt_pass_z_bits>(kZWarps * 32, kZBitsSmemMax, nullptr);
   if (e != cudaSuccess) return e;
+  const int smem = kZWarps * 2 * z_bits_words((int)d.z) * 4;  // sized by Z: more resident warps
   const long long items = (long long)((d.x + 31) / 32) * d.y;
   edt_pass_z_bits<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(d_vox, bits, (int)d.x,
                                                                                          (int)d.y, (int)d.z);
@@ -1246,12 +1252,19 @@ cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems&
     occ_insert_batch_kernel<<<blocks, 256, 0, s>>>(d_table, it.n_maps, d_xyz, d_offsets, n_total);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  const int smem = kZWarps * 2048 * 4;
-  long long blocks = 0;
-  e = kernel_setup<edt_pass_z_bits_batch>(kZWarps * 32, smem, &blocks);
+  e = kernel_setup<edt_pass_z_bits_batch>(kZWarps * 32, kZBitsSmemMax, nullptr);
   if (e != cudaSuccess) return e;
+  const int zw = z_bits_words((int)it.z_max);
+  const int smem = kZWarps * 2 * zw * 4;  // sized by the tallest map: more resident warps
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, edt_pass_z_bits_batch, kZWarps * 32, smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sm = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  long long blocks = (long long)std::max(per_sm, 1) * std::max(sm, 1);
   blocks = std::max<long long>(1, std::min<long long>(blocks, (it.total[0] + kZWarps - 1) / kZWarps));
-  edt_pass_z_bits_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0]);
+  edt_pass_z_bits_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0], zw);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32>(d_table, it, s)
                                                  : launch_yx_batch<16>(d_table, it, s);

@@ -99,6 +99,7 @@ struct BatchItems {
   uint32_t stack_len;
   unsigned* d_sync;
   unsigned sync_words;
+  uint32_t z_max;  // the tallest map's Z
 };
 
 // Error reporting shared by the ABI units.
