@@ -415,13 +415,26 @@ __device__ __forceinline__ float bisect(const Col& s1, const Col& s2) {
 }
 
 // Geometry of one warp's work item.
+// The columns of a pass are numbered slice by slice (f = z * cols + a, cols =
+// X for pass Y, Y for pass X) and an item is 32 consecutive ones, so no lane
+// idles when cols is not a multiple of 32: such an item spans two (or, with
+// cols < 32, more) slices.
 struct Sweep {
   int L;             // column length (rows)
-  int a0_base;       // column coordinate of lane 0 (x0 for pass Y, y0 for pass X)
-  int valid;         // valid lanes
-  uint32_t* slice;   // map + z * layer
+  int valid;         // valid lanes (a prefix of the warp)
+  bool one_slice;    // every valid lane in one slice (warp-uniform)
+  uint32_t* map;
   int X;             // map row length
+  uint32_t col;      // this lane's column start (element index; pass Y: row stride X, pass X: contiguous)
+  uint32_t col0;     // lane 0's column start
+  int a, z;          // this lane's column coordinate (x for pass Y, y for pass X) and slice
 };
+
+// Column start of row t of an X-pass item spanning slices: lane t's `col`
+// (all lanes take part).
+__device__ __forceinline__ uint32_t row_start(const Sweep& s, int t) {
+  return __shfl_sync(0xffffffffu, s.col, t & 31);
+}
 
 template <int kRows>
 struct SweepCfg {
@@ -452,15 +465,16 @@ struct SweepCfg {
 // depths.  All 32 lanes call this; only lane o's state changes (sec_e: the
 // packed entry below the top, decoded only when it becomes the top).
 template <class Cfg>
-__device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t* ring_base, const uint2* gstk_base, int L,
+__device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint32_t* ring_base, const uint2* gstk_base, int L,
                                           int& n, int& lo, const Col& cur, Col& top, float& top_i, uint32_t& sec_e,
                                           float& sec_i, float& i2) {
   const int lane = threadIdx.x & 31;
   const int on = __shfl_sync(kFullMask, n, o);
   const int olo = __shfl_sync(kFullMask, lo, o);
   const uint32_t ce = __shfl_sync(kFullMask, cur.e, o);
-  const float oA0 = biased((uint32_t)(a0_base + o));
-  const Col oc = make_col(ce, oA0, C0);
+  const float oA0 = __shfl_sync(kFullMask, A0, o);  // lane o's column, biased
+  const float oC0 = __shfl_sync(kFullMask, C0, o);
+  const Col oc = make_col(ce, oA0, oC0);
   uint32_t* ringE = ring_base + o;
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
   const uint2* gstk = gstk_base + (size_t)o * L;
@@ -476,7 +490,7 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t
       e = p.x;
       I = __uint_as_float(p.y);
     }
-    const Col ec = make_col(e, oA0, C0);
+    const Col ec = make_col(e, oA0, oC0);
     const float b = bisect(ec, oc);
     const bool keep = j <= 0 || I < b;
     const unsigned kb = __ballot_sync(kFullMask, keep) & 0x7fffffffu;
@@ -499,7 +513,7 @@ __device__ __forceinline__ void coop_pops(int o, int a0_base, float C0, uint32_t
       if (lane == o) {
         n = start - t + 1;
         lo = min(lo, new_lo);
-        top = make_col(e_top, oA0, C0);
+        top = make_col(e_top, oA0, oC0);
         top_i = i_top;
         i2 = b_top;
         sec_e = e_sec;
@@ -520,30 +534,41 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
   const int r0 = c * kRows;
   const int rows = min(kRows, s.L - r0);
   if (!kXPass) {
-    const uint32_t* src = s.slice + (uint64_t)r0 * s.X + s.a0_base;
-    if (vec16) {
+    if (vec16) {  // one slice, 32 lanes, 16-byte aligned: 8 lanes per row
+      const uint32_t* src = s.map + s.col0 + (uint64_t)r0 * s.X;
       const int part = lane & 7;
       for (int r = lane >> 3; r < rows; r += 4) cp_async16(tile + r * 32 + part * 4, src + (uint64_t)r * s.X + part * 4);
     } else if (lane < s.valid) {
-      for (int r = 0; r < rows; ++r) cp_async4(tile + r * 32 + lane, src + (uint64_t)r * s.X + lane);
+      const uint32_t* src = s.map + s.col + (uint64_t)r0 * s.X;
+      for (int r = 0; r < rows; ++r) cp_async4(tile + r * 32 + lane, src + (uint64_t)r * s.X);
     } else {
       for (int r = 0; r < rows; ++r) tile[r * 32 + lane] = kDvUninit;
     }
   } else {
     const int xl = lane % kRows;  // x within the chunk
     const int t0 = lane / kRows;
-    if (xl < rows) {
-      const uint32_t* src = s.slice + (uint64_t)s.a0_base * s.X + r0 + xl;
-      for (int t = t0; t < 32; t += 32 / kRows) {
-        if (t < s.valid) cp_async4(tile + xl * 33 + t, src + (uint64_t)t * s.X);
-        else tile[xl * 33 + t] = kDvUninit;
+    if (s.one_slice) {  // rows t are X apart
+      if (xl < rows) {
+        const uint32_t* src = s.map + s.col0 + r0 + xl;
+        for (int t = t0; t < 32; t += 32 / kRows) {
+          if (t < s.valid) cp_async4(tile + xl * 33 + t, src + (uint64_t)t * s.X);
+          else tile[xl * 33 + t] = kDvUninit;
+        }
+      }
+    } else {
+      for (int t = t0; t < 32; t += 32 / kRows) {  // the same trip count on every lane (row_start shuffles)
+        const uint32_t rs = row_start(s, t);
+        if (xl < rows) {
+          if (t < s.valid) cp_async4(tile + xl * 33 + t, s.map + rs + r0 + xl);
+          else tile[xl * 33 + t] = kDvUninit;
+        }
       }
     }
   }
 }
 
-// One warp item of pass Y (kXPass false) or X: 32 adjacent columns of one
-// z slice; wbase = the warp's kWarpWords of shared memory; stack = L * 64
+// One warp item of pass Y (kXPass false) or X: 32 consecutive columns (see
+// Sweep); wbase = the warp's kWarpWords of shared memory; stack = L * 64
 // words of workspace: entry d of lane l is the pair (site, bisector with the
 // entry below) at ((uint2*)stack)[l * L + d] -- each lane's stack contiguous,
 // so its spills, refills and window reads fill whole sectors.
@@ -552,24 +577,34 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
                                            int Z, long long item, uint32_t* wbase) {
   using Cfg = SweepCfg<kRows>;
   const int lane = threadIdx.x & 31;
-  const int cols = kXPass ? Y : X;  // columns per slice
+  const unsigned cols = kXPass ? Y : X;  // columns per slice
   const int L = kXPass ? X : Y;
-  const int nblk = (cols + 31) >> 5;
-  const int blk = (int)(item % nblk), z = (int)(item / nblk);
+  const unsigned total = cols * (unsigned)Z;  // below 2^30
+  const unsigned f0 = (unsigned)item * 32u;
   Sweep s;
   s.L = L;
-  s.a0_base = blk * 32;
-  s.valid = min(32, cols - s.a0_base);
-  s.slice = map + (uint64_t)z * X * Y;
   s.X = X;
-  const bool vec16 = !kXPass && s.valid == 32 && (X & 3) == 0;
+  s.map = map;
+  s.valid = (int)min(32u, total - f0);
+  {
+    const unsigned f = min(f0 + (unsigned)lane, total - 1u);  // idle lanes mirror the last column
+    s.z = (int)(f / cols);
+    s.a = (int)(f - (unsigned)s.z * cols);
+    const unsigned layer = (unsigned)X * (unsigned)Y;
+    s.col = (unsigned)s.z * layer + (kXPass ? (unsigned)s.a * (unsigned)X : (unsigned)s.a);
+    const unsigned z0 = f0 / cols;
+    s.col0 = z0 * layer + (kXPass ? (f0 - z0 * cols) * (unsigned)X : f0 - z0 * cols);
+    s.one_slice = (f0 + (unsigned)s.valid - 1u) / cols == z0;
+  }
+  // lane 0's column is a multiple of 4 when X is (f0 is a multiple of 32)
+  const bool vec16 = !kXPass && s.one_slice && s.valid == 32 && (X & 3) == 0;
   uint32_t* tile0 = wbase;
   uint32_t* tile1 = wbase + Cfg::kTileWords;
   uint32_t* ringE = wbase + 2 * Cfg::kTileWords + lane;  // slot k: ringE[k * 32]
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
   uint2* gstk = reinterpret_cast<uint2*>(stack) + (size_t)lane * L;  // this lane's stack, depth d: gstk[d]
-  const float A0 = biased((uint32_t)(s.a0_base + lane));  // this lane's column coordinate, biased
-  const float C0 = biased((uint32_t)z);
+  const float A0 = biased((uint32_t)s.a);  // this lane's column coordinate, biased
+  const float C0 = biased((uint32_t)s.z);
   const int nchunks = (L + kRows - 1) / kRows;
   const int tpitch = kXPass ? 33 : 32;
   // Pops a lane runs alone per row before the warp takes over.  Pass Y (input:
@@ -656,7 +691,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           while (deep_lanes) {
             const int o = __ffs(deep_lanes) - 1;
             deep_lanes &= deep_lanes - 1;
-            coop_pops<Cfg>(o, s.a0_base, C0, wbase + 2 * Cfg::kTileWords, gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
+            coop_pops<Cfg>(o, A0, C0, wbase + 2 * Cfg::kTileWords, gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
                            sec_e, sec_i, i2);
           }
         }
@@ -739,7 +774,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     out = out_of(t.x);
     top_b = __uint_as_float(t.y);
   }
-  uint32_t* col_out = s.slice + s.a0_base + lane;  // pass Y: this lane's column, row stride X
+  uint32_t* col_out = map + s.col;  // pass Y: this lane's column, row stride X
   const bool live = lane < s.valid;
   for (int c = (L + kP3Rows - 1) / kP3Rows - 1; c >= 0; --c) {
     const int r0 = c * kP3Rows;
@@ -761,9 +796,16 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     if (kXPass) {  // transposed flush: 4 rows of the map x 8 consecutive x per store
       __syncwarp();
       const int xl = lane >> 2, t0 = lane & 3;
-      if (xl < rows)
-        for (int t = t0; t < s.valid; t += 4)
-          s.slice[(uint64_t)(s.a0_base + t) * X + r0 + xl] = xstage[xl * Cfg::kStagePitch + t];
+      if (s.one_slice) {  // rows t are X apart
+        if (xl < rows)
+          for (int t = t0; t < s.valid; t += 4)
+            map[(uint64_t)s.col0 + (uint64_t)t * X + r0 + xl] = xstage[xl * Cfg::kStagePitch + t];
+      } else {
+        for (int t = t0; t < 32; t += 4) {  // the same trip count on every lane (row_start shuffles)
+          const uint32_t rs = row_start(s, t);
+          if (xl < rows && t < s.valid) map[(uint64_t)rs + r0 + xl] = xstage[xl * Cfg::kStagePitch + t];
+        }
+      }
       __syncwarp();
     }
   }
@@ -862,7 +904,7 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
   const int warp = threadIdx.x >> 5;
   const long long gw = (long long)blockIdx.x * Cfg::kWarps + warp;
   uint32_t* stack = stacks + (uint64_t)gw * warp_stack_words(X, Y);
-  const long long items = (long long)(((kXPass ? Y : X) + 31) >> 5) * Z;
+  const long long items = ((long long)(kXPass ? Y : X) * Z + 31) / 32;
   for (long long item = gw; item < items; item += (long long)gridDim.x * Cfg::kWarps) {
     sweep_item<kXPass, kRows>(map, stack, X, Y, Z, item, s_sweep + (size_t)warp * Cfg::kWarpWords);
     __syncwarp();
@@ -872,9 +914,10 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
 // ---------------------------------------------------------------------------
 // Fused Y -> X schedule.  Pass X on slice z reads only what pass Y wrote to
 // slice z, so one persistent launch runs both: warps take items from a queue
-// (all Y items in z order, then all X items in z order), a Y item bumps its
-// slice's completion counter, and an X item first waits for its slice's
-// counter to reach the slice's Y item count.  Every item a wait depends on
+// (all Y items in z order, then all X items in z order), a Y item bumps the
+// completion counter of each slice it touches, and an X item first waits
+// until each of its slices counts all the Y items touching it.  Every item a
+// wait depends on
 // sits earlier in the queue and was taken by a running warp that waits on
 // nothing, so the waits end; they are bounded all the same (kSpinLimit
 // sleeps, then the error word is set and the item is skipped).  The tail of
@@ -890,22 +933,40 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   return v;
 }
 
-// After a Y item: its output stores, then the slice counter.
-__device__ __forceinline__ void publish_slice(unsigned* done) {
+// Slices za..zb that item g of a pass with `cols` columns per slice touches
+// (at most 32: an item is 32 consecutive columns).
+__device__ __forceinline__ void item_slices(unsigned g, unsigned cols, unsigned Z, unsigned& za, unsigned& zb) {
+  const unsigned f0 = g * 32u;
+  za = f0 / cols;
+  zb = min(f0 + 31u, cols * Z - 1u) / cols;
+}
+
+// Y items that touch slice z (its columns z*X .. z*X + X - 1).
+__device__ __forceinline__ unsigned y_items_of_slice(unsigned z, unsigned X) {
+  return ((z + 1u) * X - 1u) / 32u - (z * X) / 32u + 1u;
+}
+
+// After a Y item: its output stores, then the counter of every slice it
+// touched (lane j bumps slice za + j).
+__device__ __forceinline__ void publish_slices(unsigned* done, unsigned za, unsigned zb) {
   __threadfence();
   __syncwarp();
-  if ((threadIdx.x & 31) == 0) {
+  const unsigned lane = threadIdx.x & 31;
+  if (lane <= zb - za) {
     __threadfence();
-    atomicAdd(done, 1u);
+    atomicAdd(done + za + lane, 1u);
   }
 }
 
-// Before an X item: wait (bounded) until `need` Y items of the slice are done.
-__device__ __forceinline__ bool wait_slice(const unsigned* done, unsigned need, unsigned* err) {
+// Before an X item: wait (bounded) until every slice it reads has all its Y
+// items done (lane j waits for slice za + j).
+__device__ __forceinline__ bool wait_slices(const unsigned* done, unsigned za, unsigned zb, unsigned X, unsigned* err) {
+  const unsigned lane = threadIdx.x & 31;
   int ok = 1;
-  if ((threadIdx.x & 31) == 0) {
+  if (lane <= zb - za) {
+    const unsigned need = y_items_of_slice(za + lane, X);
     unsigned spins = 0;
-    while (ld_acquire_gpu(done) < need) {
+    while (ld_acquire_gpu(done + za + lane) < need) {
       if (++spins > kSpinLimit) {
         atomicOr(err, 1u);
         ok = 0;
@@ -914,8 +975,8 @@ __device__ __forceinline__ bool wait_slice(const unsigned* done, unsigned need, 
       __nanosleep(128);
     }
   }
-  __syncwarp();  // orders lane 0's acquire before every lane's loads
-  ok = __shfl_sync(kFullMask, ok, 0);
+  __syncwarp();  // orders the waiting lanes' acquires before every lane's loads
+  ok = __all_sync(kFullMask, ok);
   __threadfence();
   return ok != 0;
 }
@@ -939,15 +1000,17 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
   unsigned* done = sync;
   unsigned* head = sync + Z;
   unsigned* err = head + 1;
-  const unsigned nxb = (X + 31) >> 5, nyb = (Y + 31) >> 5;
-  const unsigned ny = nxb * Z, nall = ny + nyb * Z;
+  const unsigned ny = ((unsigned)X * Z + 31u) / 32u, nall = ny + ((unsigned)Y * Z + 31u) / 32u;
   for (unsigned g = next_item(head); g < nall; g = next_item(head)) {
+    unsigned za, zb;
     if (g < ny) {
       sweep_item<false, kRows>(map, stack, X, Y, Z, g, wbase);
-      publish_slice(done + g / nxb);
+      item_slices(g, X, Z, za, zb);
+      publish_slices(done, za, zb);
     } else {
       const unsigned item = g - ny;
-      if (wait_slice(done + item / nyb, nxb, err)) sweep_item<true, kRows>(map, stack, X, Y, Z, item, wbase);
+      item_slices(item, Y, Z, za, zb);
+      if (wait_slices(done, za, zb, X, err)) sweep_item<true, kRows>(map, stack, X, Y, Z, item, wbase);
     }
     __syncwarp();
   }
@@ -978,13 +1041,14 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     const BatchMap m = maps[k];
     const unsigned item = (unsigned)(q - __ldg(prefix + k));
     unsigned* done = sync + m.sync_off;
-    const unsigned nxb = (m.X + 31) >> 5;
+    unsigned za, zb;
     if (!x_item) {
       sweep_item<false, kRows>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
-      publish_slice(done + item / nxb);
+      item_slices(item, m.X, m.Z, za, zb);
+      publish_slices(done, za, zb);
     } else {
-      const unsigned nyb = (m.Y + 31) >> 5;
-      if (wait_slice(done + item / nyb, nxb, err)) sweep_item<true, kRows>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+      item_slices(item, m.Y, m.Z, za, zb);
+      if (wait_slices(done, za, zb, m.X, err)) sweep_item<true, kRows>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
     }
     __syncwarp();
   }
@@ -1061,8 +1125,7 @@ long long sweep_blocks(long long resident, uint64_t stack_area, gvx_dims d, int 
 template <bool kXPass, int kRows>
 cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s) {
   using Cfg = SweepCfg<kRows>;
-  const long long cols = kXPass ? d.y : d.x;
-  const long long items = ((cols + 31) / 32) * d.z;
+  const long long items = edt_pass_items(d, kXPass ? 2 : 1);
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
   long long blocks = 0;
   cudaError_t e = kernel_setup<edt_sweep<kXPass, kRows>>(Cfg::kWarps * 32, smem, &blocks);
@@ -1078,7 +1141,7 @@ cudaError_t launch_sweep(uint32_t* map, uint32_t* scratch, uint64_t scratch_word
 // kFusedWarpCap warps (more than a B200 keeps resident).
 constexpr uint64_t kFusedWarpCap = 4096;
 uint64_t fused_stack_words(gvx_dims d) {
-  const uint64_t items = (uint64_t)((d.x + 31) / 32) * d.z + (uint64_t)((d.y + 31) / 32) * d.z;
+  const uint64_t items = (uint64_t)(edt_pass_items(d, 1) + edt_pass_items(d, 2));
   const uint64_t warps = std::min<uint64_t>((items + 7) / 8 * 8, kFusedWarpCap);
   return warps * warp_stack_words((int)d.x, (int)d.y);
 }
@@ -1092,7 +1155,7 @@ cudaError_t launch_sweep_yx(uint32_t* map, uint32_t* scratch, uint64_t scratch_w
   long long blocks = 0;
   cudaError_t e = kernel_setup<edt_sweep_yx<kRows>>(Cfg::kWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
-  const long long items = (long long)((d.x + 31) / 32) * d.z + (long long)((d.y + 31) / 32) * d.z;
+  const long long items = edt_pass_items(d, 1) + edt_pass_items(d, 2);
   blocks = sweep_blocks(blocks, scratch_words - sync_words(d), d, Cfg::kWarps, items);
   if (blocks < 1) return cudaErrorInvalidValue;
   unsigned* sync = scratch;
@@ -1209,8 +1272,8 @@ cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag
 long long edt_pass_items(gvx_dims d, int pass) {
   switch (pass) {
     case 0: return (long long)((d.x + 31) / 32) * d.y;
-    case 1: return (long long)((d.x + 31) / 32) * d.z;
-    default: return (long long)((d.y + 31) / 32) * d.z;
+    case 1: return ((long long)d.x * d.z + 31) / 32;  // pass Y: columns numbered slice by slice
+    default: return ((long long)d.y * d.z + 31) / 32;
   }
 }
 
