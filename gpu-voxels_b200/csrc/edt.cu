@@ -85,21 +85,25 @@ __host__ __device__ __forceinline__ uint64_t edt_sync_words(int Z) { return ((ui
 // (32 columns) one word per lane and chunk.
 __host__ __device__ __forceinline__ uint64_t zcarry_item_words(int Z) { return (uint64_t)((Z + kZChunk - 1) / kZChunk) * 32; }
 
-// One warp item of pass Z: 32 adjacent (x, y) columns; wbase = the warp's
+// Pass Z items: the (x, y) columns numbered f = y * X + x, 32 consecutive
+// ones per warp item (an item may span rows of the layer, so no lane idles).
+__host__ __device__ __forceinline__ uint64_t z_items(int X, int Y) { return ((uint64_t)X * Y + 31) / 32; }
+
+// One warp item of pass Z (columns f0 .. f0 + 31); wbase = the warp's
 // kZWarpWords of shared memory; carry = the item's zcarry_item_words(Z) words.
+// The sites carry their own coordinates, so the columns' (x, y) are not needed.
 __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, int Y, int Z, long long item,
                                             uint32_t* wbase, uint32_t* __restrict__ carry) {
   const int lane = threadIdx.x & 31;
-  const int nxb = (X + 31) >> 5;
-  const int xb = (int)(item % nxb), y = (int)(item / nxb);
-  const int x0 = xb * 32, valid_cols = min(32, X - x0);
   const uint64_t layer = (uint64_t)X * Y;
+  const uint64_t f0 = (uint64_t)item * 32;
+  const int valid_cols = layer - f0 < 32 ? (int)(layer - f0) : 32;
   uint32_t* const tile0 = wbase;
   uint32_t* const tile1 = wbase + kZChunk * 32;
   uint32_t* ringV = wbase + 2 * kZChunk * 32 + lane;  // slot k: ringV[k * 32]
   uint32_t* ringR = ringV + kZRing * 32;
-  const uint32_t* src = map + (uint64_t)y * X + x0;
-  const bool vec16 = valid_cols == 32 && (X & 3) == 0;
+  const uint32_t* src = map + f0;
+  const bool vec16 = valid_cols == 32 && (layer & 3) == 0;  // f0 is a multiple of 32
   const int nchunks = (Z + kZChunk - 1) / kZChunk;
   auto stage = [&](uint32_t* tile, int c) {
     const int r0 = c * kZChunk, rows = min(kZChunk, Z - r0);
@@ -146,7 +150,7 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
   // backward: obstacle(z) from the forward value fwd(z) = last site at or below z;
   // ties keep the lower z (<=, VoxelMapOperationsPBA.hpp:112-122)
   uint32_t obstacle = kDvUninit;
-  uint32_t* dst = map + (uint64_t)y * X + x0 + lane;
+  uint32_t* dst = map + f0 + lane;
   const bool live = lane < valid_cols;
   if (!__any_sync(kFullMask, m > kZRing)) {
     int j = m - 1;  // index of the site fwd(z)
@@ -211,18 +215,16 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
 // Voxelisation fused with pass Z.  After clearMap + insertPointCloud a
 // DistanceVoxelMap holds each occupied voxel's own coordinate and UNINIT
 // elsewhere, so it is fully described by one occupancy bit per voxel.  The
-// fused path records those bits (word ((y * nxb + xb) * Z + z), bit x & 31)
+// fused path records those bits (word (f / 32) * Z + z, bit f % 32, f = y * X + x)
 // in the workspace instead of clearing and scattering the map, and pass Z
 // reads the bits: the map is written once, by pass Z.  The flood arithmetic
 // is phase 1's (the same values, the same ties, UNINIT's z read as 1023).
 // ---------------------------------------------------------------------------
-__host__ __device__ __forceinline__ uint64_t occ_words(int X, int Y, int Z) {
-  return (uint64_t)((X + 31) >> 5) * Y * Z;
-}
+__host__ __device__ __forceinline__ uint64_t occ_words(int X, int Y, int Z) { return z_items(X, Y) * Z; }
 
 __device__ __forceinline__ void occ_set(uint32_t* bits, int X, int Z, uint32_t x, uint32_t y, uint32_t z) {
-  const uint32_t nxb = ((uint32_t)X + 31) >> 5;
-  atomicOr(bits + ((uint64_t)y * nxb + (x >> 5)) * Z + z, 1u << (x & 31));
+  const uint32_t f = y * (uint32_t)X + x;
+  atomicOr(bits + (uint64_t)(f >> 5) * Z + z, 1u << (f & 31));
 }
 
 // insertPointCloud into the occupancy bits (coordinates as
@@ -240,7 +242,7 @@ __global__ void occ_insert_kernel(uint32_t* __restrict__ bits, int X, int Y, int
   if (outside != nullptr && __any_sync(kFullMask, out) && (threadIdx.x & 31) == 0) *outside = 1u;
 }
 
-// Pass Z of one warp item (32 adjacent (x, y) columns) from occupancy bits.
+// Pass Z of one warp item (32 consecutive columns f = y * X + x) from occupancy bits.
 // The item's Z words are read 32 at a time and transposed by ballots into one
 // 32-row mask per lane; an ascending pass keeps, per 32-row chunk, each lane's
 // mask and the last occupied z below the chunk (smem), and the backward flood
@@ -249,9 +251,7 @@ __global__ void occ_insert_kernel(uint32_t* __restrict__ bits, int X, int Y, int
 __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, const uint32_t* __restrict__ bits, int X,
                                                  int Y, int Z, long long item, uint32_t* wbase, int zw) {
   const int lane = threadIdx.x & 31;
-  const int nxb = (X + 31) >> 5;
-  const int xb = (int)(item % nxb), y = (int)(item / nxb);
-  const int x = xb * 32 + lane;
+  const uint32_t f = (uint32_t)item * 32u + (uint32_t)lane;  // this lane's column y * X + x
   const uint32_t* wcol = bits + (uint64_t)item * Z;
   uint32_t* mk = wbase + lane;         // chunk c: mk[c * 32]
   uint32_t* lb = wbase + zw + lane;  // chunk c: lb[c * 32], 1023 = none
@@ -282,9 +282,11 @@ __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, con
   }
   __syncwarp();
   const uint64_t layer = (uint64_t)X * Y;
-  uint32_t* const col = map + (uint64_t)y * X + x;  // dereferenced only when live
-  const bool live = x < X;
-  const uint32_t base = (uint32_t)x | ((uint32_t)y << 10);
+  uint32_t* const col = map + f;  // dereferenced only when live
+  const bool live = f < layer;
+  const uint32_t fl = min(f, (uint32_t)layer - 1u);
+  const uint32_t y = fl / (uint32_t)X;
+  const uint32_t base = (fl - y * (uint32_t)X) | (y << 10);
   auto enc = [&](int o) -> uint32_t { return o == 1023 ? kDvUninit : base | ((uint32_t)o << 20); };
   // kernelPBAphase1FloodZ's backward loop keeps the forward-flood value fz
   // (the highest site at or below z) when |z - fz| <= |obst - z|.  Between
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(kZWarps * 32) edt_pass_z_bits(uint32_t* __rest
   extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][2 * zw]
   const int warp = threadIdx.x >> 5;
   const long long item = (long long)blockIdx.x * kZWarps + warp;
-  if (item >= (long long)((X + 31) >> 5) * Y) return;
+  if (item >= (long long)z_items(X, Y)) return;
   const int zw = z_bits_words(Z);
   pass_z_bits_item(map, bits, X, Y, Z, item, s_z + (size_t)warp * 2 * zw, zw);
 }
@@ -828,7 +830,7 @@ __global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z(uint32_t* __restri
   extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][kZWarpWords]
   const int warp = threadIdx.x >> 5;
   const long long item = (long long)blockIdx.x * kZWarps + warp;
-  if (item >= (long long)((X + 31) >> 5) * Y) return;
+  if (item >= (long long)z_items(X, Y)) return;
   pass_z_item(map, X, Y, Z, item, s_z + (size_t)warp * kZWarpWords, carries + (uint64_t)item * zcarry_item_words(Z));
 }
 
@@ -1103,7 +1105,7 @@ cudaError_t launch_pass_z(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStre
   const int smem = kZWarps * kZWarpWords * 4;
   cudaError_t e = kernel_setup<edt_pass_z>(kZWarps * 32, smem, nullptr);
   if (e != cudaSuccess) return e;
-  const long long items = (long long)((d.x + 31) / 32) * d.y;
+  const long long items = (long long)z_items((int)d.x, (int)d.y);
   edt_pass_z<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(
       map, scratch + edt_sync_words((int)d.z), (int)d.x, (int)d.y, (int)d.z);
   return cudaGetLastError();
@@ -1113,7 +1115,7 @@ cudaError_t launch_pass_z(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStre
 // [stack area: one stack of warp_stack_words per launched warp; before the
 // sweeps, pass Z keeps its chunk carries there].
 uint64_t sync_words(gvx_dims d) { return edt_sync_words((int)d.z); }
-uint64_t zcarry_words(gvx_dims d) { return (uint64_t)((d.x + 31) / 32) * d.y * zcarry_item_words((int)d.z); }
+uint64_t zcarry_words(gvx_dims d) { return z_items((int)d.x, (int)d.y) * zcarry_item_words((int)d.z); }
 
 // Blocks for a persistent sweep launch: resident, fitting the stack area, and
 // no more than the items need (0 when the area holds no block's stacks).
@@ -1271,7 +1273,7 @@ cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag
 
 long long edt_pass_items(gvx_dims d, int pass) {
   switch (pass) {
-    case 0: return (long long)((d.x + 31) / 32) * d.y;
+    case 0: return (long long)z_items((int)d.x, (int)d.y);
     case 1: return ((long long)d.x * d.z + 31) / 32;  // pass Y: columns numbered slice by slice
     default: return ((long long)d.y * d.z + 31) / 32;
   }
@@ -1296,7 +1298,7 @@ cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t s
   e = kernel_setup<edt_pass_z_bits>(kZWarps * 32, kZBitsSmemMax, nullptr);
   if (e != cudaSuccess) return e;
   const int smem = kZWarps * 2 * z_bits_words((int)d.z) * 4;  // sized by Z: more resident warps
-  const long long items = (long long)((d.x + 31) / 32) * d.y;
+  const long long items = (long long)z_items((int)d.x, (int)d.y);
   edt_pass_z_bits<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(d_vox, bits, (int)d.x,
                                                                                          (int)d.y, (int)d.z);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
