@@ -125,6 +125,13 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
   cp_async_commit();
   int m = 0;                 // sites seen
   uint32_t flood = kDvUninit;  // forward-flood value
+  // This lane's column as a DistanceVoxel without z (idle lanes: unused).
+  uint32_t xy;
+  {
+    const uint32_t f = (uint32_t)(f0 + lane < layer ? f0 + lane : layer - 1), y = f / (uint32_t)X;
+    xy = (f - y * (uint32_t)X) | (y << 10);
+  }
+  bool self = true;  // every site of the column holds its own voxel (as after insertPointCloud)
   for (int c = 0; c < nchunks; ++c) {
     cp_async_wait1();
     __syncwarp();
@@ -137,6 +144,7 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
         ringR[(m % kZRing) * 32] = (uint32_t)(r0 + r);
         ++m;
         flood = v;
+        self = self && v == (xy | ((uint32_t)(r0 + r) << 20));
       }
     }
     carry[c * 32 + lane] = flood;
@@ -152,6 +160,55 @@ __device__ __forceinline__ void pass_z_item(uint32_t* __restrict__ map, int X, i
   uint32_t obstacle = kDvUninit;
   uint32_t* dst = map + f0 + lane;
   const bool live = lane < valid_cols;
+  if (__all_sync(kFullMask, self && m <= kZRing)) {
+    // Every site holds its own voxel and the ring holds them all: the closed
+    // form of the backward rule (the occupancy-bit pass, pass_z_bits_item):
+    // between consecutive site rows s1 < s2 (s2 = 1023 above the highest,
+    // s1 = 1023 below the lowest) rows z <= (s1 + s2) / 2 take s1, the rest s2.
+    auto enc = [&](int o) -> uint32_t { return o == 1023 ? kDvUninit : xy | ((uint32_t)o << 20); };
+    int j = m - 1;  // ring index of s1
+    int s1 = j >= 0 ? (int)ringR[(j % kZRing) * 32] : 1023, s2 = 1023, sw;
+    uint32_t v1, v2;
+    auto set_pair = [&]() {
+      sw = s1 == 1023 ? -1 : (s1 + s2) >> 1;
+      v1 = enc(s1);
+      v2 = enc(s2);
+    };
+    set_pair();
+    int z = Z - 1;
+    for (; z >= 0 && ((z + 1) & 31); --z) {  // down to a multiple of 32 rows, row by row
+      if (s1 != 1023 && z < s1) {
+        s2 = s1;
+        --j;
+        s1 = j >= 0 ? (int)ringR[(j % kZRing) * 32] : 1023;
+        set_pair();
+      }
+      if (live) dst[(uint64_t)z * layer] = z <= sw ? v1 : v2;
+    }
+    for (int zc = z - 31; zc >= 0; zc -= 32) {  // 32-row chunks
+      uint32_t* d = dst + (uint64_t)(zc + 31) * layer;
+      if (__all_sync(kFullMask, s1 == 1023 || s1 < zc)) {  // no lane passes a site here
+#pragma unroll
+        for (int l = 31; l >= 0; --l) {
+          if (live) *d = zc + l <= sw ? v1 : v2;
+          d -= layer;
+        }
+      } else {
+#pragma unroll
+        for (int l = 31; l >= 0; --l) {
+          if (s1 != 1023 && zc + l < s1) {
+            s2 = s1;
+            --j;
+            s1 = j >= 0 ? (int)ringR[(j % kZRing) * 32] : 1023;
+            set_pair();
+          }
+          if (live) *d = zc + l <= sw ? v1 : v2;
+          d -= layer;
+        }
+      }
+    }
+    return;
+  }
   if (!__any_sync(kFullMask, m > kZRing)) {
     int j = m - 1;  // index of the site fwd(z)
     uint32_t fwdV = kDvUninit;
