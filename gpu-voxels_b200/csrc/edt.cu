@@ -300,8 +300,8 @@ __global__ void occ_insert_kernel(uint32_t* __restrict__ bits, int X, int Y, int
 }
 
 // Pass Z of one warp item (32 consecutive columns f = y * X + x) from occupancy bits.
-// The item's Z words are read 32 at a time and transposed by ballots into one
-// 32-row mask per lane; an ascending pass keeps, per 32-row chunk, each lane's
+// The item's Z words are read 32 at a time and bit-transposed across the warp
+// into one 32-row mask per lane; an ascending pass keeps, per 32-row chunk, each lane's
 // mask and the last occupied z below the chunk (smem), and the backward flood
 // reads the forward value of every row from them.  wbase: 2 * zw words, zw =
 // 32 * (chunks of the tallest map of the launch) (z_bits_words).
@@ -326,12 +326,16 @@ __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, con
   __syncwarp();
   uint32_t last = 1023u;
   for (int c = 0; c < nch; ++c) {
-    const uint32_t w = mk[c * 32];
-    uint32_t mine = 0u;
+    // 32 x 32 bit transpose across the warp (lane l holds row c*32 + l, bit j
+    // = column j): five butterfly stages, each swapping the off-diagonal
+    // s x s blocks between lanes l and l ^ s.
+    uint32_t mine = mk[c * 32];
 #pragma unroll
-    for (int l = 0; l < 32; ++l) {
-      const uint32_t b = __ballot_sync(kFullMask, (w >> l) & 1u);
-      if (l == lane) mine = b;
+    for (int sft = 16; sft >= 1; sft >>= 1) {
+      const uint32_t hi = sft == 16 ? 0xFFFF0000u : sft == 8 ? 0xFF00FF00u : sft == 4 ? 0xF0F0F0F0u
+                        : sft == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;  // columns j with j & sft
+      const uint32_t t = __shfl_xor_sync(kFullMask, mine, sft);
+      mine = (lane & sft) ? (mine & hi) | ((t & hi) >> sft) : (mine & ~hi) | ((t & ~hi) << sft);
     }
     mk[c * 32] = mine;
     lb[c * 32] = last;
