@@ -145,6 +145,34 @@ class Ranks:
             self.dist = None
 
 
+def gpu_local_cpus(torch):
+    """CPUs on the current GPU's NUMA node (NVML's affinity set), or None."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(torch.cuda.current_device()).uuid)
+        h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, ((os.cpu_count() or 64) + 63) // 64)
+        cpus = {w * 64 + b for w, m in enumerate(words) for b in range(64) if (int(m) >> b) & 1}
+        return (cpus & os.sched_getaffinity(0)) or None
+    except Exception:
+        return None
+
+
+def pinned_near_gpu(torch, tensors):
+    """Pinned host copies of `tensors`, allocated while this thread runs on the
+    GPU's NUMA node so the pages land there (host->device copies from the far
+    node run at a fraction of the link rate); the thread's affinity is restored."""
+    cpus, before = gpu_local_cpus(torch), os.sched_getaffinity(0)
+    if cpus:
+        os.sched_setaffinity(0, cpus)
+    try:
+        out = [t.pin_memory() for t in tensors]
+    finally:
+        os.sched_setaffinity(0, before)
+    return out, ("gpu-local NUMA node" if cpus else "default")
+
+
 def whole_job_rate(units_per_rank: float, world: int, ms: float, scale: float = 1e9) -> float:
     """Throughput of the whole job: the units every rank processed over the
     slowest rank's time (ms), in units of `scale` per second."""
@@ -569,9 +597,10 @@ def main():
     }
 
     # ---- end to end through the public API with host buffers -------------
-    pinned = torch.as_tensor(pts_host).pin_memory()
-    q_host = torch.as_tensor(np.random.default_rng(1).integers(0, nvox, 100_000).astype(np.int32)).pin_memory()
-    out_host = torch.empty(q_host.shape[0], dtype=torch.int32).pin_memory()
+    (pinned, q_host, out_host), pinned_where = pinned_near_gpu(torch, [
+        torch.as_tensor(pts_host),
+        torch.as_tensor(np.random.default_rng(1).integers(0, nvox, 100_000).astype(np.int32)),
+        torch.empty(100_000, dtype=torch.int32)])
     pts_dev = torch.empty_like(pts)
     q_dev = torch.empty(q_host.shape[0], dtype=torch.int32, device="cuda")
     out_dev = torch.empty(q_host.shape[0], dtype=torch.int32, device="cuda")
@@ -599,7 +628,8 @@ def main():
            "d2h_bytes_per_step": int(out_host.numel() * 4),
            "ms_per_step": round(e2e_ms / args.steps, 4),
            "path": "pinned points + query ids H2D, voxelize_edt (clearMap + insertPointCloud + "
-                   "parallelBanding3D in one call), getSquaredDistances (100k ids), result D2H"}
+                   "parallelBanding3D in one call), getSquaredDistances (100k ids), result D2H",
+           "pinned_memory": pinned_where}
 
     line = {
         "metric": "edt_gvoxel_per_s", "value": round(value, 3), "unit": "Gvoxel/s", "n_gpus": world,
