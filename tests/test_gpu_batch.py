@@ -92,3 +92,31 @@ def test_batch_voxelize_edt_equals_clear_insert_edt():
     assert b.edt_check() == 0
     for ma, mb in zip(maps_a, maps_b):
         assert torch.equal(ma.data(), mb.data())
+
+
+def test_batch_thin_maps_items_span_slices():
+    """Maps with x or y below 32 (or 1): one warp item covers columns of several
+    z slices, so Y items bump and X items wait on several slice counters."""
+    dims_list = [(1, 40, 60), (5, 3, 100), (33, 1, 20), (70, 9, 2), (1, 1, 300), (31, 33, 17)]
+    rng = np.random.default_rng(21)
+    scenes = []
+    for dims in dims_list:
+        n = max(1, int(np.prod(dims)) // 50)
+        pts = (rng.random((n, 3)) * np.asarray(dims)).astype(np.float32)
+        scenes.append((dims, 1.0, pts))
+    maps = [gvx.DistanceVoxelMap(d, s) for d, s, _ in scenes]
+    b = Batch(maps)
+    pts, offs = _cat(scenes)
+    b.voxelize_edt(pts, offs)
+    assert b.edt_check() == 0
+    got_fused = [to_u32(m.data()).copy() for m in maps]
+    b.clear()
+    b.insert(pts, offs)
+    b.edt()
+    assert b.edt_check() == 0
+    for k, (dims, side, p) in enumerate(scenes):
+        want = oracle.dvm_empty(dims)
+        oracle.dvm_insert(want, dims, side, p)
+        oracle.pba(want, dims)
+        assert np.array_equal(got_fused[k], want), f"voxelize_edt map {k} {dims}"
+        assert np.array_equal(to_u32(maps[k].data()), want), f"edt map {k} {dims}"

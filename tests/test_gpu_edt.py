@@ -207,3 +207,26 @@ def test_bisector_quotient_equals_ieee_divide_over_domain():
     bad = ctypes.c_uint64(1)
     _abi.check(_abi.lib().gvx_check_bisector_quotient(ctypes.byref(bad)))
     assert bad.value == 0
+
+
+@pytest.mark.parametrize("dims", [(1, 40, 60), (5, 3, 100), (33, 1, 20), (70, 9, 2), (1, 1, 300), (31, 33, 17)])
+def test_thin_maps_every_sweep_configuration(dims):
+    """x or y below 32: sweep items span z slices (several slice counters per
+    item in the fused launch); every configuration and voxelize_edt agree with
+    the oracle."""
+    rng = np.random.default_rng(sum(dims))
+    pts = (rng.random((max(1, int(np.prod(dims)) // 50), 3)) * np.asarray(dims)).astype(np.float32)
+    _, want = oracle_edt(dims, 1.0, pts)
+    p = torch.as_tensor(pts).cuda()
+    m = gvx.DistanceVoxelMap(dims, 1.0)
+    for rows in (16, 32):
+        for fused in (0, 1):
+            m.set_edt_config(rows=rows, fused=fused)
+            m.clearMap()
+            m.insertPointCloud(p)
+            m.parallelBanding3D()
+            assert m.edt_check() == 0
+            assert np.array_equal(to_u32(m.data()), want), (rows, fused)
+            m.voxelize_edt(p)
+            assert m.edt_check() == 0
+            assert np.array_equal(to_u32(m.data()), want), ("voxelize", rows, fused)
