@@ -112,11 +112,13 @@ __device__ __forceinline__ void warp_fk(const gvx_arm& arm, const float* q, Warp
   __syncwarp();
 }
 
-__device__ __forceinline__ void sphere_centre(const gvx_arm& arm, const WarpFK& fk, int s, float c[3]) {
+// Sphere centre in FP64 (the distance query splits it into cell and fraction
+// in double; only the adjoint's moment arms use it rounded to float).
+__device__ __forceinline__ void sphere_centre(const gvx_arm& arm, const WarpFK& fk, int s, double c[3]) {
   const int j = arm.link[s];
   const double t = arm.t[s];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) c[i] = (float)fma(t, fk.o[j + 1][i] - fk.o[j][i], fk.o[j][i]);
+  for (int i = 0; i < 3; ++i) c[i] = fma(t, fk.o[j + 1][i] - fk.o[j][i], fk.o[j][i]);
 }
 
 constexpr int kWarpsPerBlock = 8;
@@ -132,7 +134,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) sphere_clearance_kernel(M
     warp_fk(arm, q + cfg * arm.n_joints, s_fk[warp]);
     float best = __int_as_float(0x7f800000);  // +inf
     for (int s = lane; s < arm.n_spheres; s += 32) {
-      float c[3];
+      double c[3];
       sphere_centre(arm, s_fk[warp], s, c);
       const Tri t = trilinear(m, c[0], c[1], c[2]);
       best = fminf(best, t.d * m.side - arm.r[s]);
@@ -157,7 +159,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_kernel(MapView 
     for (uint32_t w = warp; w < n_wp; w += kWarpsPerBlock) {
       warp_fk(arm, q + (traj * n_wp + w) * arm.n_joints, s_fk[warp]);
       for (int s = lane; s < arm.n_spheres; s += 32) {
-        float c[3];
+        double c[3];
         sphere_centre(arm, s_fk[warp], s, c);
         const Tri t = trilinear(m, c[0], c[1], c[2]);
         acc += fmaxf(0.0f, margin - (t.d * m.side - arm.r[s]));
@@ -200,13 +202,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapV
       float mc[3] = {0.f, 0.f, 0.f}, gg[3] = {0.f, 0.f, 0.f};
       for (int s = lane; s < arm.n_spheres; s += 32) {
         if (arm.link[s] != j) continue;
-        float c[3];
+        double c[3];
         sphere_centre(arm, s_fk[warp], s, c);
         const Tri t = trilinear(m, c[0], c[1], c[2]);
         if (margin - (t.d * m.side - arm.r[s]) > 0.0f) {
-          mc[0] += c[1] * t.gz - c[2] * t.gy;
-          mc[1] += c[2] * t.gx - c[0] * t.gz;
-          mc[2] += c[0] * t.gy - c[1] * t.gx;
+          const float cx = (float)c[0], cy = (float)c[1], cz = (float)c[2];
+          mc[0] += cy * t.gz - cz * t.gy;
+          mc[1] += cz * t.gx - cx * t.gz;
+          mc[2] += cx * t.gy - cy * t.gx;
           gg[0] += t.gx; gg[1] += t.gy; gg[2] += t.gz;
         }
       }
