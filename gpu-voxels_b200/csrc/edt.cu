@@ -15,17 +15,19 @@
 //            again; sweeping x directly in the original frame is the same
 //            computation with the roles of the site's x and y fields swapped.
 //
-// Passes Y and X: one thread per column, a warp owns 32 adjacent columns and
-// streams them through shared memory in chunks of rows (cp.async, double
-// buffered; pass X transposes each chunk on the way in and out).  Within a
-// chunk the rows advance in lockstep and only the stack pops a row triggers
-// run divergently; a lane with a long run of pops hands it to the whole warp,
-// which tests 31 stack entries per round.  The proximate-site stack is
-// compact (depth-indexed, each entry carries its row): its top lives in an
-// on-chip ring per lane together with each entry's bisector, every push is
-// written through to the map's workspace, and phase 3 streams the stack back
-// top-down through a prefetched on-chip window.  Stack order, tests and tie
-// rules are the reference's.
+// Passes Y and X: one thread per column, a warp owns 32 consecutive columns
+// (numbered slice by slice, so an item may span slices) and streams them
+// through shared memory in chunks of rows (cp.async, double buffered; pass X
+// transposes each chunk on the way in and out).  Within a chunk the rows
+// advance in lockstep and only the stack pops a row triggers run divergently;
+// a lane with a long run of pops hands it to the whole warp, which tests 31
+// stack entries per round.  The proximate-site stack is compact
+// (depth-indexed, each entry carries its row): its top lives in an on-chip
+// ring per lane together with each entry's bisector, an entry reaches the
+// map's workspace only when the ring evicts it, and phase 3 streams the stack
+// back top-down through a prefetched on-chip window.  Stack order, tests and
+// tie rules are the reference's; the bisector's quotient is rounded exactly
+// as the IEEE divide rounds it (quotient_rn).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -315,7 +317,8 @@ __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, con
   const int nch = (Z + 31) >> 5;
   // All of the column's occupancy words in flight at once (word z of chunk c
   // lands in mk[c * 32] of lane z & 31), then transposed in place: a lane
-  // reads its word before the ballots and writes its mask after them.
+  // reads its word, the butterfly exchanges registers, and the lane writes
+  // its mask back to the same slot.
   for (int c = 0; c < nch; ++c) {
     const int z = c * 32 + lane;
     if (z < Z) cp_async4(mk + c * 32, wcol + z);
