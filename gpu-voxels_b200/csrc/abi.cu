@@ -12,6 +12,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "gvx_internal.cuh"
 
@@ -302,6 +303,8 @@ gvx_status gvx_bvm_create(const gvx_dims* dims, float voxel_side, gvx_bvm** out)
 gvx_status gvx_bvm_destroy(gvx_bvm* m) {
   if (m == nullptr) return GVX_OK;
   cudaError_t e = m->d_vox ? cudaFree(m->d_vox) : cudaSuccess;
+  if (m->d_flags) cudaFree(m->d_flags);
+  if (m->d_colliding) cudaFree(m->d_colliding);
   delete m;
   return cuda_status(e, "cudaFree(BitVectorVoxelMap)");
 }
@@ -325,6 +328,60 @@ gvx_status gvx_bvm_insert_points(gvx_bvm* m, const float* d_xyz, uint64_t n, uin
   if (meaning > 255) return fail(GVX_ERR_INVALID_ARG, "meaning must be in [0, 255]");
   return cuda_status(launch_bvm_insert(m->d_vox, m->dims, m->side, d_xyz, n, meaning, d_outside, as_stream(stream)),
                      "insertPointCloud(BitVoxelMap)");
+}
+
+gvx_status gvx_bvm_insert_meta_points_self_coll(gvx_bvm* m, const float* d_xyz, const uint64_t* offsets,
+                                                uint32_t n_clouds, const uint8_t* meanings, const uint8_t* masks,
+                                                uint8_t* colliding, int* any, uint32_t* d_outside, gvx_stream stream) {
+  if (m == nullptr || offsets == nullptr || n_clouds == 0) return fail(GVX_ERR_INVALID_ARG, "need a map and at least one sub-cloud");
+  uint64_t largest = 0;
+  for (uint32_t k = 0; k < n_clouds; ++k) {
+    if (offsets[k + 1] < offsets[k]) return fail(GVX_ERR_INVALID_ARG, "sub-cloud offsets must not decrease");
+    largest = std::max<uint64_t>(largest, offsets[k + 1] - offsets[k]);
+  }
+  if (offsets[n_clouds] > offsets[0] && d_xyz == nullptr) return fail(GVX_ERR_INVALID_ARG, "points are null");
+  // default meanings eBVM_SWEPT_VOLUME_START + k (4 .. 254) and masks: every
+  // bit but eBVM_COLLISION and the sub-cloud's own meaning (BitVoxelMap.hpp:262-293)
+  constexpr uint32_t kSweptStart = 4, kSweptEnd = 254;
+  if (meanings == nullptr && n_clouds > kSweptEnd - kSweptStart + 1)
+    return fail(GVX_ERR_INVALID_ARG, "more sub-clouds than swept-volume meanings; pass meanings");
+  std::vector<uint8_t> mean(n_clouds);
+  std::vector<uint32_t> mask((size_t)n_clouds * kBitVoxelWords);
+  for (uint32_t k = 0; k < n_clouds; ++k) {
+    mean[k] = meanings ? meanings[k] : (uint8_t)(kSweptStart + k);
+    uint32_t* mk = mask.data() + (size_t)k * kBitVoxelWords;
+    if (masks) {
+      memcpy(mk, masks + (size_t)k * kBitVoxelBytes, kBitVoxelBytes);
+    } else {
+      for (uint32_t w = 0; w < kBitVoxelWords; ++w) mk[w] = 0xFFFFFFFFu;
+      mk[kEbvmCollision >> 5] &= ~(1u << (kEbvmCollision & 31));
+      mk[mean[k] >> 5] &= ~(1u << (mean[k] & 31));
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (m->d_colliding == nullptr) e = cudaMalloc(&m->d_colliding, kBitVoxelBytes);
+  if (e == cudaSuccess && largest > m->flags_cap) {  // grows with the largest sub-cloud seen
+    if (m->d_flags) cudaFree(m->d_flags);
+    m->d_flags = nullptr;
+    m->flags_cap = 0;
+    e = cudaMalloc(&m->d_flags, largest);
+    if (e == cudaSuccess) m->flags_cap = largest;
+  }
+  if (e != cudaSuccess) return cuda_status(e, "insertMetaPointCloudWithSelfCollisionCheck workspace");
+  cudaStream_t s = as_stream(stream);
+  e = launch_meta_insert_self_coll(m->d_vox, m->dims, m->side, d_xyz, offsets, n_clouds, mean.data(), mask.data(),
+                                   m->d_flags, m->d_colliding, d_outside, s);
+  uint32_t host[kBitVoxelWords] = {};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, m->d_colliding, kBitVoxelBytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "insertMetaPointCloudWithSelfCollisionCheck");
+  if (colliding) memcpy(colliding, host, kBitVoxelBytes);
+  if (any) {
+    uint32_t o = 0;
+    for (uint32_t w = 0; w < kBitVoxelWords; ++w) o |= host[w];
+    *any = o != 0;
+  }
+  return GVX_OK;
 }
 
 gvx_status gvx_bvm_collide(gvx_bvm* self, const gvx_bvm* other, const int32_t offset[3], int mark, uint64_t* d_count,

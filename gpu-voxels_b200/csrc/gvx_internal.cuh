@@ -57,6 +57,11 @@ struct gvx_bvm {
   gvx_dims dims;
   float side;
   uint8_t* d_vox;
+  // insertMetaPointCloudWithSelfCollisionCheck: per-point hit flags of the
+  // largest sub-cloud so far, and the colliding meanings (8 words)
+  uint8_t* d_flags = nullptr;
+  uint64_t flags_cap = 0;
+  uint32_t* d_colliding = nullptr;
 };
 
 struct gvx_pvm {
@@ -135,6 +140,14 @@ cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scrat
                             cudaStream_t s, int rows = 0);
 // Synchronous read of the error word the last fused launch left (0 = ok).
 cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag);
+// Sub-clouds in order (points offsets[k] .. offsets[k+1] of d_xyz, host
+// offsets): check against the map, then insert meaning[k] (+ eBVM_COLLISION
+// where hit); masks: 8 words per sub-cloud (host); d_flags: at least the
+// largest sub-cloud's points; d_colliding: 8 words, zeroed here.
+cudaError_t launch_meta_insert_self_coll(uint8_t* d_vox, gvx_dims d, float side, const float* d_xyz,
+                                         const uint64_t* offsets, uint32_t n_clouds, const uint8_t* meanings,
+                                         const uint32_t* masks, uint8_t* d_flags, uint32_t* d_colliding,
+                                         uint32_t* d_outside, cudaStream_t s);
 // Counts the quotients of the EDT bisector domain whose bits differ from the
 // IEEE divide (every numerator and divisor the sweeps can meet).
 cudaError_t check_bisector_quotient(unsigned long long* d_mismatches, cudaStream_t s);

@@ -380,6 +380,30 @@ class BitVectorVoxelMap:
             raise TypeError("collideWithTypes expects a BitVectorVoxelMap or ProbVoxelMap")
         return int(self._count.item()), types.cpu().numpy()
 
+    def insertMetaPointCloudWithSelfCollisionCheck(self, clouds, meanings=None, masks=None,
+                                                   outside: Optional[torch.Tensor] = None):
+        """BitVoxelMap::insertMetaPointCloudWithSelfCollisionCheck
+        (GV/voxelmap/BitVoxelMap.hpp:227-341).  `clouds`: one (n_k, 3) point set
+        per sub-cloud (robot link), inserted in order, each checked against the
+        map as the earlier ones left it.  meanings: one meaning per sub-cloud
+        (default eBVM_SWEPT_VOLUME_START + k); masks: (n_clouds, 32) uint8 bit
+        vectors (default: every bit but eBVM_COLLISION and the own meaning).
+        -> (self_collision: bool, colliding meanings uint8[32])."""
+        parts = [_dev_points(c) for c in clouds]
+        offsets = np.zeros(len(parts) + 1, dtype=np.uint64)
+        offsets[1:] = np.cumsum([q.shape[0] for q in parts])
+        pts = torch.cat(parts) if parts else torch.zeros((0, 3), dtype=torch.float32, device="cuda")
+        mean = None if meanings is None else np.ascontiguousarray(np.asarray(meanings, dtype=np.uint8))
+        msk = None if masks is None else np.ascontiguousarray(np.asarray(masks, dtype=np.uint8).reshape(len(parts), 32))
+        colliding = np.zeros(32, dtype=np.uint8)
+        anyc = ctypes.c_int(0)
+        call("gvx_bvm_insert_meta_points_self_coll", self._h, _ptr(pts),
+             offsets.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), len(parts),
+             None if mean is None else mean.ctypes.data_as(ctypes.c_void_p),
+             None if msk is None else msk.ctypes.data_as(ctypes.c_void_p),
+             colliding.ctypes.data_as(ctypes.c_void_p), ctypes.byref(anyc), _ptr(outside), _stream())
+        return bool(anyc.value), colliding
+
 
 class BitVectorVoxelList:
     """BitVoxelList<256, uint32> (GV/voxellist/BitVoxelList.h): sorted unique

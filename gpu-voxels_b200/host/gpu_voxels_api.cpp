@@ -58,6 +58,97 @@ struct DeviceArray {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// MetaPointCloud and the maps' generic insertMetaPointCloud
+// ---------------------------------------------------------------------------
+MetaPointCloud::MetaPointCloud(const std::vector<uint32_t>& sizes) {
+  for (uint32_t n : sizes) addCloud(n);
+}
+
+MetaPointCloud::MetaPointCloud(const std::vector<std::vector<Vector3f> >& clouds) {
+  for (const auto& c : clouds) addCloud(c);
+}
+
+MetaPointCloud::MetaPointCloud(const MetaPointCloud& other) : m_clouds(other.m_clouds), m_sizes(other.m_sizes) {}
+
+MetaPointCloud& MetaPointCloud::operator=(const MetaPointCloud& other) {
+  if (this != &other) {
+    m_clouds = other.m_clouds;
+    m_sizes = other.m_sizes;
+    m_dirty = true;
+  }
+  return *this;
+}
+
+MetaPointCloud::~MetaPointCloud() {
+  if (m_dev_xyz) cudaFree(m_dev_xyz);
+}
+
+void MetaPointCloud::addCloud(uint32_t cloud_size) {
+  m_clouds.emplace_back(cloud_size, Vector3f());
+  m_sizes.push_back(cloud_size);
+  m_dirty = true;
+}
+
+void MetaPointCloud::addCloud(const std::vector<Vector3f>& cloud, bool sync) {
+  m_clouds.push_back(cloud);
+  m_sizes.push_back((uint32_t)cloud.size());
+  m_dirty = true;
+  if (sync) syncToDevice();
+}
+
+void MetaPointCloud::updatePointCloud(uint16_t cloud, const std::vector<Vector3f>& pointcloud, bool sync) {
+  m_clouds.at(cloud) = pointcloud;
+  m_sizes.at(cloud) = (uint32_t)pointcloud.size();
+  m_dirty = true;
+  if (sync) syncToDevice();
+}
+
+uint32_t MetaPointCloud::getAccumulatedPointcloudSize() const {
+  uint64_t n = 0;
+  for (uint32_t s : m_sizes) n += s;
+  return (uint32_t)n;
+}
+
+std::vector<uint64_t> MetaPointCloud::cloudOffsets() const {
+  std::vector<uint64_t> off(m_sizes.size() + 1, 0);
+  for (size_t k = 0; k < m_sizes.size(); ++k) off[k + 1] = off[k] + m_sizes[k];
+  return off;
+}
+
+void MetaPointCloud::syncToDevice() const {
+  const uint64_t n = getAccumulatedPointcloudSize();
+  if (n > m_dev_capacity) {
+    if (m_dev_xyz) cudaFree(m_dev_xyz);
+    m_dev_xyz = nullptr;
+    m_dev_capacity = 0;
+    if (cudaMalloc(&m_dev_xyz, n * sizeof(Vector3f)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+    m_dev_capacity = n;
+  }
+  uint64_t at = 0;
+  for (const auto& c : m_clouds) {
+    if (!c.empty())
+      cudaMemcpy(m_dev_xyz + 3 * at, c.data(), c.size() * sizeof(Vector3f), cudaMemcpyHostToDevice);
+    at += c.size();
+  }
+  m_dirty = false;
+}
+
+const float* MetaPointCloud::deviceXYZ() const {
+  if (m_dirty) syncToDevice();
+  return m_dev_xyz;
+}
+
+void GpuVoxelsMap::insertMetaPointCloud(const MetaPointCloud& meta_point_cloud,
+                                        const std::vector<BitVoxelMeaning>& voxel_meanings) {
+  if (voxel_meanings.size() != meta_point_cloud.getNumberOfPointclouds())
+    throw std::invalid_argument("gpu_voxels: insertMetaPointCloud needs one meaning per sub-cloud");
+  for (uint16_t k = 0; k < meta_point_cloud.getNumberOfPointclouds(); ++k) {
+    const Vector3f* p = meta_point_cloud.getPointCloud(k);
+    insertPointCloud(std::vector<Vector3f>(p, p + meta_point_cloud.getPointcloudSize(k)), voxel_meanings[k]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // DistanceVoxelMap
 // ---------------------------------------------------------------------------
 namespace voxelmap {
@@ -347,6 +438,32 @@ size_t BitVoxelMap<length>::collideWithTypes(const ProbVoxelMap* map, BitVectorV
           "collideWithTypes"))
     return 0;
   return read_types(m_dev_count, m_dev_types, &types, true);
+}
+
+template <size_t length>
+bool BitVoxelMap<length>::insertMetaPointCloudWithSelfCollisionCheck(const MetaPointCloud* robot_links,
+                                                                     const std::vector<BitVoxelMeaning>& voxel_meanings,
+                                                                     const std::vector<BitVector<length> >& collision_masks,
+                                                                     BitVector<length>* colliding_meanings) {
+  std::lock_guard<std::recursive_timed_mutex> guard(m_mutex);
+  if (robot_links == nullptr || robot_links->getNumberOfPointclouds() == 0) return false;
+  const uint32_t n = robot_links->getNumberOfPointclouds();
+  if ((!voxel_meanings.empty() && voxel_meanings.size() != n) || (!collision_masks.empty() && collision_masks.size() != n))
+    throw std::invalid_argument("gpu_voxels: one meaning and one collision mask per sub-cloud (or none)");
+  std::vector<uint8_t> meanings(voxel_meanings.begin(), voxel_meanings.end());
+  std::vector<uint8_t> masks;
+  for (const auto& m : collision_masks) masks.insert(masks.end(), m.data(), m.data() + BitVector<length>::m_size);
+  const std::vector<uint64_t> offsets = robot_links->cloudOffsets();
+  BitVector<length> colliding;
+  int any = 0;
+  if (!ok(gvx_bvm_insert_meta_points_self_coll(m_handle, robot_links->deviceXYZ(), offsets.data(), n,
+                                               meanings.empty() ? nullptr : meanings.data(),
+                                               masks.empty() ? nullptr : masks.data(), colliding.data(), &any, nullptr,
+                                               nullptr),
+          "insertMetaPointCloudWithSelfCollisionCheck"))
+    return false;
+  if (colliding_meanings) *colliding_meanings = colliding;
+  return any != 0;
 }
 
 template <size_t length>

@@ -11,8 +11,11 @@
 
 #include "helpers/common_defines.h"
 #include "helpers/cuda_datatypes.h"
+#include "voxel/BitVoxel.h"
 
 namespace gpu_voxels {
+
+class MetaPointCloud;
 
 class GpuVoxelsMap {
  public:
@@ -44,6 +47,28 @@ class GpuVoxelsMap {
   // map type or dims.  Maps without a file form return false.
   virtual bool writeToDisk(const std::string path) { (void)path; return false; }
   virtual bool readFromDisk(const std::string path) { (void)path; return false; }
+
+  // insertMetaPointCloud (GV/GpuVoxelsMap.h:138): sub-cloud k is inserted with
+  // voxel_meanings[k] (one meaning per sub-cloud).
+  virtual void insertMetaPointCloud(const MetaPointCloud& meta_point_cloud,
+                                    const std::vector<BitVoxelMeaning>& voxel_meanings);
+  // insertMetaPointCloudWithSelfCollisionCheck (GV/GpuVoxelsMap.h:141-153):
+  // inserts the sub-clouds in order, each checked against what the earlier
+  // ones (and the map before) hold; true if any sub-cloud collided.  Empty
+  // meanings / masks select the defaults (eBVM_SWEPT_VOLUME_START + k; every
+  // bit but eBVM_COLLISION and the own meaning).  Provided by BitVoxelMap;
+  // other maps return false, as the reference's DistanceVoxelMap does.
+  virtual bool insertMetaPointCloudWithSelfCollisionCheck(
+      const MetaPointCloud* robot_links,
+      const std::vector<BitVoxelMeaning>& voxel_meanings = std::vector<BitVoxelMeaning>(),
+      const std::vector<BitVector<BIT_VECTOR_LENGTH> >& collision_masks = std::vector<BitVector<BIT_VECTOR_LENGTH> >(),
+      BitVector<BIT_VECTOR_LENGTH>* colliding_meanings = NULL) {
+    (void)robot_links;
+    (void)voxel_meanings;
+    (void)collision_masks;
+    (void)colliding_meanings;
+    return false;
+  }
   // The map's lock, for operations that lock two maps together.
   std::recursive_timed_mutex& mutexRef() const { return m_mutex; }
 

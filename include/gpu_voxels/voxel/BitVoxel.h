@@ -50,6 +50,11 @@ class BitVector {
     for (size_t i = 0; i < m_size; ++i) r.m_bytes[i] = m_bytes[i] & o.m_bytes[i];
     return r;
   }
+  BitVector operator~() const {
+    BitVector r;
+    for (size_t i = 0; i < m_size; ++i) r.m_bytes[i] = item_type(~m_bytes[i]);
+    return r;
+  }
   BitVector& operator|=(const BitVector& o) {
     for (size_t i = 0; i < m_size; ++i) m_bytes[i] |= o.m_bytes[i];
     return *this;

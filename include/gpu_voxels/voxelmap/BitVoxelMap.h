@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../GpuVoxelsMap.h"
+#include "../helpers/MetaPointCloud.h"
 #include "../voxel/BitVoxel.h"
 #include "ProbVoxelMap.h"
 
@@ -44,6 +45,17 @@ class BitVoxelMap : public GpuVoxelsMap {
                           float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
   size_t collideWithTypes(const ProbVoxelMap* map, BitVectorVoxel& types_in_collision, float coll_threshold = 1.0,
                           const Vector3i& offset = Vector3i());
+
+  // insertMetaPointCloudWithSelfCollisionCheck (GV/voxelmap/BitVoxelMap.hpp:227-341):
+  // sub-cloud k goes in after sub-clouds 0 .. k-1; a point hits when its
+  // voxel & collision_masks[k] holds a meaning other than eBVM_FREE; the hit
+  // meanings and the sub-cloud's own meaning go to colliding_meanings and the
+  // voxel gets eBVM_COLLISION.  Returns whether any sub-cloud hit.
+  bool insertMetaPointCloudWithSelfCollisionCheck(
+      const MetaPointCloud* robot_links,
+      const std::vector<BitVoxelMeaning>& voxel_meanings = std::vector<BitVoxelMeaning>(),
+      const std::vector<BitVector<length> >& collision_masks = std::vector<BitVector<length> >(),
+      BitVector<length>* colliding_meanings = NULL) override;
 
   // Raw 32-byte voxels on the device.
   uint8_t* getDeviceDataPtr();

@@ -256,6 +256,24 @@ GVX_API gvx_status gvx_bvm_clear(gvx_bvm *m, gvx_stream stream);
  * (VoxelMapOperations.hpp:241-264): sets bit `meaning` (0..255). */
 GVX_API gvx_status gvx_bvm_insert_points(gvx_bvm *m, const float *d_xyz, uint64_t n, uint32_t meaning, uint32_t *d_outside,
                                  gvx_stream stream);
+/* Replaces BitVoxelMap::insertMetaPointCloudWithSelfCollisionCheck
+ * (GV/voxelmap/BitVoxelMap.hpp:227-341; kernel kernelInsertMetaPointCloudSelfCollCheck,
+ * VoxelMapOperations.hpp:581-631).  Sub-cloud k (a robot link) is d_xyz points
+ * offsets[k] .. offsets[k+1] (host array of n_clouds + 1 entries).  Sub-clouds
+ * go in order; each first checks its voxels against the map as the earlier
+ * ones left it (voxel bits & masks[k]; a hit is any masked bit but bit 0),
+ * then sets meanings[k] in its voxels and eBVM_COLLISION where it hit.
+ * meanings: n_clouds bytes (host), NULL = eBVM_SWEPT_VOLUME_START + k.
+ * masks: n_clouds BitVectors of 32 bytes (host), NULL = every bit but
+ * eBVM_COLLISION and the sub-cloud's own meaning.  colliding (host, 32 bytes,
+ * may be NULL) receives the OR of the masked bits of every hit plus the
+ * meanings of the sub-clouds that hit; *any (may be NULL) = colliding != 0,
+ * the reference's return value.  *d_outside = 1 if a point lies outside the
+ * map.  Synchronises the stream. */
+GVX_API gvx_status gvx_bvm_insert_meta_points_self_coll(gvx_bvm *m, const float *d_xyz, const uint64_t *offsets,
+                                                        uint32_t n_clouds, const uint8_t *meanings, const uint8_t *masks,
+                                                        uint8_t *colliding, int *any, uint32_t *d_outside,
+                                                        gvx_stream stream);
 /* Replaces BitVoxelMap::collideWith(const BitVectorVoxelMap*, thr, offset)
  * (GV/voxelmap/BitVoxelMap.hpp:198-203 -> TemplateVoxelMap.hpp:588-621 ->
  * kernelCollideVoxelMapsDebug, VoxelMapOperations.hpp:129-184, DefaultCollider

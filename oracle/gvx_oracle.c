@@ -411,6 +411,47 @@ int orc_bvm_insert(uint8_t *map, const uint32_t d[3], float side, const float *x
 }
 
 /*
+ * BitVoxelMap::insertMetaPointCloudWithSelfCollisionCheck, GV/voxelmap/BitVoxelMap.hpp:227-341,
+ * with kernelInsertMetaPointCloudSelfCollCheck, GV/voxelmap/kernels/VoxelMapOperations.hpp:581-631,
+ * run one sub-cloud after the other (the reference synchronises after each)
+ * and, inside a sub-cloud, one point after the other: masked = voxel & mask;
+ * if masked has a bit but bit 0, colliding |= masked, colliding gets the
+ * sub-cloud's meaning and the voxel eBVM_COLLISION; then the voxel gets the
+ * meaning.  (With masks that keep the sub-cloud's own meaning or
+ * eBVM_COLLISION the reference's result depends on its threads' timing; the
+ * reference's defaults clear both.)  Returns the outside flag.
+ */
+int orc_bvm_insert_meta_self_coll(uint8_t *map, const uint32_t d[3], float side, const float *xyz,
+                                  const uint64_t *offsets, uint32_t n_clouds, const uint8_t *meanings,
+                                  const uint8_t *masks, uint8_t *colliding) {
+  int outside = 0;
+  memset(colliding, 0, BITVOXEL_BYTES);
+  for (uint32_t k = 0; k < n_clouds; ++k) {
+    const uint8_t *mask = masks + (size_t)k * BITVOXEL_BYTES;
+    const uint32_t meaning = meanings[k];
+    for (uint64_t i = offsets[k]; i < offsets[k + 1]; ++i) {
+      uint32_t x = orc_coord_to_voxel(xyz[3 * i + 0], side);
+      uint32_t y = orc_coord_to_voxel(xyz[3 * i + 1], side);
+      uint32_t z = orc_coord_to_voxel(xyz[3 * i + 2], side);
+      if (!(x < d[0] && y < d[1] && z < d[2])) {
+        outside = 1;
+        continue;
+      }
+      uint8_t *v = map + ((uint64_t)z * d[0] * d[1] + (uint64_t)y * d[0] + x) * BITVOXEL_BYTES;
+      uint8_t masked[BITVOXEL_BYTES];
+      for (int b = 0; b < BITVOXEL_BYTES; ++b) masked[b] = v[b] & mask[b];
+      if (!bv_none_but_empty(masked)) {
+        for (int b = 0; b < BITVOXEL_BYTES; ++b) colliding[b] |= masked[b];
+        colliding[meaning >> 3] |= (uint8_t)(1u << (meaning & 7));
+        v[EBVM_COLLISION >> 3] |= (uint8_t)(1u << (EBVM_COLLISION & 7));
+      }
+      v[meaning >> 3] |= (uint8_t)(1u << (meaning & 7));
+    }
+  }
+  return outside;
+}
+
+/*
  * BitVoxelMap::collideWith(BitVectorVoxelMap*), GV/voxelmap/BitVoxelMap.hpp:198-203
  *  -> collisionCheckWithCounterRelativeTransform, GV/voxelmap/TemplateVoxelMap.hpp:588-621
  *  -> kernelCollideVoxelMapsDebug, GV/voxelmap/kernels/VoxelMapOperations.hpp:129-184

@@ -67,6 +67,10 @@ def lib():
         L.orc_brute_sqdist.argtypes = [_u32p, _u32p, _i32p]
         L.orc_bvm_insert.argtypes = [_u8p, _u32p, ctypes.c_float, _f32p, ctypes.c_uint64, ctypes.c_uint32]
         L.orc_bvm_insert.restype = ctypes.c_int
+        L.orc_bvm_insert_meta_self_coll.argtypes = [_u8p, _u32p, ctypes.c_float, _f32p,
+                                                    np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS"),
+                                                    ctypes.c_uint32, _u8p, _u8p, _u8p]
+        L.orc_bvm_insert_meta_self_coll.restype = ctypes.c_int
         L.orc_bvm_collide.argtypes = [_u8p, _u8p, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int]
         L.orc_bvm_collide.restype = ctypes.c_uint64
         L.orc_bvm_collide_count_omp.argtypes = [_u8p, _u8p, ctypes.c_uint64]
@@ -215,6 +219,35 @@ def bvm_empty(dims) -> np.ndarray:
 def bvm_insert(bmap: np.ndarray, dims, side: float, xyz, meaning: int) -> bool:
     p = _pts(xyz)
     return bool(lib().orc_bvm_insert(bmap, _dims(dims), np.float32(side), p, p.shape[0], int(meaning)))
+
+
+EBVM_SWEPT_VOLUME_START = 4  # GV/helpers/common_defines.h:57
+
+
+def default_self_coll_masks(meanings) -> np.ndarray:
+    """insertMetaPointCloudWithSelfCollisionCheck's default masks (BitVoxelMap.hpp:
+    278-293): every bit but eBVM_COLLISION and the sub-cloud's own meaning."""
+    masks = np.full((len(meanings), 32), 0xFF, dtype=np.uint8)
+    for k, m in enumerate(meanings):
+        masks[k, 0] &= ~np.uint8(1 << 2)
+        masks[k, m >> 3] &= ~np.uint8(1 << (m & 7))
+    return masks
+
+
+def bvm_insert_meta_self_coll(bmap: np.ndarray, dims, side: float, clouds, meanings=None, masks=None):
+    """BitVoxelMap::insertMetaPointCloudWithSelfCollisionCheck; returns
+    (self_collision, colliding uint8[32], outside)."""
+    parts = [_pts(c) for c in clouds]
+    offsets = np.zeros(len(parts) + 1, dtype=np.uint64)
+    offsets[1:] = np.cumsum([q.shape[0] for q in parts])
+    xyz = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros((0, 3), np.float32), dtype=np.float32)
+    mean = np.asarray([EBVM_SWEPT_VOLUME_START + k for k in range(len(parts))] if meanings is None else meanings,
+                      dtype=np.uint8)
+    msk = default_self_coll_masks(mean) if masks is None else np.ascontiguousarray(masks, dtype=np.uint8).reshape(-1, 32)
+    colliding = np.zeros(32, dtype=np.uint8)
+    out = lib().orc_bvm_insert_meta_self_coll(bmap, _dims(dims), np.float32(side), xyz, offsets, len(parts),
+                                              np.ascontiguousarray(mean), np.ascontiguousarray(msk), colliding)
+    return bool(colliding.any()), colliding, bool(out)
 
 
 def bvm_collide(self_map: np.ndarray, other: np.ndarray, offset_linear: int = 0, mark: bool = True) -> int:

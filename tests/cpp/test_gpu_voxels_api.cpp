@@ -240,8 +240,53 @@ static void typed_collisions() {
   CHECK(list.collideWithTypeMask(&obstacle, mask) == 0, "collideWithTypeMask with a disjoint mask: 0");
 }
 
+// selfcollision_metapointcloud (GV/test/testing_voxelmap.cu), default fixture dims 89 x 123 x 74.
+static void selfcollision_metapointcloud() {
+  for (int j = 2; j < 11; j += 8) {
+    BitVectorVoxelMap map(Vector3ui(89, 123, 74), 1.f, MT_BITVECTOR_VOXELMAP);
+    const float d = 1.0f / j;
+    std::vector<std::vector<Vector3f> > colliding = {
+        box_of_points(Vector3f(2.1f, 2.1f, 2.1f), Vector3f(5.1f, 5.1f, 5.1f), d),
+        box_of_points(Vector3f(4.1f, 4.1f, 4.1f), Vector3f(7.1f, 7.1f, 7.1f), d),
+        box_of_points(Vector3f(6.1f, 6.1f, 6.1f), Vector3f(9.1f, 9.1f, 9.1f), d),
+        box_of_points(Vector3f(10.1f, 10.1f, 10.1f), Vector3f(12.1f, 12.1f, 12.1f), d)};
+    std::vector<std::vector<Vector3f> > separate = {
+        box_of_points(Vector3f(30.1f, 30.1f, 30.1f), Vector3f(32.1f, 32.1f, 32.1f), d),
+        box_of_points(Vector3f(40.1f, 40.1f, 40.1f), Vector3f(43.1f, 43.1f, 43.1f), d),
+        box_of_points(Vector3f(60.1f, 60.1f, 60.1f), Vector3f(64.1f, 64.1f, 64.1f), d),
+        box_of_points(Vector3f(65.1f, 65.1f, 65.1f), Vector3f(68.1f, 68.1f, 68.1f), d)};
+    MetaPointCloud mc(colliding), ms(separate);
+    CHECK(map.insertMetaPointCloudWithSelfCollisionCheck(&mc), "selfcollision: default masks, overlapping boxes");
+    CHECK(!map.insertMetaPointCloudWithSelfCollisionCheck(&ms), "selfcollision: default masks, separate boxes");
+    map.clearMap();
+    std::vector<BitVoxelMeaning> meanings = {BitVoxelMeaning(51), BitVoxelMeaning(52), BitVoxelMeaning(53),
+                                             BitVoxelMeaning(54)};
+    BitVector<BIT_VECTOR_LENGTH> all;
+    all = ~all;
+    all.clearBit(eBVM_COLLISION);
+    std::vector<BitVector<BIT_VECTOR_LENGTH> > masks(4, all);
+    masks[0].clearBit(52);
+    masks[1].clearBit(51);
+    for (int k = 0; k < 4; ++k) masks[k].clearBit(51 + k);
+    BitVector<BIT_VECTOR_LENGTH> hit;
+    bool self = map.insertMetaPointCloudWithSelfCollisionCheck(&mc, meanings, masks, &hit);
+    const bool bits_ok = !hit.getBit(51) && hit.getBit(52) && hit.getBit(53) && !hit.getBit(54);
+    hit.clearBit(52);
+    hit.clearBit(53);
+    CHECK(self && bits_ok && hit.isZero(), "selfcollision: masks, meanings 52 and 53 only");
+    for (int k = 0; k < 4; ++k) {
+      masks[k] = all;
+      masks[k].clearBit(51 + k);
+    }
+    hit.clear();
+    self = map.insertMetaPointCloudWithSelfCollisionCheck(&ms, meanings, masks, &hit);
+    CHECK(!self && hit.isZero(), "selfcollision: masks, separate boxes");
+  }
+}
+
 int main() {
   GpuVoxels::getInstance();
+  selfcollision_metapointcloud();
   distance_consumers();
   typed_collisions();
   distance_extraction();

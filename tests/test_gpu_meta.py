@@ -1,0 +1,64 @@
+"""insertMetaPointCloudWithSelfCollisionCheck on the GPU against the oracle:
+the reference test's known answers, random multi-link clouds over existing
+map content, and user meanings and masks (masks clear the sub-cloud's own
+meaning and eBVM_COLLISION, as the reference's defaults do: with those bits
+kept the reference's own result depends on its threads' timing)."""
+import numpy as np
+import pytest
+import torch
+
+import gvx
+import oracle
+from test_oracle_meta import COLLIDING, DIMS, NONCOLLIDING, _all_but, _boxes
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(c):
+    return {b for b in range(256) if c[b >> 3] >> (b & 7) & 1}
+
+
+@pytest.mark.parametrize("j", [2, 10])
+def test_reference_known_answers(j):
+    m = gvx.BitVectorVoxelMap(DIMS, 1.0)
+    hit, _ = m.insertMetaPointCloudWithSelfCollisionCheck(_boxes(COLLIDING, j))
+    assert hit is True
+    hit, _ = m.insertMetaPointCloudWithSelfCollisionCheck(_boxes(NONCOLLIDING, j))
+    assert hit is False
+    m.clearMap()
+    meanings = [51, 52, 53, 54]
+    masks = np.stack([_all_but(2, 52, 51), _all_but(2, 51, 52), _all_but(2, 53), _all_but(2, 54)])
+    hit, coll = m.insertMetaPointCloudWithSelfCollisionCheck(_boxes(COLLIDING, j), meanings, masks)
+    assert hit is True and _bits(coll) == {52, 53}
+    masks = np.stack([_all_but(2, 51), _all_but(2, 52), _all_but(2, 53), _all_but(2, 54)])
+    hit, coll = m.insertMetaPointCloudWithSelfCollisionCheck(_boxes(NONCOLLIDING, j), meanings, masks)
+    assert hit is False and not coll.any()
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_random_links_match_oracle(seed):
+    rng = np.random.default_rng(seed)
+    dims = (64, 80, 50)
+    env = (rng.random((3000, 3)) * np.asarray(dims) * 0.05).astype(np.float32)
+    links = []
+    for k in range(9):  # overlapping blobs along a chain, a few points outside the map
+        c = rng.random(3) * np.asarray(dims) * 0.05
+        pts = c + rng.normal(scale=0.2, size=(int(rng.integers(50, 4000)), 3))
+        links.append(pts.astype(np.float32))
+    links[3][:5] = 1000.0  # beyond the map (negative coordinates land in voxel 0)
+    meanings = None if seed == 0 else rng.choice(np.arange(4, 255), size=len(links), replace=False)
+    masks = None
+    if seed == 2:  # random masks, own meaning and eBVM_COLLISION cleared
+        masks = rng.integers(0, 256, size=(len(links), 32)).astype(np.uint8)
+        for k, mk in enumerate(meanings):
+            masks[k] &= _all_but(2, int(mk))
+    want = oracle.bvm_empty(dims)
+    oracle.bvm_insert(want, dims, 0.05, env, 1)
+    hit_o, coll_o, out_o = oracle.bvm_insert_meta_self_coll(want, dims, 0.05, links, meanings, masks)
+    m = gvx.BitVectorVoxelMap(dims, 0.05)
+    m.insertPointCloud(torch.as_tensor(env).cuda(), meaning=1)
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    hit, coll = m.insertMetaPointCloudWithSelfCollisionCheck(links, meanings, masks, outside=flag)
+    assert hit == hit_o and np.array_equal(coll, coll_o)
+    assert bool(flag.item()) == out_o
+    assert np.array_equal(m.voxels().cpu().numpy().reshape(-1), want)
