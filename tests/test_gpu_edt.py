@@ -230,3 +230,20 @@ def test_thin_maps_every_sweep_configuration(dims):
             m.voxelize_edt(p)
             assert m.edt_check() == 0
             assert np.array_equal(to_u32(m.data()), want), ("voxelize", rows, fused)
+
+
+@pytest.mark.parametrize("dims,npts", [((1023, 40, 3), 30), ((1023, 40, 3), 20000), ((7, 1023, 5), 40),
+                                       ((1023, 1023, 1), 300)])
+def test_longest_rows(dims, npts):
+    """Rows of 1023 voxels along x or y: stacks up to 1023 entries deep and the
+    largest bisector divisors (2046), sparse and dense, fused and separate."""
+    rng = np.random.default_rng(npts)
+    pts = (rng.random((npts, 3)) * np.asarray(dims)).astype(np.float32)
+    _, want = oracle_edt(dims, 1.0, pts)
+    p = torch.as_tensor(pts).cuda()
+    m = gvx.DistanceVoxelMap(dims, 1.0)
+    for fused in (1, 0):
+        m.set_edt_config(rows=16, fused=fused)
+        m.voxelize_edt(p)
+        assert m.edt_check() == 0
+        assert np.array_equal(to_u32(m.data()), want), fused
