@@ -254,6 +254,37 @@ void DistanceVoxelMap::parallelBanding3D(uint32_t m1, uint32_t m2, uint32_t m3, 
   cudaDeviceSynchronize();  // the reference returns with the EDT complete
 }
 
+void DistanceVoxelMap::jumpFlood3D(int, int, bool) { parallelBanding3D(); }
+
+void DistanceVoxelMap::exactDistances3D(std::vector<Vector3f>& points) {
+  lock_guard g(m_mutex);
+  DevicePoints d(points);
+  ok(gvx_dvm_voxelize_edt(m_handle, d.p, points.size(), nullptr, nullptr), "exactDistances3D");
+  cudaDeviceSynchronize();
+}
+
+void DistanceVoxelMap::fill_pba_uninit() { fill_pba_uninit(*this); }
+
+void DistanceVoxelMap::fill_pba_uninit(DistanceVoxelMap& other) {
+  lock_guard g(other.m_mutex);
+  ok(gvx_dvm_clear(other.m_handle, nullptr), "fill_pba_uninit");
+  cudaDeviceSynchronize();
+}
+
+size_t DistanceVoxelMap::collideWithTypes(const GpuVoxelsMapSharedPtr, BitVectorVoxel&, float, const Vector3ui&) {
+  return 0;
+}
+
+void DistanceVoxelMap::clearBitVoxelMeaning(BitVoxelMeaning) {}
+
+bool DistanceVoxelMap::insertMetaPointCloudWithSelfCollisionCheck(const MetaPointCloud*,
+                                                                  const std::vector<BitVoxelMeaning>&,
+                                                                  const std::vector<BitVector<BIT_VECTOR_LENGTH> >&,
+                                                                  BitVector<BIT_VECTOR_LENGTH>*) {
+  std::fprintf(stderr, "gpu_voxels: insertMetaPointCloudWithSelfCollisionCheck: operation not supported by a DistanceVoxelMap\n");
+  return true;
+}
+
 void DistanceVoxelMap::extract_distances(free_space_t* dev_distances, int robot_radius) const {
   lock_guard g(m_mutex);
   ok(gvx_dvm_extract_distances(m_handle, dev_distances, robot_radius, nullptr), "extract_distances");

@@ -68,6 +68,30 @@ class DistanceVoxelMap : public GpuVoxelsMap {
                          uint32_t m2_blocksize = PBA_DEFAULT_M2_BLOCK_SIZE,
                          uint32_t m3_blocksize = PBA_DEFAULT_M3_BLOCK_SIZE, bool detailtimer = false);
 
+  // The reference's other two EDTs, kept for source compatibility.  Both
+  // compute the exact transform of parallelBanding3D: jumpFlood3D
+  // (DistanceVoxelMap.hpp:141-206) is an approximation in the reference, and
+  // exactDistances3D (DistanceVoxelMap.hpp:208-251: brute force over `points`,
+  // every voxel written) gives the same squared distances; a voxel equally
+  // near two obstacles may name the other one as its site.
+  void jumpFlood3D(int block_size = 1024, int debug = 0, bool logging_reinit = false);
+  void exactDistances3D(std::vector<Vector3f>& points);
+  // fill_pba_uninit (DistanceVoxelMap.hpp:647-657): every voxel of `other`
+  // (of this map) set to the uninitialised DistanceVoxel.
+  void fill_pba_uninit();
+  void fill_pba_uninit(DistanceVoxelMap& other);
+  // No-ops in the reference for a DistanceVoxelMap (DistanceVoxelMap.hpp:85-107):
+  // collideWithTypes returns 0, clearBitVoxelMeaning does nothing, and the
+  // self-collision insert reports the operation as unsupported and returns true.
+  size_t collideWithTypes(const GpuVoxelsMapSharedPtr other, BitVectorVoxel& meanings_in_collision,
+                          float coll_threshold = 1.0, const Vector3ui& offset = Vector3ui());
+  void clearBitVoxelMeaning(BitVoxelMeaning voxel_meaning);
+  bool insertMetaPointCloudWithSelfCollisionCheck(
+      const MetaPointCloud* robot_links,
+      const std::vector<BitVoxelMeaning>& voxel_meanings = std::vector<BitVoxelMeaning>(),
+      const std::vector<BitVector<BIT_VECTOR_LENGTH> >& collision_masks = std::vector<BitVector<BIT_VECTOR_LENGTH> >(),
+      BitVector<BIT_VECTOR_LENGTH>* colliding_meanings = NULL) override;
+
   // mergeOccupied (GV/voxelmap/DistanceVoxelMap.hpp:109-136): voxels of `other`
   // whose occupancy exceeds the threshold become sites (own coordinates +
   // voxel_offset).  Returns false when the maps' dims differ.

@@ -284,8 +284,32 @@ static void selfcollision_metapointcloud() {
   }
 }
 
+// The reference's other EDT entry points give parallelBanding3D's squared distances.
+static void other_edt_entry_points() {
+  const Vector3ui dims(40, 36, 30);
+  std::vector<Vector3f> pts = equidistant(60, dims, 1.f);
+  voxelmap::DistanceVoxelMap a(dims, 1.f), b(dims, 1.f), c(dims, 1.f);
+  a.insertPointCloud(pts, eBVM_OCCUPIED);
+  a.parallelBanding3D();
+  b.insertPointCloud(pts, eBVM_OCCUPIED);
+  b.jumpFlood3D();
+  c.insertPointCloud(std::vector<Vector3f>(1, Vector3f(1.5f, 1.5f, 1.5f)), eBVM_OCCUPIED);  // replaced below
+  c.exactDistances3D(pts);
+  bool same = true;
+  for (uint32_t z = 0; z < dims.z; z += 3)
+    for (uint32_t y = 0; y < dims.y; y += 5)
+      for (uint32_t x = 0; x < dims.x; x += 7) {
+        const int32_t d = a.getSquaredObstacleDistance(x, y, z);
+        same = same && b.getSquaredObstacleDistance(x, y, z) == d && c.getSquaredObstacleDistance(x, y, z) == d;
+      }
+  CHECK(same, "jumpFlood3D / exactDistances3D: parallelBanding3D's squared distances");
+  a.fill_pba_uninit();
+  CHECK(a.getSquaredObstacleDistance(3, 3, 3) == INT32_MAX, "fill_pba_uninit: no sites left");
+}
+
 int main() {
   GpuVoxels::getInstance();
+  other_edt_entry_points();
   selfcollision_metapointcloud();
   distance_consumers();
   typed_collisions();
