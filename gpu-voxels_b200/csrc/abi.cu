@@ -330,6 +330,19 @@ gvx_status gvx_bvm_insert_points(gvx_bvm* m, const float* d_xyz, uint64_t n, uin
                      "insertPointCloud(BitVoxelMap)");
 }
 
+gvx_status gvx_bvm_clear_bits(gvx_bvm* m, const uint8_t* bits, gvx_stream stream) {
+  if (m == nullptr || bits == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  uint32_t w[kBitVoxelWords];
+  memcpy(w, bits, kBitVoxelBytes);
+  return cuda_status(launch_bvm_clear_bits(m->d_vox, m->dims, w, as_stream(stream)), "clearBits(BitVoxelMap)");
+}
+
+gvx_status gvx_bvm_shift_swept_volume_ids(gvx_bvm* m, uint32_t shift, gvx_stream stream) {
+  if (m == nullptr) return fail(GVX_ERR_INVALID_ARG, "map is null");
+  if (shift > 56) return fail(GVX_ERR_INVALID_ARG, "maximum shift size is 56");
+  return cuda_status(launch_bvm_shift(m->d_vox, m->dims, shift, as_stream(stream)), "shiftLeftSweptVolumeIDs");
+}
+
 gvx_status gvx_bvm_insert_meta_points_self_coll(gvx_bvm* m, const float* d_xyz, const uint64_t* offsets,
                                                 uint32_t n_clouds, const uint8_t* meanings, const uint8_t* masks,
                                                 uint8_t* colliding, int* any, uint32_t* d_outside, gvx_stream stream) {

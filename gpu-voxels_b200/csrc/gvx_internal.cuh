@@ -140,6 +140,10 @@ cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scrat
                             cudaStream_t s, int rows = 0);
 // Synchronous read of the error word the last fused launch left (0 = ok).
 cudaError_t edt_read_error(const uint32_t* d_scratch, gvx_dims d, uint32_t* flag);
+// BitVoxelMap bit maintenance: clear `bits` (8 words) in every voxel; move
+// every voxel's bits down by `shift` (<= 56) and clear meanings 0..3.
+cudaError_t launch_bvm_clear_bits(uint8_t* d_vox, gvx_dims d, const uint32_t bits[8], cudaStream_t s);
+cudaError_t launch_bvm_shift(uint8_t* d_vox, gvx_dims d, uint32_t shift, cudaStream_t s);
 // Sub-clouds in order (points offsets[k] .. offsets[k+1] of d_xyz, host
 // offsets): check against the map, then insert meaning[k] (+ eBVM_COLLISION
 // where hit); masks: 8 words per sub-cloud (host); d_flags: at least the

@@ -70,6 +70,45 @@ __global__ void bvm_insert_kernel(uint32_t* __restrict__ map, uint32_t X, uint32
   if (outside != nullptr && __any_sync(0xffffffffu, out) && (threadIdx.x & 31) == 0) *outside = 1u;
 }
 
+// kernelClearVoxelMap(BitVoxel*, size, BitVector bits) (VoxelMapOperations.hpp:57-71):
+// clears `bits` in every voxel (clearBit / clearBitVoxelMeaning use one bit).
+__global__ void bvm_clear_bits_kernel(uint4* __restrict__ vox, uint64_t n, uint4 lo, uint4 hi) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint4 a = vox[2 * i], b = vox[2 * i + 1];
+    a.x &= ~lo.x; a.y &= ~lo.y; a.z &= ~lo.z; a.w &= ~lo.w;
+    b.x &= ~hi.x; b.y &= ~hi.y; b.z &= ~hi.z; b.w &= ~hi.w;
+    vox[2 * i] = a;
+    vox[2 * i + 1] = b;
+  }
+}
+
+// kernelShiftBitVector / performLeftShift (VoxelMapOperations.hpp:813-820,
+// GV/helpers/BitVector.h:355-402): every voxel's 256 bits move down by
+// `shift` (<= 56) bit positions -- swept-volume meaning k becomes k - shift --
+// and the four meanings below eBVM_SWEPT_VOLUME_START are cleared.
+__global__ void bvm_shift_kernel(uint32_t* __restrict__ vox, uint64_t n, uint32_t shift) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t ws = shift >> 5, bs = shift & 31;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t* v = vox + i * kBitVoxelWords;
+    uint32_t in[kBitVoxelWords + 2];
+#pragma unroll
+    for (int w = 0; w < (int)kBitVoxelWords; ++w) in[w] = v[w];
+    in[kBitVoxelWords] = in[kBitVoxelWords + 1] = 0u;
+    uint32_t out[kBitVoxelWords];
+#pragma unroll
+    for (int w = 0; w < (int)kBitVoxelWords; ++w) {
+      const uint32_t lo = w + ws < kBitVoxelWords + 2 ? in[w + ws] : 0u;
+      const uint32_t hi = w + ws + 1 < kBitVoxelWords + 2 ? in[w + ws + 1] : 0u;
+      out[w] = (uint32_t)((((uint64_t)hi << 32) | lo) >> bs);
+    }
+    out[0] &= ~0xFu;
+#pragma unroll
+    for (int w = 0; w < (int)kBitVoxelWords; ++w) v[w] = out[w];
+  }
+}
+
 unsigned grid_for(uint64_t n, int threads) {
   const uint64_t want = (n + threads - 1) / threads;
   const uint64_t cap = (uint64_t)num_sms() * 16;
@@ -98,6 +137,20 @@ cudaError_t launch_bvm_insert(uint8_t* d_vox, gvx_dims d, float side, const floa
   if (n == 0) return cudaSuccess;
   bvm_insert_kernel<<<grid_for(n, 256), 256, 0, s>>>(reinterpret_cast<uint32_t*>(d_vox), d.x, d.y, d.z, side, d_xyz, n,
                                                      meaning, d_outside);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bvm_clear_bits(uint8_t* d_vox, gvx_dims d, const uint32_t bits[8], cudaStream_t s) {
+  const uint64_t n = (uint64_t)d.x * d.y * d.z;
+  bvm_clear_bits_kernel<<<grid_for(n, 256), 256, 0, s>>>(reinterpret_cast<uint4*>(d_vox), n,
+                                                         make_uint4(bits[0], bits[1], bits[2], bits[3]),
+                                                         make_uint4(bits[4], bits[5], bits[6], bits[7]));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bvm_shift(uint8_t* d_vox, gvx_dims d, uint32_t shift, cudaStream_t s) {
+  const uint64_t n = (uint64_t)d.x * d.y * d.z;
+  bvm_shift_kernel<<<grid_for(n, 256), 256, 0, s>>>(reinterpret_cast<uint32_t*>(d_vox), n, shift);
   return cudaGetLastError();
 }
 

@@ -380,6 +380,24 @@ class BitVectorVoxelMap:
             raise TypeError("collideWithTypes expects a BitVectorVoxelMap or ProbVoxelMap")
         return int(self._count.item()), types.cpu().numpy()
 
+    def clearBits(self, bits) -> None:
+        """BitVoxelMap::clearBits: clear the set bits of `bits` (32 uint8) in every voxel."""
+        b = np.ascontiguousarray(np.asarray(bits, dtype=np.uint8).reshape(32))
+        call("gvx_bvm_clear_bits", self._h, b.ctypes.data_as(ctypes.c_void_p), _stream())
+
+    def clearBit(self, bit_index: int) -> None:
+        b = np.zeros(32, dtype=np.uint8)
+        b[int(bit_index) >> 3] = 1 << (int(bit_index) & 7)
+        self.clearBits(b)
+
+    def clearBitVoxelMeaning(self, voxel_meaning: int) -> None:
+        self.clearBit(voxel_meaning)
+
+    def shiftLeftSweptVolumeIDs(self, shift_size: int) -> None:
+        """BitVoxelMap::shiftLeftSweptVolumeIDs: meaning k -> k - shift_size
+        (<= 56), meanings 0..3 cleared."""
+        call("gvx_bvm_shift_swept_volume_ids", self._h, int(shift_size), _stream())
+
     def insertMetaPointCloudWithSelfCollisionCheck(self, clouds, meanings=None, masks=None,
                                                    outside: Optional[torch.Tensor] = None):
         """BitVoxelMap::insertMetaPointCloudWithSelfCollisionCheck

@@ -472,6 +472,32 @@ size_t BitVoxelMap<length>::collideWithTypes(const ProbVoxelMap* map, BitVectorV
 }
 
 template <size_t length>
+void BitVoxelMap<length>::clearBits(BitVector<length> bits) {
+  std::lock_guard<std::recursive_timed_mutex> guard(m_mutex);
+  ok(gvx_bvm_clear_bits(m_handle, bits.data(), nullptr), "clearBits");
+  cudaDeviceSynchronize();
+}
+
+template <size_t length>
+void BitVoxelMap<length>::clearBit(const uint32_t bit_index) {
+  BitVector<length> b;
+  b.setBit(bit_index);
+  clearBits(b);
+}
+
+template <size_t length>
+void BitVoxelMap<length>::clearBitVoxelMeaning(BitVoxelMeaning voxel_meaning) {
+  clearBit(uint32_t(voxel_meaning));
+}
+
+template <size_t length>
+void BitVoxelMap<length>::shiftLeftSweptVolumeIDs(uint8_t shift_size) {
+  std::lock_guard<std::recursive_timed_mutex> guard(m_mutex);
+  ok(gvx_bvm_shift_swept_volume_ids(m_handle, shift_size, nullptr), "shiftLeftSweptVolumeIDs");
+  cudaDeviceSynchronize();
+}
+
+template <size_t length>
 bool BitVoxelMap<length>::insertMetaPointCloudWithSelfCollisionCheck(const MetaPointCloud* robot_links,
                                                                      const std::vector<BitVoxelMeaning>& voxel_meanings,
                                                                      const std::vector<BitVector<length> >& collision_masks,

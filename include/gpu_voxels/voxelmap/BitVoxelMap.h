@@ -46,6 +46,16 @@ class BitVoxelMap : public GpuVoxelsMap {
   size_t collideWithTypes(const ProbVoxelMap* map, BitVectorVoxel& types_in_collision, float coll_threshold = 1.0,
                           const Vector3i& offset = Vector3i());
 
+  // clearBit / clearBits / clearBitVoxelMeaning (GV/voxelmap/BitVoxelMap.hpp:63-88,343-347):
+  // the given bit(s) cleared in every voxel.
+  void clearBit(const uint32_t bit_index);
+  void clearBits(BitVector<length> bits);
+  void clearBitVoxelMeaning(BitVoxelMeaning voxel_meaning);
+  // shiftLeftSweptVolumeIDs (BitVoxelMap.hpp:349-361): swept-volume meaning k
+  // becomes k - shift_size in every voxel, meanings 0..3 are cleared; shifts
+  // above 56 are refused (message, no change), as in the reference.
+  void shiftLeftSweptVolumeIDs(uint8_t shift_size);
+
   // insertMetaPointCloudWithSelfCollisionCheck (GV/voxelmap/BitVoxelMap.hpp:227-341):
   // sub-cloud k goes in after sub-clouds 0 .. k-1; a point hits when its
   // voxel & collision_masks[k] holds a meaning other than eBVM_FREE; the hit

@@ -256,6 +256,16 @@ GVX_API gvx_status gvx_bvm_clear(gvx_bvm *m, gvx_stream stream);
  * (VoxelMapOperations.hpp:241-264): sets bit `meaning` (0..255). */
 GVX_API gvx_status gvx_bvm_insert_points(gvx_bvm *m, const float *d_xyz, uint64_t n, uint32_t meaning, uint32_t *d_outside,
                                  gvx_stream stream);
+/* Replaces BitVoxelMap::clearBits / clearBit / clearBitVoxelMeaning
+ * (GV/voxelmap/BitVoxelMap.hpp:63-88,343-347; kernelClearVoxelMap,
+ * VoxelMapOperations.hpp:45-71): clears the set bits of `bits` (host, 32
+ * bytes, BitVector<256> layout) in every voxel. */
+GVX_API gvx_status gvx_bvm_clear_bits(gvx_bvm *m, const uint8_t *bits, gvx_stream stream);
+/* Replaces BitVoxelMap::shiftLeftSweptVolumeIDs (BitVoxelMap.hpp:349-361;
+ * performLeftShift, GV/helpers/BitVector.h:355-402): every voxel's meaning k
+ * becomes k - shift (lower ones drop out) and meanings 0..3 are cleared.
+ * shift <= 56, else GVX_ERR_INVALID_ARG and nothing changes. */
+GVX_API gvx_status gvx_bvm_shift_swept_volume_ids(gvx_bvm *m, uint32_t shift, gvx_stream stream);
 /* Replaces BitVoxelMap::insertMetaPointCloudWithSelfCollisionCheck
  * (GV/voxelmap/BitVoxelMap.hpp:227-341; kernel kernelInsertMetaPointCloudSelfCollCheck,
  * VoxelMapOperations.hpp:581-631).  Sub-cloud k (a robot link) is d_xyz points

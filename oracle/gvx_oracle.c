@@ -410,6 +410,38 @@ int orc_bvm_insert(uint8_t *map, const uint32_t d[3], float side, const float *x
   return outside;
 }
 
+/* kernelClearVoxelMap(BitVoxel*, size, BitVector bits), GV/voxelmap/kernels/VoxelMapOperations.hpp:57-71:
+ * a voxel holding any of `bits` keeps only its other bits. */
+void orc_bvm_clear_bits(uint8_t *map, uint64_t n, const uint8_t *bits) {
+  for (uint64_t i = 0; i < n; ++i) {
+    uint8_t *v = map + i * BITVOXEL_BYTES;
+    int any = 0;
+    for (int b = 0; b < BITVOXEL_BYTES; ++b) any |= v[b] & bits[b];
+    if (any)
+      for (int b = 0; b < BITVOXEL_BYTES; ++b) v[b] &= (uint8_t)~bits[b];
+  }
+}
+
+/* performLeftShift, GV/helpers/BitVector.h:355-402, on every voxel
+ * (kernelShiftBitVector, VoxelMapOperations.hpp:813-820): a 64-bit buffer
+ * holds eight input bytes; each output byte is the buffer shifted right by
+ * `shift`, the buffer then moves on by one byte and takes in the byte eight
+ * further on; output byte 0 keeps only its upper four bits. */
+void orc_bvm_shift(uint8_t *map, uint64_t n, uint32_t shift) {
+  for (uint64_t i = 0; i < n; ++i) {
+    uint8_t *v = map + i * BITVOXEL_BYTES;
+    uint64_t buffer = 0;
+    for (uint32_t b = 0; b < 8; ++b) buffer += (uint64_t)v[b] << (b * 8);
+    for (uint32_t b = 0; b < BITVOXEL_BYTES; ++b) {
+      uint8_t out = (uint8_t)(buffer >> shift);
+      if (b == 0) out &= 0xF0;
+      v[b] = out;
+      buffer >>= 8;
+      if (b + 8 < BITVOXEL_BYTES) buffer += (uint64_t)v[b + 8] << 56;
+    }
+  }
+}
+
 /*
  * BitVoxelMap::insertMetaPointCloudWithSelfCollisionCheck, GV/voxelmap/BitVoxelMap.hpp:227-341,
  * with kernelInsertMetaPointCloudSelfCollCheck, GV/voxelmap/kernels/VoxelMapOperations.hpp:581-631,

@@ -67,6 +67,8 @@ def lib():
         L.orc_brute_sqdist.argtypes = [_u32p, _u32p, _i32p]
         L.orc_bvm_insert.argtypes = [_u8p, _u32p, ctypes.c_float, _f32p, ctypes.c_uint64, ctypes.c_uint32]
         L.orc_bvm_insert.restype = ctypes.c_int
+        L.orc_bvm_clear_bits.argtypes = [_u8p, ctypes.c_uint64, _u8p]
+        L.orc_bvm_shift.argtypes = [_u8p, ctypes.c_uint64, ctypes.c_uint32]
         L.orc_bvm_insert_meta_self_coll.argtypes = [_u8p, _u32p, ctypes.c_float, _f32p,
                                                     np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS"),
                                                     ctypes.c_uint32, _u8p, _u8p, _u8p]
@@ -222,6 +224,18 @@ def bvm_insert(bmap: np.ndarray, dims, side: float, xyz, meaning: int) -> bool:
 
 
 EBVM_SWEPT_VOLUME_START = 4  # GV/helpers/common_defines.h:57
+
+
+def bvm_clear_bits(bmap: np.ndarray, bits) -> np.ndarray:
+    """BitVoxelMap::clearBits on a flat uint8 map (32 bytes per voxel), in place."""
+    lib().orc_bvm_clear_bits(bmap, bmap.shape[0] // 32, np.ascontiguousarray(np.asarray(bits, np.uint8).reshape(32)))
+    return bmap
+
+
+def bvm_shift(bmap: np.ndarray, shift: int) -> np.ndarray:
+    """BitVoxelMap::shiftLeftSweptVolumeIDs (performLeftShift per voxel), in place."""
+    lib().orc_bvm_shift(bmap, bmap.shape[0] // 32, int(shift))
+    return bmap
 
 
 def default_self_coll_masks(meanings) -> np.ndarray:

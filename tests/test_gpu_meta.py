@@ -62,3 +62,32 @@ def test_random_links_match_oracle(seed):
     assert hit == hit_o and np.array_equal(coll, coll_o)
     assert bool(flag.item()) == out_o
     assert np.array_equal(m.voxels().cpu().numpy().reshape(-1), want)
+
+
+@pytest.mark.parametrize("shift", [0, 3, 13, 31, 32, 33, 56])
+def test_shift_and_clear_match_oracle(shift):
+    """shiftLeftSweptVolumeIDs and clearBits on every voxel of a random map."""
+    dims = (33, 17, 9)
+    rng = np.random.default_rng(shift)
+    raw = rng.integers(0, 256, size=int(np.prod(dims)) * 32).astype(np.uint8)
+    m = gvx.BitVectorVoxelMap(dims, 1.0)
+    m.voxels().copy_(torch.as_tensor(raw).cuda())
+    m.shiftLeftSweptVolumeIDs(shift)
+    want = oracle.bvm_shift(raw.copy(), shift)
+    assert np.array_equal(m.voxels().cpu().numpy(), want)
+    bits = rng.integers(0, 256, size=32).astype(np.uint8)
+    m.clearBits(bits)
+    oracle.bvm_clear_bits(want, bits)
+    assert np.array_equal(m.voxels().cpu().numpy(), want)
+    m.clearBitVoxelMeaning(200)
+    oracle.bvm_clear_bits(want, _all_but(*[b for b in range(256) if b != 200]))
+    assert np.array_equal(m.voxels().cpu().numpy(), want)
+
+
+def test_shift_above_56_is_refused():
+    m = gvx.BitVectorVoxelMap((4, 4, 4), 1.0)
+    m.insertPointCloud(torch.tensor([[1.5, 1.5, 1.5]], device="cuda"), meaning=100)
+    before = m.voxels().clone()
+    with pytest.raises(Exception):
+        m.shiftLeftSweptVolumeIDs(57)
+    assert torch.equal(m.voxels(), before)
