@@ -343,6 +343,23 @@ gvx_status gvx_bvm_shift_swept_volume_ids(gvx_bvm* m, uint32_t shift, gvx_stream
   return cuda_status(launch_bvm_shift(m->d_vox, m->dims, shift, as_stream(stream)), "shiftLeftSweptVolumeIDs");
 }
 
+gvx_status gvx_blist_clear_bits(gvx_blist* l, const uint8_t* bits, gvx_stream stream) {
+  if (l == nullptr || bits == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (l->n == 0) return GVX_OK;
+  uint32_t w[kBitVoxelWords];
+  memcpy(w, bits, kBitVoxelBytes);
+  return cuda_status(launch_bvm_clear_bits(l->d_vox, gvx_dims{(uint32_t)l->n, 1u, 1u}, w, as_stream(stream)),
+                     "clearBits(BitVoxelList)");
+}
+
+gvx_status gvx_blist_shift_swept_volume_ids(gvx_blist* l, uint32_t shift, gvx_stream stream) {
+  if (l == nullptr) return fail(GVX_ERR_INVALID_ARG, "list is null");
+  if (shift > 56) return fail(GVX_ERR_INVALID_ARG, "maximum shift size is 56");
+  if (l->n == 0) return GVX_OK;
+  return cuda_status(launch_bvm_shift(l->d_vox, gvx_dims{(uint32_t)l->n, 1u, 1u}, shift, as_stream(stream)),
+                     "shiftLeftSweptVolumeIDs(BitVoxelList)");
+}
+
 gvx_status gvx_bvm_insert_meta_points_self_coll(gvx_bvm* m, const float* d_xyz, const uint64_t* offsets,
                                                 uint32_t n_clouds, const uint8_t* meanings, const uint8_t* masks,
                                                 uint8_t* colliding, int* any, uint32_t* d_outside, gvx_stream stream) {

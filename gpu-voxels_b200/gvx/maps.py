@@ -452,6 +452,16 @@ class BitVectorVoxelList:
         call("gvx_blist_size", self._h, ctypes.byref(n))
         return n.value
 
+    def shiftLeftSweptVolumeIDs(self, shift_size: int) -> None:
+        """BitVoxelList::shiftLeftSweptVolumeIDs: meaning k -> k - shift_size (<= 56)
+        in every entry, meanings 0..3 cleared."""
+        call("gvx_blist_shift_swept_volume_ids", self._h, int(shift_size), _stream())
+
+    def clearBitVoxelMeaning(self, voxel_meaning: int) -> None:
+        b = np.zeros(32, dtype=np.uint8)
+        b[int(voxel_meaning) >> 3] = 1 << (int(voxel_meaning) & 7)
+        call("gvx_blist_clear_bits", self._h, b.ctypes.data_as(ctypes.c_void_p), _stream())
+
     def ids(self) -> torch.Tensor:
         n = self.getDimensions()
         pi, pv = ctypes.c_void_p(), ctypes.c_void_p()

@@ -691,6 +691,53 @@ size_t BitVoxelList<length, ID>::collideWithTypeMask(const voxelmap::BitVoxelMap
 }
 
 template <size_t length, class ID>
+void BitVoxelList<length, ID>::insertCoordinateList(const std::vector<Vector3ui>& coordinates,
+                                                    const BitVoxelMeaning voxel_meaning) {
+  std::vector<Vector3f> pts;
+  pts.reserve(coordinates.size());
+  const float s = m_voxel_side_length;
+  for (const Vector3ui& c : coordinates)  // voxel centres land in their own voxel
+    if (c.x < m_dim.x && c.y < m_dim.y && c.z < m_dim.z)
+      pts.push_back(Vector3f((c.x + 0.5f) * s, (c.y + 0.5f) * s, (c.z + 0.5f) * s));
+  insertPointCloud(pts, voxel_meaning);
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::insertCoordinateList(const Vector3ui* d_coordinates, uint32_t size,
+                                                    const BitVoxelMeaning voxel_meaning) {
+  std::vector<Vector3ui> host(size);
+  if (size) cudaMemcpy(host.data(), d_coordinates, size * sizeof(Vector3ui), cudaMemcpyDeviceToHost);
+  insertCoordinateList(host, voxel_meaning);
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::copyCoordsToHost(std::vector<Vector3ui>& host_vec) const {
+  std::vector<ID> ids;
+  copyIdsToHost(ids);
+  host_vec.resize(ids.size());
+  const uint64_t layer = (uint64_t)m_dim.x * m_dim.y;
+  for (size_t i = 0; i < ids.size(); ++i)
+    host_vec[i] = Vector3ui((uint32_t)(ids[i] % m_dim.x), (uint32_t)((ids[i] / m_dim.x) % m_dim.y),
+                            (uint32_t)(ids[i] / layer));
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::shiftLeftSweptVolumeIDs(uint8_t shift_size) {
+  lock_guard g(m_mutex);
+  ok(gvx_blist_shift_swept_volume_ids(m_handle, shift_size, nullptr), "shiftLeftSweptVolumeIDs");
+  cudaDeviceSynchronize();
+}
+
+template <size_t length, class ID>
+void BitVoxelList<length, ID>::clearBitVoxelMeaning(BitVoxelMeaning voxel_meaning) {
+  lock_guard g(m_mutex);
+  BitVector<length> b;
+  b.setBit(uint32_t(voxel_meaning));
+  ok(gvx_blist_clear_bits(m_handle, b.data(), nullptr), "clearBitVoxelMeaning");
+  cudaDeviceSynchronize();
+}
+
+template <size_t length, class ID>
 void BitVoxelList<length, ID>::copyIdsToHost(std::vector<ID>& ids) const {
   uint64_t n = 0;
   uint32_t* d = nullptr;

@@ -53,6 +53,21 @@ class BitVoxelList : public GpuVoxelsMap {
   size_t collideWithTypeMask(const voxelmap::BitVoxelMap<length>* map, const BitVectorVoxel& types_to_check,
                              float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
 
+  // insertCoordinateList (GV/voxellist/TemplateVoxelList.hpp:396-438): voxel
+  // coordinates (host or device) inserted with `voxel_meaning`, as points at
+  // the voxel centres; coordinates outside the reference dims are dropped.
+  void insertCoordinateList(const std::vector<Vector3ui>& coordinates, const BitVoxelMeaning voxel_meaning);
+  void insertCoordinateList(const Vector3ui* d_coordinates, uint32_t size, const BitVoxelMeaning voxel_meaning);
+  // copyCoordsToHost (TemplateVoxelList.hpp:292-299): the entries' voxel
+  // coordinates, in id order.
+  void copyCoordsToHost(std::vector<Vector3ui>& host_vec) const;
+  // shiftLeftSweptVolumeIDs (GV/voxellist/BitVoxelList.hpp:641-664): meaning k
+  // of every entry becomes k - shift_size (<= 56), meanings 0..3 cleared.
+  void shiftLeftSweptVolumeIDs(uint8_t shift_size);
+  // clearBitVoxelMeaning: the meaning's bit cleared in every entry (the
+  // reference's list reports this as not yet supported).
+  void clearBitVoxelMeaning(BitVoxelMeaning voxel_meaning);
+
   // Host copies of the ids and the 32-byte voxels.
   void copyIdsToHost(std::vector<VoxelIDType>& ids) const;
   void copyVoxelsToHost(std::vector<uint8_t>& voxels) const;

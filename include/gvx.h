@@ -383,6 +383,14 @@ GVX_API gvx_status gvx_blist_clear(gvx_blist *l);
  * voxelise, drop out-of-bounds, sort and merge duplicates (make_unique, :143-212).
  * Blocking. */
 GVX_API gvx_status gvx_blist_insert_points(gvx_blist *l, const float *d_xyz, uint64_t n, uint32_t meaning, gvx_stream stream);
+/* BitVoxelList::shiftLeftSweptVolumeIDs (GV/voxellist/BitVoxelList.hpp:641-664):
+ * performLeftShift on every entry's voxel (as gvx_bvm_shift_swept_volume_ids;
+ * entries stay even when their voxel becomes empty).  shift <= 56. */
+GVX_API gvx_status gvx_blist_shift_swept_volume_ids(gvx_blist *l, uint32_t shift, gvx_stream stream);
+/* Clears the set bits of `bits` (host, 32 bytes) in every entry's voxel; the
+ * C++ BitVoxelList::clearBitVoxelMeaning uses it (the reference's list
+ * reports that operation as not yet supported, BitVoxelList.hpp:57-61). */
+GVX_API gvx_status gvx_blist_clear_bits(gvx_blist *l, const uint8_t *bits, gvx_stream stream);
 /* Replaces BitVoxelList::collideWithTypes(const BitVectorVoxelMap*, ...) and
  * (const ProbVoxelMap*, ...) (GV/voxellist/BitVoxelList.hpp:120-201 ->
  * kernelCollideWithVoxelMap, GV/voxellist/kernels/VoxelListOperations.hpp:204-260):

@@ -307,8 +307,22 @@ static void other_edt_entry_points() {
   CHECK(a.getSquaredObstacleDistance(3, 3, 3) == INT32_MAX, "fill_pba_uninit: no sites left");
 }
 
+// insertCoordinateList / copyCoordsToHost round trip; out-of-map coordinates are dropped.
+static void list_coordinates() {
+  BitVectorVoxelList list(Vector3ui(50, 40, 30), 0.01f, MT_BITVECTOR_VOXELLIST);
+  std::vector<Vector3ui> coords = {Vector3ui(49, 39, 29), Vector3ui(0, 0, 0), Vector3ui(7, 8, 9), Vector3ui(7, 8, 9),
+                                   Vector3ui(50, 1, 1)};
+  list.insertCoordinateList(coords, BitVoxelMeaning(20));
+  std::vector<Vector3ui> back;
+  list.copyCoordsToHost(back);
+  CHECK(back.size() == 3 && back[0] == Vector3ui(0, 0, 0) && back[1] == Vector3ui(7, 8, 9) &&
+            back[2] == Vector3ui(49, 39, 29),
+        "insertCoordinateList / copyCoordsToHost: 3 unique in-map voxels in id order");
+}
+
 int main() {
   GpuVoxels::getInstance();
+  list_coordinates();
   other_edt_entry_points();
   selfcollision_metapointcloud();
   distance_consumers();

@@ -91,3 +91,21 @@ def test_shift_above_56_is_refused():
     with pytest.raises(Exception):
         m.shiftLeftSweptVolumeIDs(57)
     assert torch.equal(m.voxels(), before)
+
+
+def test_list_shift_and_clear_match_oracle():
+    dims = (40, 30, 20)
+    rng = np.random.default_rng(3)
+    lst = gvx.BitVectorVoxelList(dims, 1.0)
+    for meaning in (7, 40, 200, 250):
+        lst.insertPointCloud(torch.as_tensor((rng.random((500, 3)) * np.asarray(dims)).astype(np.float32)).cuda(),
+                             meaning=meaning)
+    vox = lst.voxels().cpu().numpy().reshape(-1).copy()
+    lst.shiftLeftSweptVolumeIDs(13)
+    oracle.bvm_shift(vox, 13)
+    assert np.array_equal(lst.voxels().cpu().numpy().reshape(-1), vox)
+    lst.clearBitVoxelMeaning(237)  # 250 - 13
+    b = np.zeros(32, np.uint8)
+    b[237 >> 3] = 1 << (237 & 7)
+    oracle.bvm_clear_bits(vox, b)
+    assert np.array_equal(lst.voxels().cpu().numpy().reshape(-1), vox)
