@@ -254,14 +254,22 @@ void DistanceVoxelMap::parallelBanding3D(uint32_t m1, uint32_t m2, uint32_t m3, 
   cudaDeviceSynchronize();  // the reference returns with the EDT complete
 }
 
-void DistanceVoxelMap::jumpFlood3D(int, int, bool) { parallelBanding3D(); }
-
-void DistanceVoxelMap::exactDistances3D(std::vector<Vector3f>& points) {
+void DistanceVoxelMap::voxelizeAndTransform(const std::vector<Vector3f>& points) {
   lock_guard g(m_mutex);
   DevicePoints d(points);
-  ok(gvx_dvm_voxelize_edt(m_handle, d.p, points.size(), nullptr, nullptr), "exactDistances3D");
+  voxelizeAndTransform(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size());
+}
+
+void DistanceVoxelMap::voxelizeAndTransform(const Vector3f* d_points, uint32_t size) {
+  lock_guard g(m_mutex);
+  ok(gvx_dvm_voxelize_edt(m_handle, reinterpret_cast<const float*>(d_points), size, nullptr, nullptr),
+     "voxelizeAndTransform");
   cudaDeviceSynchronize();
 }
+
+void DistanceVoxelMap::jumpFlood3D(int, int, bool) { parallelBanding3D(); }
+
+void DistanceVoxelMap::exactDistances3D(std::vector<Vector3f>& points) { voxelizeAndTransform(points); }
 
 void DistanceVoxelMap::fill_pba_uninit() { fill_pba_uninit(*this); }
 

@@ -68,6 +68,12 @@ class DistanceVoxelMap : public GpuVoxelsMap {
                          uint32_t m2_blocksize = PBA_DEFAULT_M2_BLOCK_SIZE,
                          uint32_t m3_blocksize = PBA_DEFAULT_M3_BLOCK_SIZE, bool detailtimer = false);
 
+  // gvx extension (no reference counterpart): clearMap + insertPointCloud +
+  // parallelBanding3D in one call, the same result, without writing the
+  // inserted map first (the fastest form for a per-frame sensor loop).
+  void voxelizeAndTransform(const std::vector<Vector3f>& points);
+  void voxelizeAndTransform(const Vector3f* d_points, uint32_t size);
+
   // The reference's other two EDTs, kept for source compatibility.  Both
   // compute the exact transform of parallelBanding3D: jumpFlood3D
   // (DistanceVoxelMap.hpp:141-206) is an approximation in the reference, and

@@ -303,6 +303,15 @@ static void other_edt_entry_points() {
         same = same && b.getSquaredObstacleDistance(x, y, z) == d && c.getSquaredObstacleDistance(x, y, z) == d;
       }
   CHECK(same, "jumpFlood3D / exactDistances3D: parallelBanding3D's squared distances");
+  voxelmap::DistanceVoxelMap e(dims, 1.f);
+  e.insertPointCloud(std::vector<Vector3f>(1, Vector3f(3.5f, 3.5f, 3.5f)), eBVM_OCCUPIED);  // replaced below
+  e.voxelizeAndTransform(pts);
+  std::vector<uint32_t> all(a.getVoxelMapSize());
+  for (uint32_t i = 0; i < all.size(); ++i) all[i] = i;
+  std::vector<int32_t> da, de;
+  a.getSquaredDistancesToHost(all, da);
+  e.getSquaredDistancesToHost(all, de);
+  CHECK(da == de, "voxelizeAndTransform: clearMap + insertPointCloud + parallelBanding3D");
   a.fill_pba_uninit();
   CHECK(a.getSquaredObstacleDistance(3, 3, 3) == INT32_MAX, "fill_pba_uninit: no sites left");
 }
