@@ -357,6 +357,9 @@ def section_c4(hbm_peak):
         d = dvm.trilinear(pts, with_grad=False)
         return dvm.trilinear_backward(pts, gout)
 
+    gvx.set_query_config(256, 16)
+    ms_fb_default = _time(fwd_bwd, 20)
+    qcfg = dvm.autotune_queries(pts, with_grad=False, force=True)
     ms_fb = _time(fwd_bwd, 20)
     p = pts.clone().requires_grad_(True)
 
@@ -387,6 +390,8 @@ def section_c4(hbm_peak):
     bytes_fb = 48 + 60
     return {"workload": "256^3 map; 1M points trilinear fwd+bwd; 512 x 64 waypoints x 56 spheres hinge cost + adjoint",
             "trilinear_fwd_bwd_ms": round(ms_fb, 4), "trilinear_queries_with_grad_per_s": round(n / ms_fb * 1e3, 1),
+            "query_launch_shape": {"threads": qcfg["threads"], "blocks_per_sm": qcfg["blocks_per_sm"],
+                                   "fwd_bwd_ms_at_256x16": round(ms_fb_default, 4)},
             "trilinear_achieved_gbs": round(bytes_fb * n / (ms_fb / 1e3) / 1e9, 1),
             "autograd_step_ms": round(ms_ag, 4),
             "traj_fwd_bwd_ms": round(ms_tr, 4),

@@ -18,9 +18,6 @@
 
 namespace gvx {
 
-cudaError_t launch_trilinear(const gvx_dvm* m, const float* d_xyz, uint64_t n, float* d_dist, float* d_grad, cudaStream_t s);
-cudaError_t launch_trilinear_bwd(const gvx_dvm* m, const float* d_xyz, uint64_t n, const float* d_gout, float* d_gxyz,
-                                 cudaStream_t s);
 cudaError_t launch_sphere_clearance(const gvx_dvm* m, const gvx_arm& arm, const float* d_q, uint64_t n_cfg, float* d_out,
                                     cudaStream_t s);
 cudaError_t launch_traj_cost(const gvx_dvm* m, const gvx_arm& arm, const float* d_q, uint64_t n_traj, uint32_t n_wp,

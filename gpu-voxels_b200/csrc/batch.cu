@@ -282,8 +282,10 @@ gvx_status gvx_batch_query_trilinear(gvx_batch* b, const float* d_xyz, const uin
   if (b == nullptr || (n > 0 && (d_xyz == nullptr || d_map == nullptr || d_dist == nullptr)))
     return fail(GVX_ERR_INVALID_ARG, "null argument");
   if (n == 0) return GVX_OK;
-  const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms() * 16);
-  batch_trilinear_kernel<<<blocks, 256, 0, as_stream(stream)>>>(b->d_table, d_xyz, d_map, n, d_dist, d_grad);
+  const QueryConfig q = query_config();
+  const unsigned blocks = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>((n + q.threads - 1) / q.threads, (uint64_t)sms() * q.blocks_per_sm));
+  batch_trilinear_kernel<<<blocks, q.threads, 0, as_stream(stream)>>>(b->d_table, d_xyz, d_map, n, d_dist, d_grad);
   return cuda_status(cudaGetLastError(), "batch trilinear");
 }
 

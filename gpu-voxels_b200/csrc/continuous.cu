@@ -264,14 +264,16 @@ MapView view(const gvx_dvm* m) { return MapView{m->d_vox, (int)m->dims.x, (int)m
 
 cudaError_t launch_trilinear(const gvx_dvm* m, const float* d_xyz, uint64_t n, float* d_dist, float* d_grad, cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  trilinear_kernel<<<blocks_for(n, 256, 16), 256, 0, s>>>(view(m), d_xyz, n, d_dist, d_grad);
+  const QueryConfig q = query_config();
+  trilinear_kernel<<<blocks_for(n, q.threads, q.blocks_per_sm), q.threads, 0, s>>>(view(m), d_xyz, n, d_dist, d_grad);
   return cudaGetLastError();
 }
 
 cudaError_t launch_trilinear_bwd(const gvx_dvm* m, const float* d_xyz, uint64_t n, const float* d_gout, float* d_gxyz,
                                  cudaStream_t s) {
   if (n == 0) return cudaSuccess;
-  trilinear_bwd_kernel<<<blocks_for(n, 256, 16), 256, 0, s>>>(view(m), d_xyz, n, d_gout, d_gxyz);
+  const QueryConfig q = query_config();
+  trilinear_bwd_kernel<<<blocks_for(n, q.threads, q.blocks_per_sm), q.threads, 0, s>>>(view(m), d_xyz, n, d_gout, d_gxyz);
   return cudaGetLastError();
 }
 

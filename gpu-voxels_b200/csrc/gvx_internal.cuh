@@ -170,6 +170,19 @@ cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t s
                                 const EdtConfig& cfg = EdtConfig{});
 cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems& items, const float* d_xyz,
                                       const uint64_t* d_offsets, uint64_t n_total, cudaStream_t s, int rows = 0);
+// Launch shape of the trilinear query kernels (every shape gives the same
+// results): threads per block and the grid cap in blocks per SM.  Per process,
+// picked by gvx_query_autotune or set with gvx_set_query_config.
+struct QueryConfig {
+  int threads = 256;
+  int blocks_per_sm = 16;
+};
+QueryConfig query_config();
+void set_query_config(const QueryConfig& c);
+// Trilinear distance queries and their adjoint (continuous.cu), in that shape.
+cudaError_t launch_trilinear(const gvx_dvm* m, const float* d_xyz, uint64_t n, float* d_dist, float* d_grad, cudaStream_t s);
+cudaError_t launch_trilinear_bwd(const gvx_dvm* m, const float* d_xyz, uint64_t n, const float* d_gout, float* d_gxyz,
+                                 cudaStream_t s);
 // Autotuner cache (tune.cu): the best configuration recorded for `key` on the
 // current device, from memory or the file named by GVX_TUNE_CACHE.
 bool tune_lookup(const std::string& key, EdtConfig* cfg, float* ms);

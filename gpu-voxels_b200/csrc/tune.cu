@@ -54,6 +54,19 @@ std::string tune_device_name() {
   return name + "_sm" + std::to_string(p.multiProcessorCount);
 }
 
+QueryConfig g_query;  // guarded by g_tune_mutex
+std::map<std::string, std::pair<QueryConfig, float>> g_query_cache;
+
+QueryConfig query_config() {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  return g_query;
+}
+
+void set_query_config(const QueryConfig& c) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_query = c;
+}
+
 bool tune_lookup(const std::string& key, EdtConfig* cfg, float* ms) {
   std::lock_guard<std::mutex> lock(g_tune_mutex);
   load_file_locked();
@@ -92,6 +105,75 @@ std::string map_key(const gvx_dims& d) {
 }  // namespace
 
 extern "C" {
+
+gvx_status gvx_set_query_config(const gvx_query_config* cfg) {
+  if (cfg == nullptr) return tune_fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!(cfg->threads == 64 || cfg->threads == 128 || cfg->threads == 256 || cfg->threads == 512) ||
+      cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 64)
+    return tune_fail(GVX_ERR_INVALID_ARG, "threads must be 64, 128, 256 or 512 and blocks_per_sm in [1, 64]");
+  set_query_config(QueryConfig{(int)cfg->threads, (int)cfg->blocks_per_sm});
+  return GVX_OK;
+}
+
+gvx_status gvx_query_autotune(const gvx_dvm* m, const float* d_xyz, uint64_t n, float* d_dist, float* d_grad, int force,
+                              gvx_query_config* out, gvx_stream stream) {
+  if (m == nullptr || n == 0 || d_xyz == nullptr || d_dist == nullptr)
+    return tune_fail(GVX_ERR_INVALID_ARG, "need a map, points and a distance buffer");
+  const std::string key = tune_device_name() + "|query";
+  float best_ms = 0.f;
+  QueryConfig best;
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_query_cache.find(key);
+    if (!force && it != g_query_cache.end()) {
+      best = it->second.first;
+      best_ms = it->second.second;
+      cached = true;
+    }
+  }
+  if (!cached) {
+    cudaStream_t s = as_stream(stream);
+    cudaEvent_t a, b;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
+      return tune_fail(GVX_ERR_CUDA, "query autotune: event creation failed");
+    const QueryConfig before = query_config();
+    best_ms = -1.f;
+    cudaError_t e = cudaSuccess;
+    for (int threads : {64, 128, 256, 512}) {
+      for (int cap : {8, 16, 32}) {
+        set_query_config(QueryConfig{threads, cap});
+        float total = 0.f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {  // the first is a warm-up
+          e = cudaEventRecord(a, s);
+          if (e == cudaSuccess) e = launch_trilinear(m, d_xyz, n, d_dist, d_grad, s);
+          if (e == cudaSuccess) e = cudaEventRecord(b, s);
+          if (e == cudaSuccess) e = cudaEventSynchronize(b);
+          float ms = 0.f;
+          if (e == cudaSuccess) cudaEventElapsedTime(&ms, a, b);
+          if (rep > 0) total += ms;
+        }
+        if (e != cudaSuccess) break;
+        if (best_ms < 0.f || total / 3 < best_ms) {
+          best_ms = total / 3;
+          best = QueryConfig{threads, cap};
+        }
+      }
+      if (e != cudaSuccess) break;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (e != cudaSuccess) {
+      set_query_config(before);
+      return cuda_status(e, "query autotune");
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_query_cache[key] = {best, best_ms};
+  }
+  set_query_config(best);
+  if (out) *out = gvx_query_config{(uint32_t)best.threads, (uint32_t)best.blocks_per_sm, best_ms};
+  return GVX_OK;
+}
 
 gvx_status gvx_dvm_set_edt_config(gvx_dvm* m, const gvx_edt_config* cfg) {
   if (m == nullptr || cfg == nullptr) return tune_fail(GVX_ERR_INVALID_ARG, "null argument");

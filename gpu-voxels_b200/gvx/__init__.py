@@ -18,6 +18,7 @@ from .maps import (  # noqa: F401
     extract_given_distances,
     lists_collide_map,
     make_arm,
+    set_query_config,
 )
 
 __all__ = [
@@ -31,6 +32,7 @@ __all__ = [
     "lists_collide_map",
     "extract_given_distances",
     "make_arm",
+    "set_query_config",
     "BIT_VECTOR_LENGTH",
     "eBVM_FREE",
     "eBVM_OCCUPIED",

@@ -37,6 +37,10 @@ class EdtConfig(ctypes.Structure):
     _fields_ = [("rows", ctypes.c_uint32), ("fused", ctypes.c_uint32), ("ms", ctypes.c_float)]
 
 
+class QueryConfig(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32), ("ms", ctypes.c_float)]
+
+
 class Dims(ctypes.Structure):
     _fields_ = [("x", ctypes.c_uint32), ("y", ctypes.c_uint32), ("z", ctypes.c_uint32)]
 
@@ -88,6 +92,8 @@ PROTOTYPES = {
     "gvx_dvm_sqdist_map": [_vp, _vp, _vp],
     "gvx_query_trilinear": [_vp, _vp, _u64, _vp, _vp, _vp],
     "gvx_query_trilinear_bwd": [_vp, _vp, _u64, _vp, _vp, _vp],
+    "gvx_query_autotune": [_vp, _vp, _u64, _vp, _vp, ctypes.c_int, ctypes.POINTER(QueryConfig), _vp],
+    "gvx_set_query_config": [ctypes.POINTER(QueryConfig)],
     "gvx_sphere_clearance": [_vp, ctypes.POINTER(Arm), _vp, _u64, _vp, _vp],
     "gvx_traj_cost": [_vp, ctypes.POINTER(Arm), _vp, _u64, _u32, _f, _vp, _vp],
     "gvx_traj_cost_bwd": [_vp, ctypes.POINTER(Arm), _vp, _u64, _u32, _f, _vp, _vp, _vp],

@@ -198,6 +198,19 @@ class DistanceVoxelMap:
         call("gvx_query_trilinear", self._h, _ptr(p), n, _ptr(dist), _ptr(grad), _stream())
         return (dist, grad) if with_grad else dist
 
+    def autotune_queries(self, points: torch.Tensor, with_grad: bool = True, force: bool = False) -> dict:
+        """Pick the fastest launch shape of the trilinear query kernels, timed on
+        `points` against this map (cached per device for the process); applies
+        to every map's queries and to the batched query."""
+        p = _dev_points(points)
+        n = p.shape[0]
+        dist = torch.empty(n, dtype=torch.float32, device="cuda")
+        grad = torch.empty(n, 3, dtype=torch.float32, device="cuda") if with_grad else None
+        c = _abi.QueryConfig()
+        call("gvx_query_autotune", self._h, _ptr(p), n, _ptr(dist), _ptr(grad), int(bool(force)), ctypes.byref(c),
+             _stream())
+        return {"threads": c.threads, "blocks_per_sm": c.blocks_per_sm, "ms": c.ms}
+
     def trilinear_backward(self, points: torch.Tensor, grad_dist: torch.Tensor) -> torch.Tensor:
         p = _dev_points(points)
         g = grad_dist.to(device="cuda", dtype=torch.float32).contiguous()
@@ -519,6 +532,13 @@ class BitVectorVoxelList:
         call("gvx_blist_collide_type_mask_bvm", self._h, other.handle, _ptr(mask), _offset(offset), _ptr(self._count),
              _stream())
         return int(self._count.item())
+
+
+def set_query_config(threads: int = 256, blocks_per_sm: int = 16) -> None:
+    """Fix the launch shape of the trilinear query kernels (threads 64, 128,
+    256 or 512; blocks_per_sm 1..64).  Results do not depend on it."""
+    c = _abi.QueryConfig(threads, blocks_per_sm, 0.0)
+    call("gvx_set_query_config", ctypes.byref(c))
 
 
 def lists_collide_map(ids: torch.Tensor, voxels: torch.Tensor, offsets: torch.Tensor, bvm: BitVectorVoxelMap,

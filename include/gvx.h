@@ -173,6 +173,25 @@ GVX_API gvx_status gvx_query_trilinear(const gvx_dvm *m, const float *d_xyz, uin
 /* Adjoint: d_grad_xyz[i] = d_grad_dist[i] * grad d(x_i); recomputes the gathers. */
 GVX_API gvx_status gvx_query_trilinear_bwd(const gvx_dvm *m, const float *d_xyz, uint64_t n, const float *d_grad_dist,
                                    float *d_grad_xyz, gvx_stream stream);
+/* Launch shape of the trilinear query kernels (gvx_query_trilinear, its
+ * adjoint and gvx_batch_query_trilinear): threads per block (64, 128, 256 or
+ * 512) and the grid cap in blocks per SM (1..64; the kernels stride over the
+ * points).  One setting per process; default 256 x 16.  Every shape gives
+ * bit-identical results, only the speed changes. */
+typedef struct {
+  uint32_t threads;
+  uint32_t blocks_per_sm;
+  float ms;
+} gvx_query_config;
+/* Project-written query autotuner: times gvx_query_trilinear on the caller's
+ * points and output buffers (which it overwrites) for threads {64, 128, 256,
+ * 512} x caps {8, 16, 32} blocks per SM, sets the fastest and returns it in
+ * *out (optional).  The choice is cached per device for the process; force = 1
+ * re-times.  Synchronises the stream.  d_grad may be NULL. */
+GVX_API gvx_status gvx_query_autotune(const gvx_dvm *m, const float *d_xyz, uint64_t n, float *d_dist, float *d_grad,
+                                      int force, gvx_query_config *out, gvx_stream stream);
+/* Sets the shape explicitly (ms is ignored); GVX_ERR_INVALID_ARG outside the ranges above. */
+GVX_API gvx_status gvx_set_query_config(const gvx_query_config *cfg);
 
 /* Serial-chain arm in the reference's DH convention
  * (KinematicLink::convertDHtoM, GV/robot/dh_robot/KinematicLink.cu:24-79):

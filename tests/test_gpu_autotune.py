@@ -97,3 +97,37 @@ def test_batch_autotune_restores_maps_and_stays_exact():
         oracle.dvm_insert(want, dims, 0.01, p)
         oracle.pba(want, dims)
         assert np.array_equal(to_u32(maps[k].data()), want), dims
+
+
+def test_query_launch_shapes_are_bit_identical_and_autotune_picks_one():
+    dims = (90, 70, 50)
+    pts = _scene(dims, 7)
+    m = gvx.DistanceVoxelMap(dims, 0.01)
+    m.insertPointCloud(torch.as_tensor(pts).cuda())
+    m.parallelBanding3D()
+    rng = np.random.default_rng(3)
+    q = torch.as_tensor(((0.5 + rng.random((70_001, 3)) * (np.asarray(dims) - 1)) * 0.01).astype(np.float32)).cuda()
+    up = torch.as_tensor(rng.standard_normal(q.shape[0]).astype(np.float32)).cuda()
+    b = Batch([m])
+    mi = torch.zeros(q.shape[0], dtype=torch.int32, device="cuda")
+    gvx.set_query_config(256, 16)
+    d0, g0 = m.trilinear(q)
+    a0 = m.trilinear_backward(q, up)
+    bd0, bg0 = b.query(q, mi)
+    for threads in (64, 128, 256, 512):
+        for cap in (1, 8, 32):
+            gvx.set_query_config(threads, cap)
+            d, g = m.trilinear(q)
+            assert torch.equal(d, d0) and torch.equal(g, g0), (threads, cap)
+            assert torch.equal(m.trilinear_backward(q, up), a0), (threads, cap)
+            bd, bg = b.query(q, mi)
+            assert torch.equal(bd, bd0) and torch.equal(bg, bg0), (threads, cap)
+    for bad in ((96, 16), (256, 0), (256, 65)):
+        with pytest.raises(gvx.GvxError):
+            gvx.set_query_config(*bad)
+    cfg = m.autotune_queries(q, force=True)
+    assert cfg["threads"] in (64, 128, 256, 512) and cfg["blocks_per_sm"] in (8, 16, 32) and cfg["ms"] > 0
+    assert m.autotune_queries(q) == cfg  # cached for the process
+    d, g = m.trilinear(q)
+    assert torch.equal(d, d0) and torch.equal(g, g0)
+    gvx.set_query_config(256, 16)
