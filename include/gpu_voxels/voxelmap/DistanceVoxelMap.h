@@ -8,6 +8,11 @@
 
 #include <vector>
 
+#if __has_include(<thrust/device_ptr.h>)
+#include <thrust/device_ptr.h>
+#define GVX_HAVE_THRUST_DEVICE_PTR 1
+#endif
+
 #include "../GpuVoxelsMap.h"
 #include "ProbVoxelMap.h"
 
@@ -116,6 +121,22 @@ class DistanceVoxelMap : public GpuVoxelsMap {
   void getSquaredDistances(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, int32_t* dev_output);
   void getDistances(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, int32_t* dev_output);
   void gatherVoxelsByIndex(const uint32_t* dev_indices_begin, const uint32_t* dev_indices_end, Voxel* dev_output);
+#ifdef GVX_HAVE_THRUST_DEVICE_PTR
+  // The thrust::device_ptr forms the reference declares
+  // (GV/voxelmap/DistanceVoxelMap.h:81,84; GV/voxelmap/TemplateVoxelMap.h:111).
+  void getSquaredDistances(thrust::device_ptr<uint32_t> dev_indices_begin, thrust::device_ptr<uint32_t> dev_indices_end,
+                           thrust::device_ptr<int32_t> dev_output) {
+    getSquaredDistances(dev_indices_begin.get(), dev_indices_end.get(), dev_output.get());
+  }
+  void getDistances(thrust::device_ptr<uint32_t> dev_indices_begin, thrust::device_ptr<uint32_t> dev_indices_end,
+                    thrust::device_ptr<int32_t> dev_output) {
+    getDistances(dev_indices_begin.get(), dev_indices_end.get(), dev_output.get());
+  }
+  void gatherVoxelsByIndex(thrust::device_ptr<uint32_t> dev_indices_begin, thrust::device_ptr<uint32_t> dev_indices_end,
+                           thrust::device_ptr<Voxel> dev_output_begin) {
+    gatherVoxelsByIndex(dev_indices_begin.get(), dev_indices_end.get(), dev_output_begin.get());
+  }
+#endif
   // Host vectors; blocking (GV/voxelmap/DistanceVoxelMap.hpp:726-739,771-784).
   void getSquaredDistancesToHost(std::vector<uint32_t>& indices, std::vector<int32_t>& output);
   void getDistancesToHost(std::vector<uint32_t>& indices, std::vector<int32_t>& output);

@@ -62,7 +62,9 @@ static void distance_extraction() {
     cudaMalloc(&d_idx, idx.size() * 4);
     cudaMalloc(&d_out, idx.size() * 4);
     cudaMemcpy(d_idx, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice);
-    map.gatherVoxelsByIndex(d_idx, d_idx + idx.size(), d_out);
+    // the thrust::device_ptr form, as the reference's test calls it
+    map.gatherVoxelsByIndex(thrust::device_ptr<uint32_t>(d_idx), thrust::device_ptr<uint32_t>(d_idx + idx.size()),
+                            thrust::device_ptr<DistanceVoxel>(d_out));
     cudaMemcpy(gathered.data(), d_out, idx.size() * 4, cudaMemcpyDeviceToHost);
     cudaFree(d_idx);
     cudaFree(d_out);
@@ -85,6 +87,29 @@ static void distance_extraction() {
   }
   CHECK(zero, "distance_extraction: zero distance at obstacles");
   CHECK(differ, "distance_extraction: neighbour distance differs");
+  // device-pointer queries (raw and thrust::device_ptr) agree with the host form
+  std::vector<int32_t> sq_host, sq_raw(nb.size()), sq_thrust(nb.size()), d_host, d_thrust(nb.size());
+  map.getSquaredDistancesToHost(nb, sq_host);
+  map.getDistancesToHost(nb, d_host);
+  {
+    uint32_t* d_idx = nullptr;
+    int32_t* d_out = nullptr;
+    cudaMalloc(&d_idx, nb.size() * 4);
+    cudaMalloc(&d_out, nb.size() * 4);
+    cudaMemcpy(d_idx, nb.data(), nb.size() * 4, cudaMemcpyHostToDevice);
+    map.getSquaredDistances(d_idx, d_idx + nb.size(), d_out);
+    cudaMemcpy(sq_raw.data(), d_out, nb.size() * 4, cudaMemcpyDeviceToHost);
+    thrust::device_ptr<uint32_t> b(d_idx), e(d_idx + nb.size());
+    thrust::device_ptr<int32_t> o(d_out);
+    map.getSquaredDistances(b, e, o);
+    cudaMemcpy(sq_thrust.data(), d_out, nb.size() * 4, cudaMemcpyDeviceToHost);
+    map.getDistances(b, e, o);
+    cudaMemcpy(d_thrust.data(), d_out, nb.size() * 4, cudaMemcpyDeviceToHost);
+    cudaFree(d_idx);
+    cudaFree(d_out);
+  }
+  CHECK(sq_raw == sq_host && sq_thrust == sq_host && d_thrust == d_host,
+        "distance_extraction: device-pointer queries equal the host queries");
 }
 
 static void distance_correctness() {
