@@ -45,6 +45,14 @@ def _dev_u32(ids) -> torch.Tensor:
     return t.to("cuda").contiguous()
 
 
+def _check_clone(dst, src) -> None:
+    """TemplateVoxelMap::clone (GV/voxelmap/TemplateVoxelMap.hpp:1101-1120) copies
+    only between maps of equal dims and voxel side length."""
+    if dst.dims != src.dims or np.float32(dst.voxel_side_length) != np.float32(src.voxel_side_length):
+        raise ValueError(f"clone: dims {src.dims} / side {src.voxel_side_length} differ from "
+                         f"{dst.dims} / {dst.voxel_side_length}")
+
+
 def _offset(offset: Sequence[int]) -> ctypes.Array:
     o = (ctypes.c_int32 * 3)(*[int(v) for v in offset])
     return o
@@ -82,6 +90,12 @@ class DistanceVoxelMap:
     @property
     def size(self) -> int:
         return self.dims[0] * self.dims[1] * self.dims[2]
+
+    def clone(self, other: "DistanceVoxelMap") -> None:
+        """Copy `other`'s voxels (equal dims and side length; stream-ordered)."""
+        _check_clone(self, other)
+        if other is not self:
+            self.data().copy_(other.data())
 
     def data(self) -> torch.Tensor:
         """Borrowed int32 CUDA view of the voxel buffer (bit pattern = uint32
@@ -299,6 +313,12 @@ class ProbVoxelMap:
     def size(self) -> int:
         return self.dims[0] * self.dims[1] * self.dims[2]
 
+    def clone(self, other: "ProbVoxelMap") -> None:
+        """Copy `other`'s occupancies (equal dims and side length; stream-ordered)."""
+        _check_clone(self, other)
+        if other is not self:
+            self.data().copy_(other.data())
+
     def data(self) -> torch.Tensor:
         """Borrowed int8 CUDA view of the occupancies."""
         d, s, p = Dims(), ctypes.c_float(), ctypes.c_void_p()
@@ -347,6 +367,12 @@ class BitVectorVoxelMap:
     @property
     def size(self) -> int:
         return self.dims[0] * self.dims[1] * self.dims[2]
+
+    def clone(self, other: "BitVectorVoxelMap") -> None:
+        """Copy `other`'s bit vectors (equal dims and side length; stream-ordered)."""
+        _check_clone(self, other)
+        if other is not self:
+            self.voxels().copy_(other.voxels())
 
     def voxels(self) -> torch.Tensor:
         """Borrowed uint8 view of the 32-byte voxels (size * 32 bytes)."""

@@ -55,6 +55,22 @@ struct DeviceArray {
   ~DeviceArray() { if (p) cudaFree(p); }
 };
 
+// TemplateVoxelMap::clone (GV/voxelmap/TemplateVoxelMap.hpp:1101-1120).
+void clone_voxels(GpuVoxelsMap& self, const GpuVoxelsMap& other, void* dst, const void* src, size_t bytes) {
+  if (self.getVoxelSideLength() != other.getVoxelSideLength() || !(self.getDimensions() == other.getDimensions())) {
+    std::fprintf(stderr, "gpu_voxels: clone: map dimensions or voxel side length differ; not cloned\n");
+    return;
+  }
+  if (&self == &other) return;
+  std::unique_lock<std::recursive_timed_mutex> a(self.mutexRef(), std::defer_lock);
+  std::unique_lock<std::recursive_timed_mutex> b(other.mutexRef(), std::defer_lock);
+  std::lock(a, b);
+  cudaDeviceSynchronize();
+  if (cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToDevice) != cudaSuccess)
+    std::fprintf(stderr, "gpu_voxels: clone: device copy failed\n");
+  cudaDeviceSynchronize();
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -191,6 +207,12 @@ bool ProbVoxelMap::writeToDisk(const std::string path) {
 bool ProbVoxelMap::readFromDisk(const std::string path) {
   lock_guard g(m_mutex);
   return ok(gvx_pvm_read_from_disk(m_handle, path.c_str()), "readFromDisk");
+}
+
+void ProbVoxelMap::clone(const ProbVoxelMap& other) {
+  int8_t* src = nullptr;
+  gvx_pvm_info(other.handle(), nullptr, nullptr, &src);
+  clone_voxels(*this, other, getDeviceDataPtr(), src, getVoxelMapSize());
 }
 
 Probability* ProbVoxelMap::getDeviceDataPtr() {
@@ -375,6 +397,12 @@ DistanceVoxel::pba_dist_t DistanceVoxelMap::getObstacleDistance(uint32_t x, uint
 
 DistanceVoxel::pba_dist_t DistanceVoxelMap::getObstacleDistance(const Vector3ui& p) { return getObstacleDistance(p.x, p.y, p.z); }
 
+void DistanceVoxelMap::clone(const DistanceVoxelMap& other) {
+  uint32_t* src = nullptr;
+  gvx_dvm_info(other.handle(), nullptr, nullptr, &src);
+  clone_voxels(*this, other, getDeviceDataPtr(), src, getVoxelMapSize() * sizeof(DistanceVoxel));
+}
+
 DistanceVoxel* DistanceVoxelMap::getDeviceDataPtr() {
   uint32_t* p = nullptr;
   gvx_dvm_info(m_handle, nullptr, nullptr, &p);
@@ -548,6 +576,13 @@ uint8_t* BitVoxelMap<length>::getDeviceDataPtr() {
   uint8_t* p = nullptr;
   gvx_bvm_info(m_handle, nullptr, nullptr, &p);
   return p;
+}
+
+template <size_t length>
+void BitVoxelMap<length>::clone(const BitVoxelMap& other) {
+  uint8_t* src = nullptr;
+  gvx_bvm_info(other.handle(), nullptr, nullptr, &src);
+  clone_voxels(*this, other, getDeviceDataPtr(), src, getVoxelMapSize() * 32);
 }
 
 template class BitVoxelMap<BIT_VECTOR_LENGTH>;
@@ -819,6 +854,14 @@ bool GpuVoxels::addMap(const MapType map_type, const std::string& map_name) {
   }
   m_managed_maps[map_name] = map;
   return true;
+}
+
+bool GpuVoxels::visualizeMap(const std::string& map_name, const bool /*force_repaint*/) {
+  if (!getMap(map_name)) {
+    std::fprintf(stderr, "gpu_voxels: Map with name '%s' not found.\n", map_name.c_str());
+    return false;
+  }
+  return false;  // no viewer
 }
 
 bool GpuVoxels::delMap(const std::string& map_name) {

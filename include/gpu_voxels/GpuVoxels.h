@@ -41,6 +41,10 @@ class GpuVoxels {
   void getDimensions(uint32_t& dim_x, uint32_t& dim_y, uint32_t& dim_z) const;
   void getDimensions(Vector3ui& dim) const;
   void getVoxelSideLength(float& voxel_side_length) const;
+  // visualizeMap (GV/GpuVoxels.cpp:585-594) hands the map to the separate
+  // shared-memory viewer program, which this library does not provide: false
+  // always, with the reference's message for an unknown map name.
+  bool visualizeMap(const std::string& map_name, const bool force_repaint = true);
 
  private:
   GpuVoxels();

@@ -67,6 +67,11 @@ class BitVoxelMap : public GpuVoxelsMap {
       const std::vector<BitVector<length> >& collision_masks = std::vector<BitVector<length> >(),
       BitVector<length>* colliding_meanings = NULL) override;
 
+  // TemplateVoxelMap::clone (GV/voxelmap/TemplateVoxelMap.hpp:1101-1120): copies
+  // the other map's voxels when dims and voxel side length match; otherwise an
+  // error message and no change.  Blocking.
+  void clone(const BitVoxelMap& other);
+
   // Raw 32-byte voxels on the device.
   uint8_t* getDeviceDataPtr();
   size_t getVoxelMapSize() const { return (size_t)m_dim.x * m_dim.y * m_dim.z; }

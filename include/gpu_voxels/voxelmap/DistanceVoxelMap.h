@@ -145,6 +145,11 @@ class DistanceVoxelMap : public GpuVoxelsMap {
   DistanceVoxel::pba_dist_t getObstacleDistance(const Vector3ui& pos);
   DistanceVoxel::pba_dist_t getObstacleDistance(uint32_t x, uint32_t y, uint32_t z);
 
+  // TemplateVoxelMap::clone (GV/voxelmap/TemplateVoxelMap.hpp:1101-1120): copies
+  // the other map's voxels when dims and voxel side length match; otherwise an
+  // error message and no change.  Blocking.
+  void clone(const DistanceVoxelMap& other);
+
   Voxel* getDeviceDataPtr();
   const Voxel* getConstDeviceDataPtr() const;
   size_t getVoxelMapSize() const { return (size_t)m_dim.x * m_dim.y * m_dim.z; }

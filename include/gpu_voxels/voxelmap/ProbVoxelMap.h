@@ -34,6 +34,11 @@ class ProbVoxelMap : public GpuVoxelsMap {
   bool writeToDisk(const std::string path) override;
   bool readFromDisk(const std::string path) override;
 
+  // TemplateVoxelMap::clone (GV/voxelmap/TemplateVoxelMap.hpp:1101-1120): copies
+  // the other map's voxels when dims and voxel side length match; otherwise an
+  // error message and no change.  Blocking.
+  void clone(const ProbVoxelMap& other);
+
   Probability* getDeviceDataPtr();
   size_t getVoxelMapSize() const { return (size_t)m_dim.x * m_dim.y * m_dim.z; }
   gvx_pvm* handle() const { return m_handle; }

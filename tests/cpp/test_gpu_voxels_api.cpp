@@ -341,6 +341,40 @@ static void other_edt_entry_points() {
   CHECK(a.getSquaredObstacleDistance(3, 3, 3) == INT32_MAX, "fill_pba_uninit: no sites left");
 }
 
+// clone (TemplateVoxelMap.hpp:1101-1120) of each map type; a map of other dims is left alone;
+// visualizeMap has no viewer to hand to.
+static void clone_maps() {
+  const Vector3ui dims(30, 26, 22);
+  std::vector<Vector3f> pts = equidistant(40, dims, 1.f);
+  voxelmap::DistanceVoxelMap a(dims, 1.f), b(dims, 1.f), other(Vector3ui(30, 26, 21), 1.f);
+  a.insertPointCloud(pts, eBVM_OCCUPIED);
+  a.parallelBanding3D();
+  b.clone(a);
+  other.clone(a);  // message, no change
+  std::vector<uint32_t> all(a.getVoxelMapSize());
+  for (uint32_t i = 0; i < all.size(); ++i) all[i] = i;
+  std::vector<int32_t> da, db;
+  a.getSquaredDistancesToHost(all, da);
+  b.getSquaredDistancesToHost(all, db);
+  CHECK(da == db, "clone: DistanceVoxelMap copy has the same distances");
+  CHECK(other.getSquaredObstacleDistance(0, 0, 0) == INT32_MAX, "clone: other dims refused, map unchanged");
+  BitVectorVoxelMap ba(dims, 1.f, MT_BITVECTOR_VOXELMAP), bb(dims, 1.f, MT_BITVECTOR_VOXELMAP),
+      bs(dims, 0.5f, MT_BITVECTOR_VOXELMAP);
+  ba.insertPointCloud(pts, eBVM_OCCUPIED);
+  bb.clone(ba);
+  bs.clone(ba);  // other side length: refused
+  CHECK(bb.collideWith(&ba) == pts.size() && bs.collideWith(&ba) == 0, "clone: BitVectorVoxelMap");
+  voxelmap::ProbVoxelMap pa(dims, 1.f), pb(dims, 1.f);
+  pa.insertPointCloud(pts, eBVM_OCCUPIED);
+  pb.clone(pa);
+  std::vector<int8_t> ha(pa.getVoxelMapSize()), hb(pb.getVoxelMapSize());
+  cudaMemcpy(ha.data(), pa.getDeviceDataPtr(), ha.size(), cudaMemcpyDeviceToHost);
+  cudaMemcpy(hb.data(), pb.getDeviceDataPtr(), hb.size(), cudaMemcpyDeviceToHost);
+  CHECK(ha == hb, "clone: ProbVoxelMap");
+  GpuVoxelsSharedPtr gvl = GpuVoxels::getInstance();
+  CHECK(!gvl->visualizeMap("no such map"), "visualizeMap: unknown map -> false");
+}
+
 // insertCoordinateList / copyCoordsToHost round trip; out-of-map coordinates are dropped.
 static void list_coordinates() {
   BitVectorVoxelList list(Vector3ui(50, 40, 30), 0.01f, MT_BITVECTOR_VOXELLIST);
@@ -357,6 +391,7 @@ static void list_coordinates() {
 int main() {
   GpuVoxels::getInstance();
   list_coordinates();
+  clone_maps();
   other_edt_entry_points();
   selfcollision_metapointcloud();
   distance_consumers();

@@ -109,3 +109,26 @@ def test_list_shift_and_clear_match_oracle():
     b[237 >> 3] = 1 << (237 & 7)
     oracle.bvm_clear_bits(vox, b)
     assert np.array_equal(lst.voxels().cpu().numpy().reshape(-1), vox)
+
+
+def test_clone_every_map_type_and_refusals():
+    """TemplateVoxelMap::clone (GV/voxelmap/TemplateVoxelMap.hpp:1101-1120)."""
+    dims = (31, 27, 19)
+    rng = np.random.default_rng(11)
+    pts = torch.as_tensor((rng.random((3000, 3)) * np.asarray(dims) * 0.05).astype(np.float32)).cuda()
+    a, b = gvx.DistanceVoxelMap(dims, 0.05), gvx.DistanceVoxelMap(dims, 0.05)
+    a.voxelize_edt(pts)
+    b.clone(a)
+    assert torch.equal(a.data(), b.data())
+    with pytest.raises(ValueError):
+        gvx.DistanceVoxelMap((31, 27, 18), 0.05).clone(a)
+    with pytest.raises(ValueError):
+        gvx.DistanceVoxelMap(dims, 0.04).clone(a)
+    ba, bb = gvx.BitVectorVoxelMap(dims, 0.05), gvx.BitVectorVoxelMap(dims, 0.05)
+    ba.insertPointCloud(pts, 9)
+    bb.clone(ba)
+    assert torch.equal(ba.voxels(), bb.voxels())
+    pa, pb = gvx.ProbVoxelMap(dims, 0.05), gvx.ProbVoxelMap(dims, 0.05)
+    pa.insertPointCloud(pts)
+    pb.clone(pa)
+    assert torch.equal(pa.data(), pb.data())
