@@ -80,8 +80,8 @@ constexpr int kZBitsSmemMax = kZWarps * 2 * z_bits_words(1024) * 4;
 constexpr int kZWarpWords = 2 * kZChunk * 32 + 2 * kZRing * 32;
 
 // Words of the EDT workspace's counter area (Z slice counters, queue head,
-// error word, padded to 32).
-__host__ __device__ __forceinline__ uint64_t edt_sync_words(int Z) { return ((uint64_t)Z + 2 + 31) / 32 * 32; }
+// error word, pass Z's other-sites flag, padded to 32).
+__host__ __device__ __forceinline__ uint64_t edt_sync_words(int Z) { return ((uint64_t)Z + 3 + 31) / 32 * 32; }
 
 // Workspace words of pass Z's chunk carries for a map: per warp item
 // (32 columns) one word per lane and chunk.
@@ -405,9 +405,13 @@ __device__ __forceinline__ void pass_z_bits_item(uint32_t* __restrict__ map, con
   }
 }
 
+// skip (optional): the flag occ_from_map_kernel sets when the general pass Z
+// has to run instead.
 __global__ void __launch_bounds__(kZWarps * 32) edt_pass_z_bits(uint32_t* __restrict__ map,
-                                                                 const uint32_t* __restrict__ bits, int X, int Y, int Z) {
+                                                                 const uint32_t* __restrict__ bits, int X, int Y, int Z,
+                                                                 const uint32_t* __restrict__ skip) {
   extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][2 * zw]
+  if (skip != nullptr && *skip != 0u) return;
   const int warp = threadIdx.x >> 5;
   const long long item = (long long)blockIdx.x * kZWarps + warp;
   if (item >= (long long)z_items(X, Y)) return;
@@ -889,9 +893,11 @@ __device__ __forceinline__ uint32_t batch_owner(const long long* __restrict__ pr
 }
 
 // carries: the map's workspace past its counters (zcarry_item_words per item)
+// run_if (optional): runs only when this flag is set (occ_from_map_kernel).
 __global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z(uint32_t* __restrict__ map, uint32_t* __restrict__ carries,
-                                                               int X, int Y, int Z) {
+                                                               int X, int Y, int Z, const uint32_t* __restrict__ run_if) {
   extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][kZWarpWords]
+  if (run_if != nullptr && *run_if == 0u) return;
   const int warp = threadIdx.x >> 5;
   const long long item = (long long)blockIdx.x * kZWarps + warp;
   if (item >= (long long)z_items(X, Y)) return;
@@ -945,6 +951,74 @@ __global__ void occ_insert_batch_kernel(const BatchMap* __restrict__ maps, uint3
                    z = coord_to_voxel(__ldg(xyz + 3 * i + 2), m.side);
     if (x < (uint32_t)m.X && y < (uint32_t)m.Y && z < (uint32_t)m.Z) occ_set(batch_occ(m), m.X, m.Z, x, y, z);
   }
+}
+
+// Occupancy bits of a filled map for the bits pass Z.  After clearMap and
+// insertPointCloud every voxel is UNINIT or holds its own coordinates, and
+// kernelPBAphase1FloodZ (GV/voxelmap/kernels/VoxelMapOperationsPBA.hpp:63-124)
+// then depends only on which voxels are sites.  A voxel holding any other
+// site (a map transformed before, sites moved by mergeOccupied's offset,
+// caller-written data) sets *other_sites, and the general pass Z runs instead.
+// One warp task = one item (32 columns) x 32 rows, lane r on row zc + r: the
+// lane reads its row's 32 columns (eight 16-byte loads when vec) and sets
+// bit k of its word for column k, which is the occupancy word's layout, so
+// the warp's 32 words go out as one 128-byte store.  Consecutive warps take
+// consecutive items of the same rows.  vec: map and rows 16-byte aligned.
+__global__ void __launch_bounds__(256) occ_from_map_kernel(const uint32_t* __restrict__ map, uint32_t* __restrict__ bits,
+                                                           int X, int Y, int Z, uint32_t* __restrict__ other_sites,
+                                                           int vec) {
+  const int lane = threadIdx.x & 31;
+  const long long items = (long long)z_items(X, Y);
+  const long long tasks = items * ((Z + 31) >> 5);
+  const uint32_t layer = (uint32_t)X * (uint32_t)Y;
+  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const bool x_aligned = (X & 31) == 0;  // an item's 32 columns lie in one y row
+  bool other = false;
+  for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tasks; t += warps) {
+    const int chunk = (int)(t / items);
+    const uint32_t item = (uint32_t)(t - (long long)chunk * items);
+    const int z = chunk * 32 + lane;
+    if (z >= Z) continue;
+    const uint32_t f0 = item * 32u;
+    const int ncols = (int)min(32u, layer - f0);
+    const uint32_t* row = map + (uint64_t)z * layer + f0;
+    uint32_t v[32];
+    if (vec && ncols == 32) {
+      const uint4* q = reinterpret_cast<const uint4*>(row);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint4 w = __ldg(q + j);
+        v[4 * j] = w.x;
+        v[4 * j + 1] = w.y;
+        v[4 * j + 2] = w.z;
+        v[4 * j + 3] = w.w;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 32; ++k) v[k] = k < ncols ? __ldg(row + k) : kDvUninit;
+    }
+    uint32_t word = 0u;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) word |= (uint32_t)(v[k] != kDvUninit) << k;
+    const uint32_t y0 = f0 / (uint32_t)X, x0 = f0 - y0 * (uint32_t)X;
+    if (x_aligned) {
+      const uint32_t c0 = x0 | (y0 << 10) | ((uint32_t)z << 20);
+#pragma unroll
+      for (int k = 0; k < 32; ++k) other |= v[k] != kDvUninit && v[k] != c0 + (uint32_t)k;
+    } else {
+      uint32_t x = x0, y = y0;
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        other |= v[k] != kDvUninit && v[k] != (x | (y << 10) | ((uint32_t)z << 20));
+        if (++x == (uint32_t)X) {
+          x = 0u;
+          ++y;
+        }
+      }
+    }
+    bits[(uint64_t)item * Z + z] = word;
+  }
+  if (__any_sync(kFullMask, other) && lane == 0) atomicOr(other_sites, 1u);
 }
 
 __global__ void __launch_bounds__(kZWarps * 32) edt_pass_z_bits_batch(const BatchMap* __restrict__ maps,
@@ -1165,13 +1239,36 @@ cudaError_t kernel_setup(int threads, int smem, long long* resident) {
   return st.err[dev];
 }
 
+// Pass Z of a filled map: occupancy bits from the map, then the bits pass;
+// when some voxel holds another site than its own, the bits pass skips and
+// the general pass runs (both are launched; the flag picks on the device).
+// The bits and the general pass's chunk carries share the workspace area
+// after the counters.
 cudaError_t launch_pass_z(uint32_t* map, uint32_t* scratch, gvx_dims d, cudaStream_t s) {
-  const int smem = kZWarps * kZWarpWords * 4;
-  cudaError_t e = kernel_setup<edt_pass_z>(kZWarps * 32, smem, nullptr);
+  const int X = (int)d.x, Y = (int)d.y, Z = (int)d.z;
+  uint32_t* other = scratch + (uint64_t)Z + 2;
+  uint32_t* area = scratch + edt_sync_words(Z);
+  cudaError_t e = cudaMemsetAsync(other, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
-  const long long items = (long long)z_items((int)d.x, (int)d.y);
-  edt_pass_z<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(
-      map, scratch + edt_sync_words((int)d.z), (int)d.x, (int)d.y, (int)d.z);
+  int dev = 0, sm = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, occ_from_map_kernel, 256, 0)) != cudaSuccess) return e;
+  const long long tasks = (long long)z_items(X, Y) * ((Z + 31) >> 5);  // one per warp, 8 warps per block
+  const long long occ_blocks =
+      std::max<long long>(1, std::min<long long>((tasks + 7) / 8, (long long)std::max(sm, 1) * std::max(per_sm, 1)));
+  const int vec = ((reinterpret_cast<uintptr_t>(map) & 15u) == 0 && ((uint64_t)X * Y) % 4 == 0) ? 1 : 0;
+  occ_from_map_kernel<<<(unsigned)occ_blocks, 256, 0, s>>>(map, area, X, Y, Z, other, vec);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const long long items = (long long)z_items(X, Y);
+  const unsigned z_blocks = (unsigned)((items + kZWarps - 1) / kZWarps);
+  if ((e = kernel_setup<edt_pass_z_bits>(kZWarps * 32, kZBitsSmemMax, nullptr)) != cudaSuccess) return e;
+  edt_pass_z_bits<<<z_blocks, kZWarps * 32, kZWarps * 2 * z_bits_words(Z) * 4, s>>>(map, area, X, Y, Z, other);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int smem = kZWarps * kZWarpWords * 4;
+  if ((e = kernel_setup<edt_pass_z>(kZWarps * 32, smem, nullptr)) != cudaSuccess) return e;
+  edt_pass_z<<<z_blocks, kZWarps * 32, smem, s>>>(map, area, X, Y, Z, other);
   return cudaGetLastError();
 }
 
@@ -1364,7 +1461,7 @@ cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t s
   const int smem = kZWarps * 2 * z_bits_words((int)d.z) * 4;  // sized by Z: more resident warps
   const long long items = (long long)z_items((int)d.x, (int)d.y);
   edt_pass_z_bits<<<(unsigned)((items + kZWarps - 1) / kZWarps), kZWarps * 32, smem, s>>>(d_vox, bits, (int)d.x,
-                                                                                         (int)d.y, (int)d.z);
+                                                                                         (int)d.y, (int)d.z, nullptr);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (cfg.fused) return launch_edt_pass(d_vox, d_scratch, scratch_words, d, 3, s, cfg.rows);
   e = launch_edt_pass(d_vox, d_scratch, scratch_words, d, 1, s, cfg.rows);

@@ -247,3 +247,31 @@ def test_longest_rows(dims, npts):
         m.voxelize_edt(p)
         assert m.edt_check() == 0
         assert np.array_equal(to_u32(m.data()), want), fused
+
+
+@pytest.mark.parametrize("dims", [(64, 40, 70), (37, 29, 33), (5, 3, 40)])
+@pytest.mark.parametrize("where", ["first", "middle", "last"])
+def test_filled_map_with_one_moved_site_takes_the_general_pass(dims, where):
+    """parallelBanding3D on an inserted map reads occupancy bits when every
+    voxel is UNINIT or its own site; one voxel holding another voxel's
+    coordinates must send pass Z down the general path, bit-exact."""
+    rng = np.random.default_rng(len(where) + dims[0])
+    pts = (rng.random((300, 3)) * np.asarray(dims)).astype(np.float32)
+    ins = oracle.dvm_empty(dims)
+    oracle.dvm_insert(ins, dims, 1.0, pts)
+    n = int(np.prod(dims))
+    idx = {"first": 0, "middle": n // 2 + 7, "last": n - 1}[where]
+    ins[idx] = np.uint32(3 | (1 << 10) | (2 << 20))  # the site (3, 1, 2), not this voxel's own
+    want = ins.copy()
+    oracle.pba(want, dims)
+    m = gvx.DistanceVoxelMap(dims, 1.0)
+    m.data().copy_(torch.as_tensor(ins.view(np.int32)).cuda())
+    m.parallelBanding3D()
+    assert m.edt_check() == 0
+    assert np.array_equal(to_u32(m.data()), want), first_mismatch(to_u32(m.data()), want, dims)
+    # and the plain inserted map (no moved site) still matches through the bits path
+    m.clearMap()
+    m.insertPointCloud(torch.as_tensor(pts).cuda())
+    m.parallelBanding3D()
+    _, want2 = oracle_edt(dims, 1.0, pts)
+    assert np.array_equal(to_u32(m.data()), want2)
