@@ -959,15 +959,19 @@ __global__ void occ_insert_batch_kernel(const BatchMap* __restrict__ maps, uint3
 // then depends only on which voxels are sites.  A voxel holding any other
 // site (a map transformed before, sites moved by mergeOccupied's offset,
 // caller-written data) sets *other_sites, and the general pass Z runs instead.
-// One warp task = one item (32 columns) x 32 rows, lane r on row zc + r: the
-// lane reads its row's 32 columns (eight 16-byte loads when vec) and sets
-// bit k of its word for column k, which is the occupancy word's layout, so
-// the warp's 32 words go out as one 128-byte store.  Consecutive warps take
-// consecutive items of the same rows.  vec: map and rows 16-byte aligned.
+// One warp task = one item (32 columns) x 32 rows.  Lane L reads columns
+// 4 * (L & 7) .. + 3 of rows zc + (L >> 3) + 4 j, j = 0..7 (one 16-byte load
+// each when vec), so a load instruction covers 4 whole rows of the item; the
+// 8 lanes of a row OR their 4-bit pieces into the row's occupancy word
+// (bit k = column k) with three xor shuffles, and lane L stores the word of
+// row (L >> 3) + 4 (L & 7): the warp's 32 words as one 128-byte store.
+// Consecutive warps take consecutive items of the same rows.  vec: map and
+// rows 16-byte aligned.
 __global__ void __launch_bounds__(256) occ_from_map_kernel(const uint32_t* __restrict__ map, uint32_t* __restrict__ bits,
                                                            int X, int Y, int Z, uint32_t* __restrict__ other_sites,
                                                            int vec) {
   const int lane = threadIdx.x & 31;
+  const int g = lane >> 3, q = lane & 7;
   const long long items = (long long)z_items(X, Y);
   const long long tasks = items * ((Z + 31) >> 5);
   const uint32_t layer = (uint32_t)X * (uint32_t)Y;
@@ -977,46 +981,65 @@ __global__ void __launch_bounds__(256) occ_from_map_kernel(const uint32_t* __res
   for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tasks; t += warps) {
     const int chunk = (int)(t / items);
     const uint32_t item = (uint32_t)(t - (long long)chunk * items);
-    const int z = chunk * 32 + lane;
-    if (z >= Z) continue;
-    const uint32_t f0 = item * 32u;
-    const int ncols = (int)min(32u, layer - f0);
-    const uint32_t* row = map + (uint64_t)z * layer + f0;
-    uint32_t v[32];
-    if (vec && ncols == 32) {
-      const uint4* q = reinterpret_cast<const uint4*>(row);
+    const int zc = chunk * 32;
+    const uint32_t f = item * 32u + 4u * (uint32_t)q;  // this lane's first column
+    const int ncols = (int)min(32u, layer - item * 32u);
+    const uint32_t y0 = f / (uint32_t)X, x0 = f - y0 * (uint32_t)X;  // f < layer when 4q < ncols
+    // all eight row pieces in flight before any is used
+    uint32_t vv[8][4];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const uint4 w = __ldg(q + j);
-        v[4 * j] = w.x;
-        v[4 * j + 1] = w.y;
-        v[4 * j + 2] = w.z;
-        v[4 * j + 3] = w.w;
-      }
-    } else {
+    for (int j = 0; j < 8; ++j) {
+      const int z = zc + g + 4 * j;
 #pragma unroll
-      for (int k = 0; k < 32; ++k) v[k] = k < ncols ? __ldg(row + k) : kDvUninit;
-    }
-    uint32_t word = 0u;
+      for (int i = 0; i < 4; ++i) vv[j][i] = kDvUninit;
+      if (z < Z) {
+        const uint32_t* row = map + (uint64_t)z * layer + f;
+        if (vec && ncols == 32) {
+          const uint4 w = __ldg(reinterpret_cast<const uint4*>(row));
+          vv[j][0] = w.x;
+          vv[j][1] = w.y;
+          vv[j][2] = w.z;
+          vv[j][3] = w.w;
+        } else {
 #pragma unroll
-    for (int k = 0; k < 32; ++k) word |= (uint32_t)(v[k] != kDvUninit) << k;
-    const uint32_t y0 = f0 / (uint32_t)X, x0 = f0 - y0 * (uint32_t)X;
-    if (x_aligned) {
-      const uint32_t c0 = x0 | (y0 << 10) | ((uint32_t)z << 20);
-#pragma unroll
-      for (int k = 0; k < 32; ++k) other |= v[k] != kDvUninit && v[k] != c0 + (uint32_t)k;
-    } else {
-      uint32_t x = x0, y = y0;
-#pragma unroll
-      for (int k = 0; k < 32; ++k) {
-        other |= v[k] != kDvUninit && v[k] != (x | (y << 10) | ((uint32_t)z << 20));
-        if (++x == (uint32_t)X) {
-          x = 0u;
-          ++y;
+          for (int i = 0; i < 4; ++i)
+            if (4 * q + i < ncols) vv[j][i] = __ldg(row + i);
         }
       }
     }
-    bits[(uint64_t)item * Z + z] = word;
+    uint32_t word = 0u;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int z = zc + g + 4 * j;
+      const uint32_t* v = vv[j];
+      uint32_t piece = 0u;
+      if (x_aligned) {
+        const uint32_t c0 = (x0 | (y0 << 10)) + ((uint32_t)z << 20);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          piece |= (uint32_t)(v[i] != kDvUninit) << i;
+          other |= v[i] != kDvUninit && v[i] != c0 + (uint32_t)i;
+        }
+      } else {
+        uint32_t x = x0, y = y0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          piece |= (uint32_t)(v[i] != kDvUninit) << i;
+          other |= v[i] != kDvUninit && v[i] != (x | (y << 10) | ((uint32_t)z << 20));
+          if (++x == (uint32_t)X) {
+            x = 0u;
+            ++y;
+          }
+        }
+      }
+      uint32_t rw = piece << (4 * q);
+      rw |= __shfl_xor_sync(kFullMask, rw, 1);
+      rw |= __shfl_xor_sync(kFullMask, rw, 2);
+      rw |= __shfl_xor_sync(kFullMask, rw, 4);
+      if (j == q) word = rw;  // row g + 4 q
+    }
+    const int zs = zc + g + 4 * q;
+    if (zs < Z) bits[(uint64_t)item * Z + zs] = word;
   }
   if (__any_sync(kFullMask, other) && lane == 0) atomicOr(other_sites, 1u);
 }
