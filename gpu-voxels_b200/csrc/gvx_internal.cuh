@@ -135,7 +135,8 @@ struct EdtConfig {
 };
 cudaError_t launch_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, cudaStream_t s,
                        const EdtConfig& cfg = EdtConfig{});
-// pass 0 = Z, 1 = Y, 2 = X (one launch each), 3 = fused Y -> X
+// pass 0 = Z (occupancy bits from the map, the bits pass, and the general
+// pass when a voxel holds another site), 1 = Y, 2 = X, 3 = fused Y -> X
 cudaError_t launch_edt_pass(uint32_t* d_vox, uint32_t* d_scratch, uint64_t scratch_words, gvx_dims d, int pass,
                             cudaStream_t s, int rows = 0);
 // Synchronous read of the error word the last fused launch left (0 = ok).

@@ -97,8 +97,10 @@ GVX_API gvx_status gvx_dvm_edt(gvx_dvm *m, uint32_t m1, uint32_t m2, uint32_t m3
  * cleared, scattered and re-read.  No counterpart in the reference. */
 GVX_API gvx_status gvx_dvm_voxelize_edt(gvx_dvm *m, const float *d_xyz, uint64_t n, uint32_t *d_outside,
                                         gvx_stream stream);
-/* One stage of the EDT, for per-pass timing and tests: 0 = the z sweep,
- * 1 = the y sweep, 2 = the x sweep (one launch each), 3 = the y and x sweeps
+/* One stage of the EDT, for per-pass timing and tests: 0 = the z sweep (when
+ * every voxel is UNINIT or its own site: occupancy bits read from the map,
+ * then the sweep over the bits; otherwise the general sweep), 1 = the y sweep,
+ * 2 = the x sweep (one launch each), 3 = the y and x sweeps
  * as the single fused launch gvx_dvm_edt uses (0 then 3 == gvx_dvm_edt;
  * 0, 1, 2 gives the same result).  Pass 0 alone equals the reference's
  * phase 1 (kernelPBAphase1FloodZ, GV/voxelmap/kernels/VoxelMapOperationsPBA.hpp:63-124). */
