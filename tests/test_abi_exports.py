@@ -40,3 +40,17 @@ def test_error_path_without_device():
     assert lib.gvx_dvm_create(ctypes.byref(d), 1.0, ctypes.byref(out)) == 2
     with pytest.raises(abi.GvxError):
         abi.call("gvx_dvm_edt", None, 1, 1, 1, None)
+
+
+def test_query_config_validation_without_device():
+    """gvx_set_query_config is host-only: shapes outside threads {64,128,256,512}
+    x blocks_per_sm [1,64] are refused with GVX_ERR_INVALID_ARG (1), valid ones
+    accepted; the library default (256 x 16) is restored at the end."""
+    import gvx._abi as abi
+    lib = abi.lib()
+    for threads, cap, want in [(64, 1, 0), (512, 64, 0), (128, 32, 0), (96, 16, 1), (1024, 16, 1), (256, 0, 1),
+                               (256, 65, 1)]:
+        c = abi.QueryConfig(threads, cap, 0.0)
+        assert lib.gvx_set_query_config(ctypes.byref(c)) == want, (threads, cap)
+    assert lib.gvx_set_query_config(None) == 1
+    assert lib.gvx_set_query_config(ctypes.byref(abi.QueryConfig(256, 16, 0.0))) == 0
