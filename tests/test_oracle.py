@@ -236,3 +236,52 @@ def test_list_vs_list_46():
     ids, _ = _list_from_boxes(dims)
     assert oracle.list_collide_list(ids, ids) == 46
     assert oracle.list_collide_list(ids[:10], ids[5:]) == 5
+
+
+def _closed_form_phase1(occ: np.ndarray) -> np.ndarray:
+    """The per-column closed form the occupancy-bit pass Z uses (edt.cu,
+    pass_z_bits_item): between consecutive sites s1 < s2 of a column (s2 = 1023
+    above the highest site, s1 = 1023 below the lowest), rows z <= (s1 + s2) >> 1
+    take s1 and the others s2; with s1 = 1023 every row takes s2.  occ: bool
+    [Z, Y, X]; returns the site z per voxel (1023 = none)."""
+    Z = occ.shape[0]
+    out = np.full(occ.shape, 1023, dtype=np.int64)
+    for y in range(occ.shape[1]):
+        for x in range(occ.shape[2]):
+            sites = [int(z) for z in np.flatnonzero(occ[:, y, x])]
+            for z in range(Z):
+                below = [s for s in sites if s <= z]
+                above = [s for s in sites if s > z]
+                s1 = below[-1] if below else 1023
+                s2 = above[0] if above else 1023
+                if s1 == z:
+                    out[z, y, x] = z
+                elif s1 == 1023:
+                    out[z, y, x] = s2
+                else:
+                    out[z, y, x] = s1 if z <= (s1 + s2) >> 1 else s2
+    return out
+
+
+@pytest.mark.parametrize("dims,density,seed", [((7, 5, 40), 0.05, 0), ((6, 4, 33), 0.3, 1), ((5, 5, 64), 0.01, 2),
+                                               ((3, 2, 1), 0.5, 3)])
+def test_closed_form_backward_flood_equals_phase1(dims, density, seed):
+    """kernelPBAphase1FloodZ (GV/voxelmap/kernels/VoxelMapOperationsPBA.hpp:63-124)
+    on an inserted map, restated by the oracle, equals the closed form above,
+    ties (z equidistant from two sites) and the UNINIT-as-1023 arithmetic
+    included."""
+    X, Y, Z = dims
+    rng = np.random.default_rng(seed)
+    occ = rng.random((Z, Y, X)) < density
+    occ[:, 0, 0] = False  # one empty column
+    vmap = oracle.dvm_empty(dims)
+    zz, yy, xx = np.nonzero(occ)
+    vmap.reshape(Z, Y, X)[zz, yy, xx] = (xx | (yy << 10) | (zz << 20)).astype(np.uint32)
+    oracle.phase1(vmap, dims)
+    got = vmap.reshape(Z, Y, X)
+    want_z = _closed_form_phase1(occ)
+    gx = np.arange(X)[None, None, :]
+    gy = np.arange(Y)[None, :, None]
+    want = np.where(want_z == 1023, np.uint32(0x3FFFFFFF),
+                    (gx | (gy << 10) | (want_z << 20)).astype(np.uint32))
+    assert np.array_equal(got, want)
