@@ -4,7 +4,9 @@
 Headline (one JSON line on rank 0): exact-EDT throughput in Gvoxel/s on the
 512^3 @ 5 mm depth-image scene (voxelise ~1.2M points + EDT per step), with
 the EDT kernels' HBM roofline, an end-to-end number through the public API
-with host buffers, the CPU oracle as a reported baseline and, when built,
+with host buffers (double-buffered: the next step's host->device copy runs on
+a copy stream during this step; the serial loop is reported beside it), the
+CPU oracle as a reported baseline and, when built,
 gpu-voxels' own kernels timed on the same GPU.  Secondary sections cover the
 other configs (128^3 queries, 512^3 BitVoxelMap collision, batched lists,
 sphere/trajectory queries with gradients, many uneven maps).
