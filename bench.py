@@ -175,6 +175,15 @@ def pinned_near_gpu(torch, tensors):
     return out, ("gpu-local NUMA node" if cpus else "default")
 
 
+def bench_config(world: int) -> dict:
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD, "map_dims": list(C2_DIMS), "voxel_side_m": C2_SIDE,
+            "map_bytes": int(np.prod(C2_DIMS)) * 4,
+            "l2": (f"map ({int(np.prod(C2_DIMS)) * 4 >> 20} MiB) larger than L2 (126 MB); no flush needed"
+                   if np.prod(C2_DIMS) * 4 > 126e6 else "map fits in L2 (profiling case only)"),
+            "parallelism": f"replicas x{world}"}
+
+
 def whole_job_rate(units_per_rank: float, world: int, ms: float, scale: float = 1e9) -> float:
     """Throughput of the whole job: the units every rank processed over the
     slowest rank's time (ms), in units of `scale` per second."""
@@ -191,7 +200,7 @@ def run_reference(args):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    from gvx import workloads
+    import workloads
 
     pts = workloads.c2_points()
     base = oracle.dvm_empty(C2_DIMS)
@@ -216,7 +225,7 @@ def run_reference(args):
         "impl": "reference", "metric": "edt_gvoxel_per_s", "value": round(value, 4), "unit": "Gvoxel/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * total / len(times), 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32 (fp32 bisector)",
-        "data": "synthetic", "config": {"workload": WORKLOAD},
+        "data": "synthetic", "config": bench_config(args.gpus),
         "cpu_baseline": {"value": round(value, 4), "unit": "Gvoxel/s", "cores": cores, "kind": "port",
                          "sample": "each step: insert + full 512^3 EDT of the C2 scene on the host cores (OpenMP)"},
         "e2e": {"value": round(value, 4), "unit": "Gvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -248,7 +257,7 @@ def _time(fn, reps, warm=2):
 def section_c1(hbm_peak):
     import torch
     import gvx
-    from gvx import workloads
+    import workloads
     sc = workloads.c1_scene()
     dvm = gvx.DistanceVoxelMap(sc.dims, sc.side)
     pts = torch.as_tensor(sc.points).cuda()
@@ -271,7 +280,7 @@ def section_c1(hbm_peak):
 def section_c2_collide(hbm_peak, pts_host):
     import torch
     import gvx
-    from gvx import workloads
+    import workloads
     dims = C2_DIMS
     nvox = int(np.prod(dims))
     scene = gvx.BitVectorVoxelMap(dims, C2_SIDE)
@@ -293,7 +302,7 @@ def section_c2_collide(hbm_peak, pts_host):
 def section_c3(hbm_peak):
     import torch
     import gvx
-    from gvx import workloads
+    import workloads
     sc = workloads.c3_scene()
     dvm = gvx.DistanceVoxelMap(sc.dims, sc.side)
     dvm.insertPointCloud(torch.as_tensor(sc.points).cuda())
@@ -346,7 +355,8 @@ def section_c3(hbm_peak):
 def section_c4(hbm_peak):
     import torch
     import gvx
-    from gvx import autograd, workloads
+    import workloads
+    from gvx import autograd
     sc = workloads.c3_scene()
     dvm = gvx.DistanceVoxelMap(sc.dims, sc.side)
     dvm.insertPointCloud(torch.as_tensor(sc.points).cuda())
@@ -408,7 +418,7 @@ def section_c5(hbm_peak):
     CUDA graph.  The batch results are checked bit-equal to the loop's."""
     import torch
     import gvx
-    from gvx import workloads
+    import workloads
     from gvx.batch import Batch
     scenes = workloads.c5_maps()
     maps = [gvx.DistanceVoxelMap(s.dims, s.side) for s in scenes]
@@ -508,7 +518,7 @@ def main():
 
     import torch
     import gvx
-    from gvx import workloads
+    import workloads
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -689,10 +699,9 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32 (fp32 bisector)",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "call": "voxelize_edt (clearMap + insertPointCloud + parallelBanding3D in one)",
-                   "three_call_step_ms": round(three_ms, 4),
-                   "map_bytes": nvox * 4, "l2": "map (512 MiB) larger than L2; no flush needed",
-                   "parallelism": f"replicas x{world}"},
+        "config": bench_config(world),
+        "call": "voxelize_edt (clearMap + insertPointCloud + parallelBanding3D in one)",
+        "three_call_step_ms": round(three_ms, 4),
         "roofline": roofline, "e2e": e2e, "edt_config": edt_config,
         "gpu_launches": 3 * args.steps,  # occupancy insert, z sweep from bits, fused y->x sweep (+ 2 memsets)
         "clocks": clocks.summary(),

@@ -74,16 +74,7 @@ __global__ void batch_trilinear_kernel(const BatchMap* __restrict__ maps, const 
   }
 }
 
-int g_sms = 0;
-int sms() {
-  if (g_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sms <= 0) g_sms = 148;
-  }
-  return g_sms;
-}
+int sms() { return device_sms(); }
 
 gvx_status fail(gvx_status st, const char* msg) {
   set_error(msg);

@@ -18,16 +18,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-int g_sms = 0;
-int sms() {
-  if (g_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sms <= 0) g_sms = 148;
-  }
-  return g_sms;
-}
+int sms() { return device_sms(); }
 
 // Non-empty test of one 16-byte half; `low` marks the half holding bit 0.
 __device__ __forceinline__ uint32_t half_bits(uint4 v, bool low) {

@@ -153,9 +153,7 @@ __global__ void __launch_bounds__(256) list_list_types_kernel(const uint32_t* __
 }
 
 unsigned grid_for(uint64_t n) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int sms = device_sms();
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8));
 }
 

@@ -243,16 +243,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapV
   }
 }
 
-int g_sms = 0;
-int sms() {
-  if (g_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sms <= 0) g_sms = 148;
-  }
-  return g_sms;
-}
+int sms() { return device_sms(); }
 
 unsigned blocks_for(uint64_t items, uint64_t per_block, uint64_t cap_per_sm) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + per_block - 1) / per_block, (uint64_t)sms() * cap_per_sm));

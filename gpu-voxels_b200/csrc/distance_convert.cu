@@ -154,9 +154,7 @@ __global__ void __launch_bounds__(256) band_write_kernel(const uint32_t* __restr
 }
 
 unsigned grid_for(uint64_t n) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int sms = device_sms();
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 16));
 }
 

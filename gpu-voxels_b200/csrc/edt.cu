@@ -1475,7 +1475,7 @@ cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t s
   cudaError_t e = cudaMemsetAsync(bits, 0, occ_words((int)d.x, (int)d.y, (int)d.z) * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   if (n > 0) {
-    const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
+    const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)device_sms() * 16);
     occ_insert_kernel<<<blocks, 256, 0, s>>>(bits, (int)d.x, (int)d.y, (int)d.z, side, d_xyz, n, d_outside);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
@@ -1497,7 +1497,7 @@ cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems&
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if (n_total > 0) {
-    const unsigned blocks = (unsigned)std::min<uint64_t>((n_total + 255) / 256, 148ull * 16);
+    const unsigned blocks = (unsigned)std::min<uint64_t>((n_total + 255) / 256, (uint64_t)device_sms() * 16);
     occ_insert_batch_kernel<<<blocks, 256, 0, s>>>(d_table, it.n_maps, d_xyz, d_offsets, n_total);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }

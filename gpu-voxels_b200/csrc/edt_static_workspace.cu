@@ -12,10 +12,18 @@
 //
 // The workspace is a file-scope __device__ array of kStaticWorkspaceWords
 // 32-bit words: 64 MiB of stack area plus 8 KiB for the EDT's per-slice
-// counters.  Every GPU on which the library's kernels are loaded holds it
-// until the process exits.  Maps whose EDT workspace would exceed it (more
-// than 16,777,216 voxels once x and y are rounded up to multiples of 32;
-// 256^3 fits) are rejected with GVX_ERR_OUT_OF_DOMAIN.
+// counters.  This file is its own device module (the library is built
+// without relocatable device code), so when the array is placed on a GPU
+// follows CUDA's module loading: under lazy loading (CUDA_MODULE_LOADING=LAZY,
+// the default) at the first call on that device, under eager loading in
+// every device context the process creates.  Either way it stays there until
+// the process exits.  Maps whose EDT workspace would exceed it (more than
+// 16,777,216 voxels once x and y are rounded up to multiples of 32; 256^3
+// fits) are rejected with GVX_ERR_OUT_OF_DOMAIN.
+//
+// The fused y -> x sweep's bounded waits report a give-up in an error word
+// inside this workspace (word dims.z + 1, zeroed by every call), which
+// gvx_dvm_edt_static_workspace_check reads without a map handle.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -38,7 +46,10 @@ uint32_t* g_workspace_addr[kMaxDevices] = {};
 
 // Device address of the workspace on the current device.  In host code the
 // array's name is only a host-side stand-in, so the address is looked up once
-// per device with cudaGetSymbolAddress (with that device current) and cached.
+// per device with cudaGetSymbolAddress (with that device current) and cached
+// for the life of the process.  The cache does not survive cudaDeviceReset
+// (or any other teardown of the device's primary context): the module, and
+// with it the array, is then placed anew at another address.
 gvx_status workspace_address(uint32_t** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -86,4 +97,28 @@ extern "C" gvx_status gvx_dvm_edt_static_workspace(uint32_t* d_voxels, const gvx
   gvx_status st = workspace_address(&workspace);
   if (st != GVX_OK) return st;
   return cuda_status(launch_edt(d_voxels, workspace, kStaticWorkspaceWords, *dims, as_stream(stream)), "EDT (static workspace)");
+}
+
+extern "C" gvx_status gvx_dvm_edt_static_workspace_check(const gvx_dims* dims, uint32_t* flags) {
+  using namespace gvx;
+  if (dims == nullptr || flags == nullptr) {
+    set_error("null argument");
+    return GVX_ERR_INVALID_ARG;
+  }
+  if (dims->z < 1 || dims->z > kMaxDim) {
+    set_error("every map axis must be in [1, 1023] (10-bit DistanceVoxel coordinates)");
+    return GVX_ERR_OUT_OF_DOMAIN;
+  }
+  // The counter area is [slice counters: z][queue head][error word]; a copy
+  // from the symbol needs no device address and allocates nothing.
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess)
+    e = cudaMemcpyFromSymbol(flags, g_edt_workspace, sizeof(uint32_t), (size_t)(dims->z + 1) * sizeof(uint32_t),
+                             cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e, "static-workspace EDT check");
+  if (*flags != 0) {
+    set_error("EDT (static workspace): a slice wait of the fused y->x sweep gave up (results invalid)");
+    return GVX_ERR_TIMEOUT;
+  }
+  return GVX_OK;
 }

@@ -109,6 +109,9 @@ struct BatchItems {
 
 // Error reporting shared by the ABI units.
 void set_error(const std::string& msg);
+// Streaming multiprocessors of the current device (cudaDevAttrMultiProcessorCount,
+// cached per device; 1 if the query fails), for grid sizing.
+int device_sms();
 gvx_status cuda_status(cudaError_t e, const char* what);
 
 inline uint64_t num_voxels(const gvx_dims& d) { return (uint64_t)d.x * d.y * d.z; }

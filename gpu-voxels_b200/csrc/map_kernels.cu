@@ -1,5 +1,7 @@
 // Map fill and point-cloud voxelisation kernels.
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <stdint.h>
 
 #include <algorithm>
@@ -9,16 +11,6 @@
 namespace gvx {
 namespace {
 
-int g_num_sms = 0;
-int num_sms() {
-  if (g_num_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
-  }
-  return g_num_sms;
-}
 
 // clearMap for DistanceVoxel (GV/voxelmap/TemplateVoxelMap.hpp:244-271):
 // 16-byte stores of the uninitialised value; the map base is 256-B aligned.
@@ -111,11 +103,29 @@ __global__ void bvm_shift_kernel(uint32_t* __restrict__ vox, uint64_t n, uint32_
 
 unsigned grid_for(uint64_t n, int threads) {
   const uint64_t want = (n + threads - 1) / threads;
-  const uint64_t cap = (uint64_t)num_sms() * 16;
+  const uint64_t cap = (uint64_t)device_sms() * 16;
   return (unsigned)std::max<uint64_t>(1, std::min(want, cap));
 }
 
 }  // namespace
+
+namespace {
+constexpr int kSmsDevices = 64;
+std::atomic<int> g_sms_of[kSmsDevices];
+}  // namespace
+
+int device_sms() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  if (dev >= 0 && dev < kSmsDevices) {
+    const int cached = g_sms_of[dev].load(std::memory_order_relaxed);
+    if (cached > 0) return cached;
+  }
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) return 1;
+  if (dev >= 0 && dev < kSmsDevices) g_sms_of[dev].store(sms, std::memory_order_relaxed);
+  return sms;
+}
 
 cudaError_t launch_dvm_clear(uint32_t* d_vox, uint64_t n, cudaStream_t s) {
   const uint64_t n4 = n / 4;

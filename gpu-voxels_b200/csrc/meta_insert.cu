@@ -82,9 +82,7 @@ __global__ void meta_insert_kernel(uint32_t* __restrict__ map, uint32_t X, uint3
 }
 
 unsigned grid_for(uint64_t n) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int sms = device_sms();
   const uint64_t want = (n + 255) / 256;
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)std::max(sms, 1) * 16));
 }

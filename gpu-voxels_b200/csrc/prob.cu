@@ -81,9 +81,7 @@ __global__ void merge_occupied_kernel(uint32_t* __restrict__ dvm, const int8_t* 
 }
 
 unsigned grid_for(uint64_t n, int threads) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int sms = device_sms();
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + threads - 1) / threads, (uint64_t)sms * 16));
 }
 

@@ -55,15 +55,8 @@ __global__ void sqdist_map_kernel(const uint32_t* __restrict__ map, uint32_t X, 
   }
 }
 
-int g_sms = 0;
 unsigned grid_for(uint64_t n) {
-  if (g_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_sms <= 0) g_sms = 148;
-  }
-  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)g_sms * 16));
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)device_sms() * 16));
 }
 
 }  // namespace

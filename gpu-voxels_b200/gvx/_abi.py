@@ -86,6 +86,7 @@ PROTOTYPES = {
     "gvx_dvm_autotune": [_vp, ctypes.c_int, ctypes.POINTER(EdtConfig), _vp],
     "gvx_dvm_set_edt_config": [_vp, ctypes.POINTER(EdtConfig)],
     "gvx_dvm_edt_static_workspace": [_vp, ctypes.POINTER(Dims), _vp],
+    "gvx_dvm_edt_static_workspace_check": [ctypes.POINTER(Dims), ctypes.POINTER(_u32)],
     "gvx_dvm_sqdist": [_vp, _vp, _u64, _vp, _vp],
     "gvx_dvm_dist": [_vp, _vp, _u64, _vp, _vp],
     "gvx_dvm_gather": [_vp, _vp, _u64, _vp, _vp],

@@ -140,17 +140,28 @@ GVX_API gvx_status gvx_check_bisector_quotient(uint64_t *mismatches);
  * aligned), for callers that may not allocate device memory once running
  * (real-time control loops, plugins inside a host that owns all device
  * memory).  It calls no cudaMalloc/cudaFree and no allocating library
- * routine: its workspace is a 64 MiB array built into the library, held on
- * every GPU that loads the library's kernels until the process exits.
+ * routine: its workspace is a 64 MiB array built into the library.  Under
+ * CUDA's default lazy module loading the array is committed on a device at
+ * this entry point's first call there; under eager loading
+ * (CUDA_MODULE_LOADING=EAGER) in every device context the process creates.
+ * It stays committed until the process exits.
  * Limit: the map must need at most 16,777,216 workspace words, i.e. at most
  * 16,777,216 voxels with x and y rounded up to multiples of 32 (256^3 fits);
  * larger maps return GVX_ERR_OUT_OF_DOMAIN and are left untouched.
  * The first call on each device looks up the workspace's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * (cudaGetSymbolAddress) and caches it; make that first call before any
+ * stream capture.  The cached address does not survive cudaDeviceReset.
  * All calls share the one workspace and no part of it has to start at zero,
  * but calls that overlap on the GPU (other streams, other threads) race on
  * it: order them on one stream or synchronise between them. */
 GVX_API gvx_status gvx_dvm_edt_static_workspace(uint32_t *d_voxels, const gvx_dims *dims, gvx_stream stream);
+/* No counterpart in the reference.  The handle-free form of gvx_dvm_edt_check
+ * for gvx_dvm_edt_static_workspace: synchronises the device and reads the
+ * error word of the last static-workspace EDT (the one with these dims):
+ * *flags = 0 when every bounded wait of its fused y -> x sweep ended in
+ * time, else non-zero with GVX_ERR_TIMEOUT (that map's content is then
+ * invalid).  Allocates nothing. */
+GVX_API gvx_status gvx_dvm_edt_static_workspace_check(const gvx_dims *dims, uint32_t *flags);
 
 /* Replaces DistanceVoxelMap::getSquaredDistances(device_ptr<uint> b, e, device_ptr<int32_t> out)
  * (DistanceVoxelMap.hpp:741-752): squared voxel distance to the nearest site

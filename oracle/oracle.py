@@ -34,10 +34,19 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
 
 
+def ref_src():
+    """The gpu-voxels source tree (packages/gpu_voxels/src): the environment
+    variable GVX_REF_SRC, else the reference checkout beside the repository
+    (../reference); None when neither exists."""
+    src = os.environ.get("GVX_REF_SRC") or os.path.join(
+        os.path.dirname(_HERE), "..", "reference", "packages", "gpu_voxels", "src")
+    return os.path.abspath(src) if os.path.isdir(src) else None
+
+
 def build_ref():
     """Compile _ref/libgvref.so from the reference source tree when present."""
-    src = "/root/reference/packages/gpu_voxels/src"
-    if not os.path.isdir(src):
+    src = ref_src()
+    if src is None:
         return False
     subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_SRC={src}"], check=True)
     return True

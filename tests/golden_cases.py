@@ -30,6 +30,6 @@ def points_for(spec) -> np.ndarray:
     if kind == "fixed":
         return np.asarray(spec["pts"], dtype=np.float32)
     if kind == "boxes":
-        from gvx import workloads
+        import workloads
         return workloads.box_scene(spec["seed"], dims * side, n_boxes=12, n_points=20_000)
     raise ValueError(kind)

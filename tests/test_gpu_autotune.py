@@ -13,7 +13,7 @@ import torch
 import gvx
 import oracle
 from gpu_helpers import to_u32
-from gvx import workloads
+import workloads
 from gvx.batch import Batch
 
 pytestmark = pytest.mark.gpu

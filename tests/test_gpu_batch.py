@@ -6,7 +6,7 @@ import torch
 
 import gvx
 import oracle
-from gvx import workloads
+import workloads
 from gvx.batch import Batch
 from gpu_helpers import to_u32
 

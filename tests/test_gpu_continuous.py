@@ -8,7 +8,7 @@ import torch
 import gvx
 import oracle
 from gpu_helpers import gpu_edt, to_u32
-from gvx import workloads
+import workloads
 
 pytestmark = pytest.mark.gpu
 

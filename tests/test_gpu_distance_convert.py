@@ -8,7 +8,7 @@ import torch
 import gvx
 import oracle
 from gpu_helpers import gpu_edt
-from gvx import workloads
+import workloads
 
 pytestmark = pytest.mark.gpu
 

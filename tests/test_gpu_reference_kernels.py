@@ -11,7 +11,7 @@ import gvx
 import oracle
 import refgeom
 from gpu_helpers import first_mismatch, gpu_edt, oracle_edt, to_u32
-from gvx import workloads
+import workloads
 
 pytestmark = pytest.mark.gpu
 

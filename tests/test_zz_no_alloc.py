@@ -4,11 +4,14 @@ It exists for callers that may not allocate device memory once running (a
 real-time control loop, a plugin inside a host application that owns all
 device memory): it runs the EDT in place on the caller's voxel buffer with a
 workspace built into the library.  This test drives it through the C ABI with
-ctypes and checks, on two calls in a row, that it returns exactly what the
+ctypes and checks, on three calls in a row, that it returns exactly what the
 regular entry point (gvx_dvm_create + gvx_dvm_edt) returns -- the EDT is
 integer work, so the tolerance is bit equality, as in the other EDT tests.
-The second call reuses the workspace left over from the first.  This file is
-collected last so a failure here comes after every other test has run.
+The 256^3 map runs first and a small map twice after it, so the small map's
+calls meet the counters, stacks and occupancy words a larger map left in the
+shared workspace.  After every call the handle-free check must report that
+no bounded wait gave up.  This file is collected last so a failure here
+comes after every other test has run.
 """
 import ctypes
 
@@ -53,21 +56,22 @@ def _copy_from(device_ptr, dst):
 
 def test_static_workspace_edt_matches_regular_entry_point_twice():
     import gvx._abi as abi
-    from gvx import workloads
+    import workloads
 
     lib = abi.lib()
     rng = np.random.default_rng(2024)
     sc = workloads.c3_scene()  # 256^3: the largest cube the built-in workspace takes
-    cases = [
-        ((96, 64, 80), 1.0, (rng.random((3000, 3)) * [96, 64, 80]).astype(np.float32)),
-        (sc.dims, sc.side, sc.points),
-    ]
+    small = ((96, 64, 80), 1.0, (rng.random((3000, 3)) * [96, 64, 80]).astype(np.float32))
+    cases = [(sc.dims, sc.side, sc.points), small, small]
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    for dims, side, pts in cases:  # two calls in a row on one shared workspace
+    for dims, side, pts in cases:  # calls in a row on one shared workspace
         before, want = _regular_edt(abi, dims, side, pts)
         buf = before.clone()
         d = abi.Dims(*dims)
         abi.check(lib.gvx_dvm_edt_static_workspace(ctypes.c_void_p(buf.data_ptr()), ctypes.byref(d), stream))
+        flags = ctypes.c_uint32(7)
+        abi.check(lib.gvx_dvm_edt_static_workspace_check(ctypes.byref(d), ctypes.byref(flags)))
+        assert flags.value == 0
         torch.cuda.synchronize()
         assert torch.equal(buf, want), f"static-workspace EDT differs from gvx_dvm_edt on {dims}"
 
