@@ -137,6 +137,9 @@ def ref_lib():
         R.ref_dvm_insert.restype = ctypes.c_int
         R.ref_bvm_collide.argtypes = [_u8p, _u8p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)]
         R.ref_bvm_collide.restype = ctypes.c_int
+        R.ref_lists_collide_map.argtypes = [_u32p, _u8p, _u64p, ctypes.c_uint32, _u8p, _u32p,
+                                            np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS"), _u64p]
+        R.ref_lists_collide_map.restype = ctypes.c_int
         _REF = R
     return _REF
 

@@ -13,6 +13,11 @@
 // (GV = packages/gpu_voxels/src/gpu_voxels/).  Built by oracle/Makefile `ref`.
 #include <gpu_voxels/voxelmap/kernels/VoxelMapOperationsPBA.hpp>
 #include <gpu_voxels/voxel/DefaultCollider.hpp>
+// The list kernel names voxelmap::getHighestVoxelPtr unqualified; the
+// reference's own translation units see it through their using-directives.
+#include <gpu_voxels/voxelmap/kernels/VoxelMapOperations.h>
+namespace gpu_voxels { namespace voxellist { using voxelmap::getHighestVoxelPtr; } }
+#include <gpu_voxels/voxellist/kernels/VoxelListOperations.hpp>
 
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -24,11 +29,6 @@ using namespace gpu_voxels;
 using namespace gpu_voxels::voxelmap;
 
 namespace {
-
-// kernelCollideWithVoxelMap is declared in the list operations header, which
-// pulls in the octree; its body is restated nowhere -- the map-vs-map kernel
-// covers the collider, and list collisions are pinned by the known answers of
-// GV/test/testing_voxellist.cu instead.
 
 // computeLinearLoad (GV/helpers/MathHelpers.cpp:29-83), restated: 1024
 // threads per block, at most cMAX_NR_OF_BLOCKS blocks (kernels grid-stride).
@@ -205,6 +205,56 @@ int ref_bvm_collide(uint8_t* h_self, const uint8_t* h_other, uint32_t nvox, uint
   if (!rc) rc = check(cudaMemcpy(h_self, a, bytes, cudaMemcpyDeviceToHost));
   cudaFree(a);
   cudaFree(b);
+  cudaFree(res);
+  return rc;
+}
+
+// kernelCollideWithVoxelMap<BitVectorVoxel, BitVectorVoxel, DefaultCollider>
+// (GV/voxellist/kernels/VoxelListOperations.hpp:146-197) over many lists
+// against one BitVectorVoxelMap, one launch per list with the launch sizing of
+// TemplateVoxelList::collisionCheckWithCollider (TemplateVoxelList.hpp:
+// 1170-1213): computeLinearLoad(list size), cMAX_THREADS_PER_BLOCK BitVectorVoxels
+// of dynamic shared memory, per-block uint16 counts summed on the host.
+// Lists are CSR on the host (ids, 32-byte voxels, offsets[n_lists + 1]); the
+// list voxels receive the reference's collision marks.  `offset` is the
+// relative map offset in voxels (x, y, z).
+int ref_lists_collide_map(const uint32_t* h_ids, uint8_t* h_list_vox, const uint64_t* h_offsets, uint32_t n_lists,
+                          const uint8_t* h_map, const uint32_t dims[3], const int32_t offset[3], uint64_t* h_counts) {
+  const Vector3ui dim(dims[0], dims[1], dims[2]);
+  const Vector3i off(offset[0], offset[1], offset[2]);
+  const uint64_t nvox = (uint64_t)dims[0] * dims[1] * dims[2];
+  const uint64_t n_ids = h_offsets[n_lists];
+  BitVectorVoxel *map = nullptr, *lvox = nullptr;
+  MapVoxelID* ids = nullptr;
+  uint16_t* res = nullptr;
+  if (cudaMalloc(&map, nvox * sizeof(BitVectorVoxel)) || cudaMalloc(&lvox, (n_ids + 1) * sizeof(BitVectorVoxel)) ||
+      cudaMalloc(&ids, (n_ids + 1) * sizeof(MapVoxelID)) ||
+      cudaMalloc(&res, cMAX_NR_OF_BLOCKS * sizeof(uint16_t))) {
+    cudaFree(map); cudaFree(lvox); cudaFree(ids); cudaFree(res);
+    return -1;
+  }
+  int rc = check(cudaMemcpy(map, h_map, nvox * sizeof(BitVectorVoxel), cudaMemcpyHostToDevice));
+  if (!rc) rc = check(cudaMemcpy(lvox, h_list_vox, n_ids * sizeof(BitVectorVoxel), cudaMemcpyHostToDevice));
+  if (!rc) rc = check(cudaMemcpy(ids, h_ids, n_ids * sizeof(MapVoxelID), cudaMemcpyHostToDevice));
+  std::vector<uint16_t> h(cMAX_NR_OF_BLOCKS);
+  DefaultCollider collider(1.0f);
+  const size_t dyn_smem = sizeof(BitVectorVoxel) * cMAX_THREADS_PER_BLOCK;
+  for (uint32_t l = 0; l < n_lists && !rc; ++l) {
+    const uint32_t n = (uint32_t)(h_offsets[l + 1] - h_offsets[l]);
+    uint32_t blocks, threads;
+    linear_load(n, &blocks, &threads);
+    voxellist::kernelCollideWithVoxelMap<<<blocks, threads, dyn_smem>>>(ids + h_offsets[l], lvox + h_offsets[l], n, map,
+                                                                        dim, collider, off, res);
+    rc = check(cudaDeviceSynchronize());
+    if (!rc) rc = check(cudaMemcpy(h.data(), res, blocks * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    uint64_t c = 0;
+    for (uint32_t i = 0; i < blocks; ++i) c += h[i];
+    h_counts[l] = c;
+  }
+  if (!rc) rc = check(cudaMemcpy(h_list_vox, lvox, n_ids * sizeof(BitVectorVoxel), cudaMemcpyDeviceToHost));
+  cudaFree(map);
+  cudaFree(lvox);
+  cudaFree(ids);
   cudaFree(res);
   return rc;
 }

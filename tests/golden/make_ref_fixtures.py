@@ -1,11 +1,13 @@
 """Generate golden fixtures from gpu-voxels' OWN kernels (oracle/_ref/libgvref.so,
 built from the reference sources for sm_100a) -- needs a GPU.
 
-    python tests/golden/make_ref_fixtures.py <out_dir>
+    python tests/golden/make_ref_fixtures.py <out_dir> [lists]
 
 Each fixture holds the seeded inputs' description and the reference's output
 map after insertPointCloud + parallelBanding3D(1,1,1) (zlib-compressed), plus
-the reference's squared distances and a BitVoxel collision count.  The CPU
+the reference's squared distances and a BitVoxel collision count; the list
+fixture holds the reference's per-list counts and marked list voxels of
+LIST_CASE (`lists` makes only that one).  The CPU
 test suite (tests/test_golden.py) checks the oracle against them without a GPU.
 """
 import ctypes
@@ -19,7 +21,7 @@ sys.path[:0] = [os.path.join(ROOT, "oracle"), os.path.join(ROOT, "gpu-voxels_b20
 
 import oracle  # noqa: E402
 import refgeom  # noqa: E402
-from golden_cases import CASES, points_for  # noqa: E402
+from golden_cases import CASES, LIST_CASE, list_inputs, points_for  # noqa: E402
 
 
 def main(out_dir):
@@ -54,7 +56,32 @@ def main(out_dir):
     assert R.ref_bvm_collide(a_ref, b, a.shape[0] // 32, ctypes.byref(cnt)) == 0
     np.savez_compressed(os.path.join(out_dir, "ref_bvm_collide.npz"), count=np.uint64(cnt.value), marked=a_ref)
     print("bvm collide", cnt.value)
+    make_list_fixture(R, out_dir)
+
+
+def make_list_fixture(R, out_dir):
+    """Per-list counts and the marked list voxels of the reference's list-vs-map
+    kernel, for every offset of LIST_CASE."""
+    bmap, ids, vox, offs = list_inputs(LIST_CASE)
+    dims = np.asarray(LIST_CASE["dims"], np.uint32)
+    counts, marked = [], []
+    for off in LIST_CASE["offsets"]:
+        c = np.zeros(offs.shape[0] - 1, dtype=np.uint64)
+        v = vox.copy()
+        assert R.ref_lists_collide_map(ids, v, offs, c.shape[0], bmap, dims, np.asarray(off, np.int32), c) == 0
+        counts.append(c)
+        marked.append(v)
+        print("list collide", off, c.tolist())
+    np.savez_compressed(os.path.join(out_dir, "ref_list_collide.npz"), offsets=np.asarray(LIST_CASE["offsets"]),
+                        counts=np.stack(counts), marked=np.stack(marked))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))
+    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden")
+    if len(sys.argv) > 2 and sys.argv[2] == "lists":
+        R = oracle.ref_lib()
+        assert R is not None and R.ref_available(), "reference kernels not built or no GPU"
+        os.makedirs(out, exist_ok=True)
+        make_list_fixture(R, out)
+    else:
+        main(out)

@@ -51,3 +51,31 @@ def test_oracle_collision_matches_reference_kernel():
     oracle.bvm_insert(b, dims, 1.0, pb, 33)
     assert oracle.bvm_collide(a, b) == int(f["count"])
     assert np.array_equal(a, f["marked"])
+
+
+def test_oracle_list_collision_matches_reference_kernel():
+    """The oracle's list-vs-map restatement against the reference's own
+    kernelCollideWithVoxelMap: per-list counts and the collision marks left
+    in the list voxels, at four map offsets (one list entry per id; ids beyond
+    the map and free-only voxels included)."""
+    from golden_cases import LIST_CASE, linear_offset, list_inputs
+
+    path = os.path.join(HERE, "ref_list_collide.npz")
+    if not os.path.exists(path):
+        pytest.skip("fixture not generated")
+    f = np.load(path)
+    bmap, ids, vox, offs = list_inputs(LIST_CASE)
+    dims = LIST_CASE["dims"]
+    assert [tuple(o) for o in f["offsets"]] == [tuple(o) for o in LIST_CASE["offsets"]]
+    for k, off in enumerate(LIST_CASE["offsets"]):
+        lin = linear_offset(dims, off)
+        v = vox.copy()
+        got = []
+        for l in range(offs.shape[0] - 1):
+            a, b = int(offs[l]), int(offs[l + 1])
+            seg = v[a * 32:b * 32].copy()
+            got.append(oracle.list_collide_map(ids[a:b], seg, bmap, lin, True))
+            v[a * 32:b * 32] = seg
+        assert got == [int(c) for c in f["counts"][k]], off
+        assert np.array_equal(v, f["marked"][k]), off
+    assert int(f["counts"].sum()) > 0
