@@ -400,7 +400,9 @@ def section_c4(hbm_peak):
 
     ms_trl = _time(traj_loop, 1, warm=1)
     bytes_fb = 48 + 60
-    return {"workload": "256^3 map; 1M points trilinear fwd+bwd; 512 x 64 waypoints x 56 spheres hinge cost + adjoint",
+    errors = c4_errors(dvm, sc, pts, arm, workloads)
+    return {"errors_vs_fp64": errors,
+            "workload": "256^3 map; 1M points trilinear fwd+bwd; 512 x 64 waypoints x 56 spheres hinge cost + adjoint",
             "trilinear_fwd_bwd_ms": round(ms_fb, 4), "trilinear_queries_with_grad_per_s": round(n / ms_fb * 1e3, 1),
             "query_launch_shape": {"threads": qcfg["threads"], "blocks_per_sm": qcfg["blocks_per_sm"],
                                    "fwd_bwd_ms_at_256x16": round(ms_fb_default, 4)},
@@ -409,6 +411,49 @@ def section_c4(hbm_peak):
             "traj_fwd_bwd_ms": round(ms_tr, 4),
             "traj_sphere_evals_with_grad_per_s": round(B * T * arm.n_spheres / ms_tr * 1e3, 1),
             "traj_per_trajectory_loop_ms": round(ms_trl, 2), "traj_speedup_vs_loop": round(ms_trl / ms_tr, 1)}
+
+
+def c4_errors(dvm, sc, pts, arm, workloads):
+    """Accuracy of the C4 queries (checker leg, outside every timed region):
+    FP32 results against the FP64 oracle restatements of the same functions.
+    Distances in voxel units; spatial gradients d(distance)/d(position)
+    (dimensionless, so also voxel per voxel); the trajectory adjoint relative
+    to the summed moment arms it is multiplied with (gcost * sum |z_k x
+    (c_s - o_k)|_1 over the active spheres), i.e. in the same units as the
+    spatial gradient."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    edt = dvm.data().cpu().numpy().view(np.uint32).copy()
+    sample = pts[::5]  # 200k of the 1M points
+    d32, g32 = dvm.trilinear(sample)
+    xyz = sample.cpu().numpy()
+    d64, g64 = oracle.trilinear64(edt, sc.dims, sc.side, xyz)
+    derr = np.abs(d32.cpu().numpy().astype(np.float64) - d64) / sc.side
+    u = xyz.astype(np.float64) / np.float64(np.float32(sc.side)) - 0.5
+    fr = u - np.floor(u)
+    off_face = ~np.any((fr < 1e-6) | (fr > 1 - 1e-6), axis=1)  # the gradient jumps across cell faces
+    gerr = np.abs(g32.cpu().numpy().astype(np.float64) - g64)[off_face]
+    spec = workloads.arm_spec()
+    q = workloads.c4_trajectories(16, 64)
+    gcost = np.ones(q.shape[0], dtype=np.float32)
+    cost32 = dvm.traj_cost(arm, torch.as_tensor(q).cuda(), 0.05).cpu().numpy().astype(np.float64)
+    gq = dvm.traj_cost_backward(arm, torch.as_tensor(q).cuda(), 0.05,
+                                torch.as_tensor(gcost).cuda()).cpu().numpy().astype(np.float64)
+    cost64 = oracle.traj_cost64(edt, sc.dims, sc.side, spec, q, 0.05)
+    g64q, scale, gap = oracle.traj_cost_grad64(edt, sc.dims, sc.side, spec, q, 0.05, gcost)
+    ok = np.broadcast_to((gap > 1e-6)[..., None], g64q.shape) & (scale > 0)
+    rel = np.abs(gq - g64q)[ok] / scale[ok]
+    return {
+        "trilinear_points": int(xyz.shape[0]),
+        "trilinear_err_max_vox": float(derr.max()), "trilinear_err_rms_vox": float(np.sqrt((derr ** 2).mean())),
+        "grad_err_max": float(gerr.max()), "grad_err_rms": float(np.sqrt((gerr ** 2).mean())),
+        "traj_cost_err_max_m": float(np.abs(cost32 - cost64).max()),
+        "traj_cost_err_rel_max": float((np.abs(cost32 - cost64) / np.maximum(np.abs(cost64), 1e-30)).max()),
+        "traj_adjoint_err_per_moment_arm_max": float(rel.max()),
+        "traj_adjoint_err_per_moment_arm_rms": float(np.sqrt((rel ** 2).mean())),
+        "traj_trajectories": int(q.shape[0]),
+    }
 
 
 def section_c5(hbm_peak):

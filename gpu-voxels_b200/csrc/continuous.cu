@@ -113,7 +113,7 @@ __device__ __forceinline__ void warp_fk(const gvx_arm& arm, const float* q, Warp
 }
 
 // Sphere centre in FP64 (the distance query splits it into cell and fraction
-// in double; only the adjoint's moment arms use it rounded to float).
+// in double, and the adjoint's moment arms use it as it is).
 __device__ __forceinline__ void sphere_centre(const gvx_arm& arm, const WarpFK& fk, int s, double c[3]) {
   const int j = arm.link[s];
   const double t = arm.t[s];
@@ -183,13 +183,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_kernel(MapView 
 //   d cost / d q_k = -grad d(c_s) . (z_k x (c_s - o_k))   for k <= j,
 // which sums per joint to -z_k . (M_k - o_k x G_k) with suffix sums over links
 // M_k = sum c_s x g_s, G_k = sum g_s.  One warp per waypoint, FK recomputed.
+// The moment sums run in FP64: M_k and o_k x G_k are of the order of the
+// arm's reach while their difference is of the order of the lever arm, so
+// FP32 sums would lose that ratio in relative accuracy; the spatial gradients
+// g_s stay FP32 (the trilinear query's own precision).
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapView m, gvx_arm arm,
                                                                            const float* __restrict__ q, uint64_t n_traj,
                                                                            uint32_t n_wp, float margin,
                                                                            const float* __restrict__ gcost,
                                                                            float* __restrict__ gq) {
   __shared__ WarpFK s_fk[kWarpsPerBlock];
-  __shared__ float s_link[kWarpsPerBlock][GVX_MAX_JOINTS][6];
+  __shared__ double s_link[kWarpsPerBlock][GVX_MAX_JOINTS][6];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int J = arm.n_joints;
   const uint64_t n_items = n_traj * n_wp;
@@ -199,18 +203,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapV
     warp_fk(arm, q + item * J, s_fk[warp]);
     for (int j = 0; j < J; ++j) {
       // per-link sums of c x g and g over this lane's active spheres
-      float mc[3] = {0.f, 0.f, 0.f}, gg[3] = {0.f, 0.f, 0.f};
+      double mc[3] = {0.0, 0.0, 0.0}, gg[3] = {0.0, 0.0, 0.0};
       for (int s = lane; s < arm.n_spheres; s += 32) {
         if (arm.link[s] != j) continue;
         double c[3];
         sphere_centre(arm, s_fk[warp], s, c);
         const Tri t = trilinear(m, c[0], c[1], c[2]);
         if (margin - (t.d * m.side - arm.r[s]) > 0.0f) {
-          const float cx = (float)c[0], cy = (float)c[1], cz = (float)c[2];
-          mc[0] += cy * t.gz - cz * t.gy;
-          mc[1] += cz * t.gx - cx * t.gz;
-          mc[2] += cx * t.gy - cy * t.gx;
-          gg[0] += t.gx; gg[1] += t.gy; gg[2] += t.gz;
+          const double gx = t.gx, gy = t.gy, gz = t.gz;
+          mc[0] += c[1] * gz - c[2] * gy;
+          mc[1] += c[2] * gx - c[0] * gz;
+          mc[2] += c[0] * gy - c[1] * gx;
+          gg[0] += gx; gg[1] += gy; gg[2] += gz;
         }
       }
 #pragma unroll
@@ -228,7 +232,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapV
     __syncwarp();
     if (lane == 0) {
       const float g = __ldg(gcost + traj);
-      float M[3] = {0.f, 0.f, 0.f}, G[3] = {0.f, 0.f, 0.f};
+      double M[3] = {0.0, 0.0, 0.0}, G[3] = {0.0, 0.0, 0.0};
       for (int k = J - 1; k >= 0; --k) {
         for (int i = 0; i < 3; ++i) { M[i] += s_link[warp][k][i]; G[i] += s_link[warp][k][3 + i]; }
         const double* o = s_fk[warp].o[k];

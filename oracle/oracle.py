@@ -470,7 +470,9 @@ def sphere_centres64(arm: dict, q: np.ndarray) -> np.ndarray:
     link j spans the origins of F_j = base*A_0*...*A_{j-1} and F_{j+1}."""
     q = np.asarray(q, dtype=np.float64)
     J = arm["n_joints"]
-    F = np.broadcast_to(np.asarray(arm["base"], dtype=np.float64).reshape(4, 4), q.shape[:-1] + (4, 4)).copy()
+    # every arm parameter as the device holds it (float32), then FP64
+    F = np.broadcast_to(np.asarray(arm["base"], dtype=np.float32).astype(np.float64).reshape(4, 4),
+                        q.shape[:-1] + (4, 4)).copy()
     origins = [F[..., :3, 3].copy()]
     for j in range(J):
         A = dh_matrix64(float(np.float32(arm["theta"][j])), float(np.float32(arm["d"][j])),
@@ -499,3 +501,57 @@ def traj_cost64(vmap, dims, side, arm, q, margin) -> np.ndarray:
     r = np.asarray(arm["r"], dtype=np.float32).astype(np.float64)
     clear = d.reshape(shp[:-1]) - r
     return np.maximum(0.0, float(np.float32(margin)) - clear).sum(axis=(-1, -2))
+
+
+def arm_frames64(arm: dict, q: np.ndarray):
+    """FP64 chain of KinematicChain::setConfiguration (KinematicChain.cu:104-124):
+    -> (origins o_0..o_J [..., J+1, 3], joint axes z_0..z_{J-1} [..., J, 3]);
+    joint j turns about z_j (third column of F_j) through o_j."""
+    q = np.asarray(q, dtype=np.float64)
+    J = arm["n_joints"]
+    F = np.broadcast_to(np.asarray(arm["base"], dtype=np.float32).astype(np.float64).reshape(4, 4),
+                        q.shape[:-1] + (4, 4)).copy()
+    origins, axes = [F[..., :3, 3].copy()], []
+    for j in range(J):
+        axes.append(F[..., :3, 2].copy())
+        A = dh_matrix64(float(np.float32(arm["theta"][j])), float(np.float32(arm["d"][j])),
+                        float(np.float32(arm["a"][j])), float(np.float32(arm["alpha"][j])), q[..., j])
+        F = F @ A
+        origins.append(F[..., :3, 3].copy())
+    return np.stack(origins, axis=-2), np.stack(axes, axis=-2)
+
+
+def traj_cost_grad64(vmap, dims, side, arm, q, margin, gcost):
+    """Analytic FP64 adjoint of traj_cost64 (TEST INFRASTRUCTURE).
+
+    For an active sphere s (margin - (d(c_s) - r_s) > 0) on link j,
+    d cost / d q_k = -grad d(c_s) . (z_k x (c_s - o_k)) for every k <= j.
+    Returns (grad [B, W, J] = gcost[b] * d cost_b / d q, scale [B, W, J] =
+    gcost[b] * sum over active spheres on links >= k of |z_k x (c_s - o_k)|_1,
+    gap [B, W] = the smallest |margin - clearance| of the waypoint's spheres).
+    `scale` times a bound on the spatial gradient's component error bounds the
+    adjoint's error; `gap` tells waypoints whose active set a rounding could flip.
+    """
+    q = np.asarray(q, dtype=np.float64)
+    B, W, J = q.shape
+    O, Z = arm_frames64(arm, q)                                   # [B,W,J+1,3], [B,W,J,3]
+    link = np.asarray(arm["link"], dtype=np.int64)
+    t = np.asarray(arm["t"], dtype=np.float32).astype(np.float64)[:, None]
+    C = O[..., link, :] + t * (O[..., link + 1, :] - O[..., link, :])   # [B,W,S,3]
+    d, g = trilinear64(vmap, dims, side, C.reshape(-1, 3))
+    S = C.shape[2]
+    d = d.reshape(B, W, S)
+    g = g.reshape(B, W, S, 3)
+    r = np.asarray(arm["r"], dtype=np.float32).astype(np.float64)
+    m = float(np.float32(margin))
+    gap_all = m - (d - r)
+    active = gap_all > 0
+    gc = np.asarray(gcost, dtype=np.float64)[:, None, None]
+    grad = np.zeros((B, W, J))
+    scale = np.zeros((B, W, J))
+    for k in range(J):
+        on = active & (link[None, None, :] >= k)                   # spheres moved by joint k
+        lever = np.cross(Z[..., k, None, :], C - O[..., k, None, :])  # z_k x (c_s - o_k)
+        grad[..., k] = -(np.einsum("bwsi,bwsi->bws", g, lever) * on).sum(-1)
+        scale[..., k] = (np.abs(lever).sum(-1) * on).sum(-1)
+    return grad * gc, scale * gc, np.abs(gap_all).min(-1)
