@@ -420,6 +420,16 @@ gvx_status gvx_bvm_collide(gvx_bvm* self, const gvx_bvm* other, const int32_t of
                      "collideWith(BitVectorVoxelMap)");
 }
 
+gvx_status gvx_bvm_collide_pvm(gvx_bvm* self, const gvx_pvm* other, float coll_threshold, const int32_t offset[3],
+                               int mark, uint64_t* d_count, gvx_stream stream) {
+  if (self == nullptr || other == nullptr || d_count == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(self->dims, other->dims)) return fail(GVX_ERR_INVALID_ARG, "maps differ in dimensions");
+  return cuda_status(launch_bvm_collide_pvm(self->d_vox, other->d_vox, num_voxels(self->dims),
+                                            linear_offset(self->dims, offset), prob_threshold(coll_threshold), mark,
+                                            reinterpret_cast<unsigned long long*>(d_count), as_stream(stream)),
+                     "collideWith(ProbVoxelMap)");
+}
+
 /* ---- typed collisions ---------------------------------------------------- */
 
 gvx_status gvx_bvm_collide_types(gvx_bvm* self, const gvx_bvm* other, uint64_t* d_count, uint8_t* d_types,
@@ -520,6 +530,9 @@ gvx_status gvx_blist_destroy(gvx_blist* l) {
   if (l == nullptr) return GVX_OK;
   if (l->d_ids) cudaFree(l->d_ids);
   if (l->d_vox) cudaFree(l->d_vox);
+  if (l->d_ids2) cudaFree(l->d_ids2);
+  if (l->d_vox2) cudaFree(l->d_vox2);
+  if (l->d_work) cudaFree(l->d_work);
   delete l;
   return GVX_OK;
 }
@@ -623,12 +636,35 @@ __global__ void list_merge_kernel(const uint32_t* __restrict__ keys, const uint3
   }
 }
 
-struct DevBuf {
-  void* p = nullptr;
-  ~DevBuf() { if (p) cudaFree(p); }
-  cudaError_t alloc(size_t bytes) { return cudaMalloc(&p, bytes ? bytes : 16); }
-  template <class T> T* as() { return static_cast<T*>(p); }
-};
+// Grow-only device buffer: reallocated (contents dropped) only when `need`
+// exceeds what it holds, then with headroom so slowly growing inputs
+// reallocate rarely.  cudaFree waits for work still using the old buffer.
+cudaError_t grow(void** p, size_t* have, size_t need) {
+  if (need <= *have && *p != nullptr) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  const size_t bytes = std::max<size_t>(need + need / 4, 4096);
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess) *have = bytes;
+  return e;
+}
+
+// Spare list storage for at least `cap` entries (the merged list's target).
+cudaError_t blist_spare(gvx_blist* l, uint64_t cap) {
+  if (cap <= l->cap2 && l->d_ids2 != nullptr) return cudaSuccess;
+  size_t have_i = 0, have_v = 0;
+  void* ids = l->d_ids2;
+  void* vox = l->d_vox2;
+  cudaError_t e = grow(&ids, &have_i, cap * sizeof(uint32_t));
+  if (e == cudaSuccess) e = grow(&vox, &have_v, cap * kBitVoxelBytes);
+  l->d_ids2 = static_cast<uint32_t*>(ids);
+  l->d_vox2 = static_cast<uint8_t*>(vox);
+  l->cap2 = e == cudaSuccess ? std::min<uint64_t>(have_i / sizeof(uint32_t), have_v / kBitVoxelBytes) : 0;
+  return e;
+}
+
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 }  // namespace
 }  // namespace gvx
@@ -642,51 +678,48 @@ gvx_status gvx_blist_insert_points(gvx_blist* l, const float* d_xyz, uint64_t n,
   cudaStream_t s = as_stream(stream);
   const uint64_t total = l->n + n;
   if (total >= 0xFFFFFFFFull) return fail(GVX_ERR_OUT_OF_DOMAIN, "list too long");
-  DevBuf keys, vals, keys2, vals2, head, pos, tmp, out_ids, out_vox;
-  cudaError_t e = keys.alloc(total * 4);
-  if (e == cudaSuccess) e = vals.alloc(total * 4);
-  if (e == cudaSuccess) e = keys2.alloc(total * 4);
-  if (e == cudaSuccess) e = vals2.alloc(total * 4);
-  if (e == cudaSuccess) e = head.alloc(total * 4);
-  if (e == cudaSuccess) e = pos.alloc(total * 4);
-  if (e != cudaSuccess) return cuda_status(e, "list insert buffers");
+  // work area: keys, vals, sorted keys, sorted vals, run heads, run positions
+  // (total words each), then CUB's temporary storage
+  size_t sort_bytes = 0, scan_bytes = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                                  (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)total, 0, 32, s);
+  if (e == cudaSuccess)
+    e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)total, s);
+  if (e != cudaSuccess) return cuda_status(e, "list sort sizing");
+  const size_t arr = align256(total * 4);
+  if ((e = grow(&l->d_work, &l->work_bytes, 6 * arr + align256(std::max(sort_bytes, scan_bytes)))) != cudaSuccess)
+    return cuda_status(e, "list insert buffers");
+  char* w = static_cast<char*>(l->d_work);
+  uint32_t* keys = reinterpret_cast<uint32_t*>(w);
+  uint32_t* vals = reinterpret_cast<uint32_t*>(w + arr);
+  uint32_t* keys2 = reinterpret_cast<uint32_t*>(w + 2 * arr);
+  uint32_t* vals2 = reinterpret_cast<uint32_t*>(w + 3 * arr);
+  uint32_t* head = reinterpret_cast<uint32_t*>(w + 4 * arr);
+  uint32_t* pos = reinterpret_cast<uint32_t*>(w + 5 * arr);
+  void* tmp = w + 6 * arr;
   const unsigned blocks = (unsigned)std::min<uint64_t>((total + 255) / 256, 4096);
-  list_keys_kernel<<<blocks, 256, 0, s>>>(d_xyz, n, l->ref, l->side, l->d_ids, l->n, keys.as<uint32_t>(), vals.as<uint32_t>());
-  size_t tmp_bytes = 0, scan_bytes = 0;
-  e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys.as<uint32_t>(), keys2.as<uint32_t>(), vals.as<uint32_t>(),
-                                      vals2.as<uint32_t>(), (int64_t)total, 0, 32, s);
-  if (e == cudaSuccess)
-    e = cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, head.as<uint32_t>(), pos.as<uint32_t>(), (int64_t)total, s);
-  if (e == cudaSuccess) e = tmp.alloc(std::max(tmp_bytes, scan_bytes));
-  if (e == cudaSuccess)
-    e = cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, keys.as<uint32_t>(), keys2.as<uint32_t>(), vals.as<uint32_t>(),
-                                        vals2.as<uint32_t>(), (int64_t)total, 0, 32, s);
+  list_keys_kernel<<<blocks, 256, 0, s>>>(d_xyz, n, l->ref, l->side, l->d_ids, l->n, keys, vals);
+  e = cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, keys, keys2, vals, vals2, (int64_t)total, 0, 32, s);
   if (e != cudaSuccess) return cuda_status(e, "list sort");
-  list_heads_kernel<<<blocks, 256, 0, s>>>(keys2.as<uint32_t>(), total, head.as<uint32_t>());
-  e = cub::DeviceScan::ExclusiveSum(tmp.p, scan_bytes, head.as<uint32_t>(), pos.as<uint32_t>(), (int64_t)total, s);
+  list_heads_kernel<<<blocks, 256, 0, s>>>(keys2, total, head);
+  e = cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, head, pos, (int64_t)total, s);
   uint32_t last_head = 0, last_pos = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&last_head, head.as<uint32_t>() + total - 1, 4, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&last_pos, pos.as<uint32_t>() + total - 1, 4, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&last_head, head + total - 1, 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&last_pos, pos + total - 1, 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the merged list's length sizes its storage
   if (e != cudaSuccess) return cuda_status(e, "list scan");
   const uint64_t n_out = (uint64_t)last_pos + last_head;
-  e = out_ids.alloc(n_out * 4);
-  if (e == cudaSuccess) e = out_vox.alloc(n_out * kBitVoxelBytes);
-  if (e != cudaSuccess) return cuda_status(e, "list output");
-  list_merge_kernel<<<blocks, 256, 0, s>>>(keys2.as<uint32_t>(), vals2.as<uint32_t>(), total, head.as<uint32_t>(),
-                                           pos.as<uint32_t>(), reinterpret_cast<const uint32_t*>(l->d_vox), l->n, meaning,
-                                           out_ids.as<uint32_t>(), out_vox.as<uint32_t>());
+  if ((e = blist_spare(l, n_out)) != cudaSuccess) return cuda_status(e, "list output");
+  list_merge_kernel<<<blocks, 256, 0, s>>>(keys2, vals2, total, head, pos, reinterpret_cast<const uint32_t*>(l->d_vox),
+                                           l->n, meaning, l->d_ids2, reinterpret_cast<uint32_t*>(l->d_vox2));
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // blocking, as the reference's insert
   if (e != cudaSuccess) return cuda_status(e, "list merge");
-  if (l->d_ids) cudaFree(l->d_ids);
-  if (l->d_vox) cudaFree(l->d_vox);
-  l->d_ids = out_ids.as<uint32_t>();
-  l->d_vox = out_vox.as<uint8_t>();
-  out_ids.p = nullptr;
-  out_vox.p = nullptr;
+  // the merged list becomes the list; the old storage is the next call's spare
+  std::swap(l->d_ids, l->d_ids2);
+  std::swap(l->d_vox, l->d_vox2);
+  std::swap(l->cap, l->cap2);
   l->n = n_out;
-  l->cap = n_out;
   return GVX_OK;
 }
 
@@ -806,6 +839,17 @@ gvx_status gvx_blist_collide_bvm(gvx_blist* l, const gvx_bvm* map, const int32_t
                                              linear_offset(map->dims, offset), mark,
                                              reinterpret_cast<unsigned long long*>(d_count), as_stream(stream)),
                      "collideWith(BitVoxelList, BitVectorVoxelMap)");
+}
+
+gvx_status gvx_blist_collide_pvm(gvx_blist* l, const gvx_pvm* map, float coll_threshold, const int32_t offset[3],
+                                 int mark, uint64_t* d_count, gvx_stream stream) {
+  if (l == nullptr || map == nullptr || d_count == nullptr) return fail(GVX_ERR_INVALID_ARG, "null argument");
+  if (!same_dims(l->ref, map->dims))
+    return fail(GVX_ERR_INVALID_ARG, "the list's reference map dimensions differ from the colliding map's");
+  return cuda_status(launch_list_collide_pvm(l->d_ids, l->d_vox, l->n, map->d_vox, num_voxels(map->dims),
+                                             linear_offset(map->dims, offset), prob_threshold(coll_threshold), mark,
+                                             reinterpret_cast<unsigned long long*>(d_count), as_stream(stream)),
+                     "collideWith(BitVoxelList, ProbVoxelMap)");
 }
 
 gvx_status gvx_blist_collide_blist(const gvx_blist* l, const gvx_blist* other, const int32_t offset[3], uint64_t* d_count,

@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "gvx_internal.cuh"
 
@@ -163,6 +164,72 @@ __global__ void __launch_bounds__(256) lists_collide_map_kernel(const uint32_t* 
   }
 }
 
+// BitVoxel test of a whole 32-byte voxel: a meaning other than eBVM_FREE.
+__device__ __forceinline__ bool bitvoxel_occupied(const uint32_t* v) {
+  const uint4 lo = __ldg(reinterpret_cast<const uint4*>(v));
+  const uint4 hi = __ldg(reinterpret_cast<const uint4*>(v) + 1);
+  return ((lo.x & ~1u) | lo.y | lo.z | lo.w | hi.x | hi.y | hi.z | hi.w) != 0u;
+}
+
+// kernelCollideVoxelMapsDebug with DefaultCollider::collide(BitVoxel,
+// ProbabilisticVoxel) (GV/voxelmap/kernels/VoxelMapOperations.hpp:129-184,
+// GV/voxel/DefaultCollider.hpp:68-73): count i where other[i]'s occupancy
+// reaches `thr` and self[i+off] holds a meaning other than eBVM_FREE; mark
+// self with eBVM_COLLISION.  A thread takes 4 consecutive occupancy bytes
+// (one 4-byte load, a warp reads 128 contiguous bytes) and loads the 32-byte
+// BitVoxel only where the occupancy passes.
+__global__ void __launch_bounds__(256) bvm_collide_pvm_kernel(uint32_t* __restrict__ self, const int8_t* __restrict__ other,
+                                                              uint64_t n, int64_t off, int thr, int mark,
+                                                              unsigned long long* __restrict__ count) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long hits = 0;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t * 4 < n; t += stride) {
+    const uint64_t i0 = t * 4;
+    int p[4];
+    if (i0 + 4 <= n) {
+      const char4 c = __ldcs(reinterpret_cast<const char4*>(other) + t);
+      p[0] = c.x; p[1] = c.y; p[2] = c.z; p[3] = c.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) p[k] = i0 + k < n ? (int)other[i0 + k] : INT_MIN;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t j = (int64_t)(i0 + k) + off;
+      if (p[k] >= thr && j >= 0 && j < (int64_t)n) {
+        uint32_t* v = self + (uint64_t)j * kBitVoxelWords;
+        if (bitvoxel_occupied(v)) {
+          ++hits;
+          if (mark) v[0] |= 1u << kCollisionBit;
+        }
+      }
+    }
+  }
+  block_count_add(hits, count);
+}
+
+// kernelCollideWithVoxelMap with DefaultCollider::collide(BitVoxel,
+// ProbabilisticVoxel) (GV/voxellist/kernels/VoxelListOperations.hpp:146-197):
+// entry k collides when map voxel ids[k] + off lies in the map, its occupancy
+// reaches `thr` and the entry holds a meaning other than eBVM_FREE.
+__global__ void __launch_bounds__(256) list_collide_pvm_kernel(const uint32_t* __restrict__ ids, uint32_t* __restrict__ lvox,
+                                                               uint64_t n, const int8_t* __restrict__ map, uint64_t map_n,
+                                                               int64_t off, int thr, int mark,
+                                                               unsigned long long* __restrict__ count) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long hits = 0;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+    const int64_t j = (int64_t)__ldg(ids + k) + off;
+    if (j < 0 || j >= (int64_t)map_n || (int)__ldg(map + j) < thr) continue;
+    uint32_t* v = lvox + k * kBitVoxelWords;
+    if (bitvoxel_occupied(v)) {
+      ++hits;
+      if (mark) v[0] |= 1u << kCollisionBit;
+    }
+  }
+  block_count_add(hits, count);
+}
+
 // collideVoxellists (GV/voxellist/TemplateVoxelList.hpp:231-289): count of ids
 // of `a` found in the sorted list `b` (thrust::binary_search semantics).
 __global__ void __launch_bounds__(256) list_collide_list_kernel(const uint32_t* __restrict__ a, uint64_t na,
@@ -217,6 +284,25 @@ cudaError_t launch_lists_collide_map(const uint32_t* d_ids, uint8_t* d_vox, cons
   lists_collide_map_kernel<<<grid_cap(n_total, 8 * 16), 256, 0, s>>>(
       d_ids, reinterpret_cast<uint32_t*>(d_vox), d_offsets, n_lists, n_total, reinterpret_cast<const uint32_t*>(d_map),
       map_n, mark, d_counts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bvm_collide_pvm(uint8_t* d_self, const int8_t* d_other, uint64_t n, int64_t off, int thr, int mark,
+                                   unsigned long long* d_count, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess || n == 0) return e;
+  bvm_collide_pvm_kernel<<<grid_cap((n + 3) / 4, 256), 256, 0, s>>>(reinterpret_cast<uint32_t*>(d_self), d_other, n, off,
+                                                                    thr, mark, d_count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_list_collide_pvm(const uint32_t* d_ids, uint8_t* d_list_vox, uint64_t n, const int8_t* d_map,
+                                    uint64_t map_n, int64_t off, int thr, int mark, unsigned long long* d_count,
+                                    cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess || n == 0) return e;
+  list_collide_pvm_kernel<<<grid_cap(n, 256), 256, 0, s>>>(d_ids, reinterpret_cast<uint32_t*>(d_list_vox), n, d_map,
+                                                           map_n, off, thr, mark, d_count);
   return cudaGetLastError();
 }
 

@@ -77,6 +77,14 @@ struct gvx_blist {
   uint8_t* d_vox;
   uint64_t n;
   uint64_t cap;
+  // insertPointCloud's device buffers, kept with the list and grown only
+  // when a call needs more: the sort/scan work area and the spare storage
+  // the merged list is written to (then swapped with d_ids / d_vox).
+  void* d_work = nullptr;
+  size_t work_bytes = 0;
+  uint32_t* d_ids2 = nullptr;
+  uint8_t* d_vox2 = nullptr;
+  uint64_t cap2 = 0;
 };
 
 namespace gvx {
@@ -221,6 +229,13 @@ cudaError_t launch_dvm_sqdist(const uint32_t* d_vox, gvx_dims d, const uint32_t*
 cudaError_t launch_dvm_sqdist_map(const uint32_t* d_vox, gvx_dims d, int32_t* d_out, cudaStream_t s);
 cudaError_t launch_bvm_collide(uint8_t* d_self, const uint8_t* d_other, uint64_t n, int64_t off, int mark,
                                unsigned long long* d_count, cudaStream_t s);
+// ProbVoxelMap forms of collideWith (DefaultCollider): thr is the occupancy
+// threshold as a Probability (floatToProbability, clamped).
+cudaError_t launch_bvm_collide_pvm(uint8_t* d_self, const int8_t* d_other, uint64_t n, int64_t off, int thr, int mark,
+                                   unsigned long long* d_count, cudaStream_t s);
+cudaError_t launch_list_collide_pvm(const uint32_t* d_ids, uint8_t* d_list_vox, uint64_t n, const int8_t* d_map,
+                                    uint64_t map_n, int64_t off, int thr, int mark, unsigned long long* d_count,
+                                    cudaStream_t s);
 cudaError_t launch_list_collide_map(const uint32_t* d_ids, uint8_t* d_list_vox, uint64_t n, const uint8_t* d_map,
                                     uint64_t map_n, int64_t off, int mark, unsigned long long* d_count, cudaStream_t s);
 cudaError_t launch_lists_collide_map(const uint32_t* d_ids, uint8_t* d_vox, const uint64_t* d_offsets, uint32_t n_lists,

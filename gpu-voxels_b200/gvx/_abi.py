@@ -115,6 +115,8 @@ PROTOTYPES = {
     "gvx_bvm_clear": [_vp, _vp],
     "gvx_bvm_insert_points": [_vp, _vp, _u64, _u32, _vp, _vp],
     "gvx_bvm_clear_bits": [_vp, _vp, _vp],
+    "gvx_bvm_collide_pvm": [_vp, _vp, _f, _vp, ctypes.c_int, _vp, _vp],
+    "gvx_blist_collide_pvm": [_vp, _vp, _f, _vp, ctypes.c_int, _vp, _vp],
     "gvx_blist_clear_bits": [_vp, _vp, _vp],
     "gvx_blist_shift_swept_volume_ids": [_vp, _u32, _vp],
     "gvx_bvm_shift_swept_volume_ids": [_vp, _u32, _vp],

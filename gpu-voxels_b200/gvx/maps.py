@@ -395,14 +395,23 @@ class BitVectorVoxelMap:
         p = _dev_points(points)
         call("gvx_bvm_insert_points", self._h, _ptr(p), p.shape[0], int(meaning), _ptr(outside), _stream())
 
-    def collideWithAsync(self, other: "BitVectorVoxelMap", offset=(0, 0, 0), mark: bool = True,
-                         out: Optional[torch.Tensor] = None) -> torch.Tensor:
+    def collideWithAsync(self, other, offset=(0, 0, 0), mark: bool = True, out: Optional[torch.Tensor] = None,
+                         coll_threshold: float = 1.0) -> torch.Tensor:
+        """Stream-ordered collideWith: the count lands in `out` (int64 CUDA)."""
         out = self._count if out is None else out
-        call("gvx_bvm_collide", self._h, other.handle, _offset(offset), 1 if mark else 0, _ptr(out), _stream())
+        if isinstance(other, BitVectorVoxelMap):
+            call("gvx_bvm_collide", self._h, other.handle, _offset(offset), 1 if mark else 0, _ptr(out), _stream())
+        elif isinstance(other, ProbVoxelMap):
+            call("gvx_bvm_collide_pvm", self._h, other.handle, float(coll_threshold), _offset(offset),
+                 1 if mark else 0, _ptr(out), _stream())
+        else:
+            raise TypeError("collideWith expects a BitVectorVoxelMap or a ProbVoxelMap")
         return out
 
-    def collideWith(self, other: "BitVectorVoxelMap", coll_threshold: float = 1.0, offset=(0, 0, 0)) -> int:
-        return int(self.collideWithAsync(other, offset).item())
+    def collideWith(self, other, coll_threshold: float = 1.0, offset=(0, 0, 0)) -> int:
+        """BitVoxelMap::collideWith(BitVectorVoxelMap* | ProbVoxelMap*, coll_threshold, offset):
+        the threshold applies to a ProbVoxelMap's occupancy (DefaultCollider)."""
+        return int(self.collideWithAsync(other, offset, coll_threshold=coll_threshold).item())
 
     def collideWithTypes(self, other, coll_threshold: float = 1.0, offset=(0, 0, 0)):
         """-> (count, types uint8[32]): swept-volume types colliding with a
@@ -528,10 +537,13 @@ class BitVectorVoxelList:
         if isinstance(other, BitVectorVoxelMap):
             call("gvx_blist_collide_bvm", self._h, other.handle, _offset(offset), 1 if mark else 0, _ptr(self._count),
                  _stream())
+        elif isinstance(other, ProbVoxelMap):
+            call("gvx_blist_collide_pvm", self._h, other.handle, float(coll_threshold), _offset(offset),
+                 1 if mark else 0, _ptr(self._count), _stream())
         elif isinstance(other, BitVectorVoxelList):
             call("gvx_blist_collide_blist", self._h, other.handle, _offset(offset), _ptr(self._count), _stream())
         else:
-            raise TypeError("collideWith expects a BitVectorVoxelMap or BitVectorVoxelList")
+            raise TypeError("collideWith expects a BitVectorVoxelMap, ProbVoxelMap or BitVectorVoxelList")
         return int(self._count.item())
 
     def collideWithTypes(self, other, coll_threshold: float = 1.0, offset=(0, 0, 0)):

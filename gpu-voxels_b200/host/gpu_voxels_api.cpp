@@ -34,26 +34,6 @@ void require(gvx_status st, const char* what) {
 
 gvx_dims to_dims(const Vector3ui& d) { return gvx_dims{d.x, d.y, d.z}; }
 
-// Temporary device copy of a host point cloud.
-struct DevicePoints {
-  float* p = nullptr;
-  explicit DevicePoints(const std::vector<Vector3f>& pts) {
-    if (pts.empty()) return;
-    if (cudaMalloc(&p, pts.size() * sizeof(Vector3f)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
-    cudaMemcpy(p, pts.data(), pts.size() * sizeof(Vector3f), cudaMemcpyHostToDevice);
-  }
-  ~DevicePoints() { if (p) cudaFree(p); }
-};
-
-template <class T>
-struct DeviceArray {
-  T* p = nullptr;
-  size_t n = 0;
-  explicit DeviceArray(size_t count) : n(count) {
-    if (count && cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
-  }
-  ~DeviceArray() { if (p) cudaFree(p); }
-};
 
 // TemplateVoxelMap::clone (GV/voxelmap/TemplateVoxelMap.hpp:1101-1120).
 void clone_voxels(GpuVoxelsMap& self, const GpuVoxelsMap& other, void* dst, const void* src, size_t bytes) {
@@ -72,6 +52,37 @@ void clone_voxels(GpuVoxelsMap& self, const GpuVoxelsMap& other, void* dst, cons
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// GpuVoxelsMap: the staging area of the host-vector overloads
+// ---------------------------------------------------------------------------
+GpuVoxelsMap::~GpuVoxelsMap() {
+  if (m_staging) cudaFree(m_staging);
+}
+
+void* GpuVoxelsMap::stagingBuffer(size_t bytes) const {
+  if (bytes <= m_staging_bytes && m_staging != nullptr) return m_staging;
+  if (m_staging) cudaFree(m_staging);  // waits for work still reading it
+  m_staging = nullptr;
+  m_staging_bytes = 0;
+  const size_t cap = std::max<size_t>(bytes + bytes / 4, 1 << 16);
+  if (cudaMalloc(&m_staging, cap) != cudaSuccess) {
+    m_staging = nullptr;
+    throw std::runtime_error("gpu_voxels: cudaMalloc of the staging area failed");
+  }
+  m_staging_bytes = cap;
+  return m_staging;
+}
+
+const Vector3f* GpuVoxelsMap::stagePoints(const std::vector<Vector3f>& points) const {
+  if (points.empty()) return nullptr;
+  void* d = stagingBuffer(points.size() * sizeof(Vector3f));
+  // synchronous copy on the legacy default stream: ordered after earlier
+  // default-stream work that read the area
+  if (cudaMemcpy(d, points.data(), points.size() * sizeof(Vector3f), cudaMemcpyHostToDevice) != cudaSuccess)
+    throw std::runtime_error("gpu_voxels: point cloud upload failed");
+  return static_cast<const Vector3f*>(d);
+}
 
 // ---------------------------------------------------------------------------
 // MetaPointCloud and the maps' generic insertMetaPointCloud
@@ -185,8 +196,7 @@ void ProbVoxelMap::clearMap() {
 
 void ProbVoxelMap::insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) {
   lock_guard g(m_mutex);
-  DevicePoints d(points);
-  insertPointCloud(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size(), voxel_meaning);
+  insertPointCloud(stagePoints(points), (uint32_t)points.size(), voxel_meaning);
   cudaDeviceSynchronize();
 }
 
@@ -243,8 +253,7 @@ void DistanceVoxelMap::clearMap() {
 
 void DistanceVoxelMap::insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) {
   lock_guard g(m_mutex);
-  DevicePoints d(points);
-  insertPointCloud(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size(), voxel_meaning);
+  insertPointCloud(stagePoints(points), (uint32_t)points.size(), voxel_meaning);
   cudaDeviceSynchronize();
 }
 
@@ -278,8 +287,7 @@ void DistanceVoxelMap::parallelBanding3D(uint32_t m1, uint32_t m2, uint32_t m3, 
 
 void DistanceVoxelMap::voxelizeAndTransform(const std::vector<Vector3f>& points) {
   lock_guard g(m_mutex);
-  DevicePoints d(points);
-  voxelizeAndTransform(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size());
+  voxelizeAndTransform(stagePoints(points), (uint32_t)points.size());
 }
 
 void DistanceVoxelMap::voxelizeAndTransform(const Vector3f* d_points, uint32_t size) {
@@ -356,25 +364,26 @@ void DistanceVoxelMap::gatherVoxelsByIndex(const uint32_t* b, const uint32_t* e,
   ok(gvx_dvm_gather(m_handle, b, (uint64_t)(e - b), reinterpret_cast<uint32_t*>(out), nullptr), "gatherVoxelsByIndex");
 }
 
-static void host_query(gvx_dvm* h, std::vector<uint32_t>& idx, std::vector<int32_t>& out, bool squared) {
+// Host-vector queries: ids and results share the map's staging area.
+static void host_query(gvx_dvm* h, void* stage, std::vector<uint32_t>& idx, std::vector<int32_t>& out, bool squared) {
   out.resize(idx.size());
   if (idx.empty()) return;
-  DeviceArray<uint32_t> di(idx.size());
-  DeviceArray<int32_t> dout(idx.size());
-  cudaMemcpy(di.p, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice);
-  gvx_status st = squared ? gvx_dvm_sqdist(h, di.p, idx.size(), dout.p, nullptr) : gvx_dvm_dist(h, di.p, idx.size(), dout.p, nullptr);
+  uint32_t* di = static_cast<uint32_t*>(stage);
+  int32_t* dout = reinterpret_cast<int32_t*>(static_cast<char*>(stage) + ((idx.size() * 4 + 255) & ~(size_t)255));
+  cudaMemcpy(di, idx.data(), idx.size() * 4, cudaMemcpyHostToDevice);
+  gvx_status st = squared ? gvx_dvm_sqdist(h, di, idx.size(), dout, nullptr) : gvx_dvm_dist(h, di, idx.size(), dout, nullptr);
   if (ok(st, squared ? "getSquaredDistancesToHost" : "getDistancesToHost"))
-    cudaMemcpy(out.data(), dout.p, idx.size() * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(out.data(), dout, idx.size() * 4, cudaMemcpyDeviceToHost);
 }
 
 void DistanceVoxelMap::getSquaredDistancesToHost(std::vector<uint32_t>& indices, std::vector<int32_t>& output) {
   lock_guard g(m_mutex);
-  host_query(m_handle, indices, output, true);
+  host_query(m_handle, stagingBuffer(2 * ((indices.size() * 4 + 255) & ~(size_t)255) + 256), indices, output, true);
 }
 
 void DistanceVoxelMap::getDistancesToHost(std::vector<uint32_t>& indices, std::vector<int32_t>& output) {
   lock_guard g(m_mutex);
-  host_query(m_handle, indices, output, false);
+  host_query(m_handle, stagingBuffer(2 * ((indices.size() * 4 + 255) & ~(size_t)255) + 256), indices, output, false);
 }
 
 DistanceVoxel::pba_dist_t DistanceVoxelMap::getSquaredObstacleDistance(uint32_t x, uint32_t y, uint32_t z) {
@@ -444,8 +453,7 @@ void BitVoxelMap<length>::clearMap() {
 template <size_t length>
 void BitVoxelMap<length>::insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) {
   lock_guard g(m_mutex);
-  DevicePoints d(points);
-  insertPointCloud(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size(), voxel_meaning);
+  insertPointCloud(stagePoints(points), (uint32_t)points.size(), voxel_meaning);
   cudaDeviceSynchronize();
 }
 
@@ -469,6 +477,19 @@ size_t BitVoxelMap<length>::collideWith(const BitVoxelMap<length>* map, float, c
   std::lock_guard<std::recursive_timed_mutex> g2(map->m_mutex, std::adopt_lock);
   const int32_t off[3] = {offset.x, offset.y, offset.z};
   if (!ok(gvx_bvm_collide(m_handle, map->m_handle, off, 1, m_dev_count, nullptr), "collideWith")) return 0;
+  uint64_t count = 0;
+  cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
+  return (size_t)count;
+}
+
+template <size_t length>
+size_t BitVoxelMap<length>::collideWith(const ProbVoxelMap* map, float coll_threshold, const Vector3i& offset) {
+  std::lock(m_mutex, map->mutexRef());
+  std::lock_guard<std::recursive_timed_mutex> g1(m_mutex, std::adopt_lock);
+  std::lock_guard<std::recursive_timed_mutex> g2(map->mutexRef(), std::adopt_lock);
+  const int32_t off[3] = {offset.x, offset.y, offset.z};
+  if (!ok(gvx_bvm_collide_pvm(m_handle, map->handle(), coll_threshold, off, 1, m_dev_count, nullptr), "collideWith"))
+    return 0;
   uint64_t count = 0;
   cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
   return (size_t)count;
@@ -619,8 +640,7 @@ void BitVoxelList<length, ID>::clearMap() {
 template <size_t length, class ID>
 void BitVoxelList<length, ID>::insertPointCloud(const std::vector<Vector3f>& points, BitVoxelMeaning voxel_meaning) {
   lock_guard g(m_mutex);
-  DevicePoints d(points);
-  insertPointCloud(reinterpret_cast<const Vector3f*>(d.p), (uint32_t)points.size(), voxel_meaning);
+  insertPointCloud(stagePoints(points), (uint32_t)points.size(), voxel_meaning);
 }
 
 template <size_t length, class ID>
@@ -653,6 +673,22 @@ size_t BitVoxelList<length, ID>::collideWith(const voxelmap::BitVoxelMap<length>
   lock_guard g(m_mutex);
   const int32_t off[3] = {offset.x, offset.y, offset.z};
   if (!ok(gvx_blist_collide_bvm(m_handle, map->handle(), off, 1, m_dev_count, nullptr), "collideWith")) return 0;
+  uint64_t count = 0;
+  cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
+  return (size_t)count;
+}
+
+template <size_t length, class ID>
+size_t BitVoxelList<length, ID>::collideWith(const voxelmap::ProbVoxelMap* map, float coll_threshold,
+                                             const Vector3i& offset) {
+  if (map->getDimensions() != m_dim) {
+    std::fprintf(stderr, "gpu_voxels: list reference dims differ from the map's; not checking collisions\n");
+    return SSIZE_MAX;
+  }
+  lock_guard g(m_mutex);
+  const int32_t off[3] = {offset.x, offset.y, offset.z};
+  if (!ok(gvx_blist_collide_pvm(m_handle, map->handle(), coll_threshold, off, 1, m_dev_count, nullptr), "collideWith"))
+    return 0;
   uint64_t count = 0;
   cudaMemcpy(&count, m_dev_count, sizeof(count), cudaMemcpyDeviceToHost);
   return (size_t)count;
@@ -834,9 +870,12 @@ void GpuVoxels::initialize(uint32_t dim_x, uint32_t dim_y, uint32_t dim_z, float
   m_voxel_side_length = voxel_side_length;
 }
 
-bool GpuVoxels::addMap(const MapType map_type, const std::string& map_name) {
+GpuVoxelsMapSharedPtr GpuVoxels::addMap(const MapType map_type, const std::string& map_name) {
   std::lock_guard<std::recursive_mutex> g(m_mutex);
-  if (m_managed_maps.count(map_name)) return false;
+  if (m_managed_maps.count(map_name)) {
+    std::fprintf(stderr, "gpu_voxels: a map named '%s' exists already\n", map_name.c_str());
+    return GpuVoxelsMapSharedPtr();
+  }
   GpuVoxelsMapSharedPtr map;
   try {
     switch (map_type) {
@@ -846,14 +885,14 @@ bool GpuVoxels::addMap(const MapType map_type, const std::string& map_name) {
       case MT_PROBAB_VOXELMAP: map.reset(new voxelmap::ProbVoxelMap(m_dim, m_voxel_side_length, map_type)); break;
       default:
         std::fprintf(stderr, "gpu_voxels: map type %d is outside the distance-field collision path\n", (int)map_type);
-        return false;
+        return GpuVoxelsMapSharedPtr();
     }
   } catch (const std::exception& e) {
     std::fprintf(stderr, "%s\n", e.what());
-    return false;
+    return GpuVoxelsMapSharedPtr();
   }
   m_managed_maps[map_name] = map;
-  return true;
+  return map;
 }
 
 bool GpuVoxels::visualizeMap(const std::string& map_name, const bool /*force_repaint*/) {

@@ -30,8 +30,10 @@ class GpuVoxels {
   ~GpuVoxels();
 
   void initialize(uint32_t dim_x, uint32_t dim_y, uint32_t dim_z, float voxel_side_length);
-  // addMap (GV/GpuVoxels.cpp:164-302); false for a duplicate name or an unsupported type.
-  bool addMap(const MapType map_type, const std::string& map_name);
+  // addMap (GV/GpuVoxels.cpp:164-302): the new map, or an empty pointer for
+  // a duplicate name or a type outside this library (the reference returns
+  // an empty pointer for both too).
+  GpuVoxelsMapSharedPtr addMap(const MapType map_type, const std::string& map_name);
   bool delMap(const std::string& map_name);
   GpuVoxelsMapSharedPtr getMap(const std::string& map_name);
   bool clearMap(const std::string& map_name);

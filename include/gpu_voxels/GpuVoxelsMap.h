@@ -21,7 +21,7 @@ class GpuVoxelsMap {
  public:
   GpuVoxelsMap(MapType type, const Vector3ui& dims, float voxel_side_length)
       : m_map_type(type), m_dim(dims), m_voxel_side_length(voxel_side_length) {}
-  virtual ~GpuVoxelsMap() {}
+  virtual ~GpuVoxelsMap();
 
   GpuVoxelsMap(const GpuVoxelsMap&) = delete;
   GpuVoxelsMap& operator=(const GpuVoxelsMap&) = delete;
@@ -74,10 +74,21 @@ class GpuVoxelsMap {
 
  protected:
   typedef std::lock_guard<std::recursive_timed_mutex> lock_guard;
+  // Device staging area of the host-vector overloads (point clouds, query
+  // ids and results): enlarged when a call needs more than it holds and
+  // otherwise reused, so repeated calls allocate no device memory.  Freed
+  // with the map.  Callers hold the map's mutex.
+  void* stagingBuffer(size_t bytes) const;
+  // A host point cloud copied into the staging area (nullptr when empty).
+  const Vector3f* stagePoints(const std::vector<Vector3f>& points) const;
   MapType m_map_type;
   Vector3ui m_dim;
   float m_voxel_side_length;
   mutable std::recursive_timed_mutex m_mutex;
+
+ private:
+  mutable void* m_staging = nullptr;
+  mutable size_t m_staging_bytes = 0;
 };
 
 typedef std::shared_ptr<GpuVoxelsMap> GpuVoxelsMapSharedPtr;

@@ -34,6 +34,14 @@ class BitVoxelList : public GpuVoxelsMap {
   // Returns SSIZE_MAX when the map's dims differ from the list's reference dims.
   size_t collideWith(const voxelmap::BitVoxelMap<length>* map, float coll_threshold = 1.0,
                      const Vector3i& offset = Vector3i());
+  // collideWith(const ProbVoxelMap*) (GV/voxellist/BitVoxelList.hpp:63-69,
+  // DefaultCollider GV/voxel/DefaultCollider.hpp:68-73): entries whose map
+  // voxel (id + offset, inside the map) has an occupancy reaching
+  // floatToProbability(coll_threshold) and that hold a meaning other than
+  // eBVM_FREE; they get eBVM_COLLISION.  SSIZE_MAX when the map's dims
+  // differ from the list's reference dims.
+  size_t collideWith(const voxelmap::ProbVoxelMap* map, float coll_threshold = 1.0,
+                     const Vector3i& offset = Vector3i());
   // collideWith(const BitVectorVoxelList*) (GV/voxellist/BitVoxelList.hpp:79-92):
   // number of this list's ids present in `other`; offsets are not supported (returns 0).
   size_t collideWith(const BitVoxelList<length, VoxelIDType>* other, float coll_threshold = 1.0,

@@ -36,6 +36,12 @@ class BitVoxelMap : public GpuVoxelsMap {
   // voxels where both maps hold a meaning other than eBVM_FREE, this map
   // shifted by `offset`; colliding voxels of this map get eBVM_COLLISION.
   size_t collideWith(const BitVoxelMap<length>* map, float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
+  // collideWith(const ProbVoxelMap*, float, const Vector3i&) (GV/voxelmap/BitVoxelMap.hpp:205-210,
+  // DefaultCollider GV/voxel/DefaultCollider.hpp:68-73): voxels where the
+  // ProbVoxelMap's occupancy reaches floatToProbability(coll_threshold) and
+  // this map (shifted by `offset`) holds a meaning other than eBVM_FREE;
+  // colliding voxels of this map get eBVM_COLLISION.
+  size_t collideWith(const ProbVoxelMap* map, float coll_threshold = 1.0, const Vector3i& offset = Vector3i());
 
   // collideWithTypes (GV/voxelmap/BitVoxelMap.hpp:212-224): the swept-volume
   // types colliding with `map` (with a ProbVoxelMap: this map's types where

@@ -327,6 +327,18 @@ GVX_API gvx_status gvx_bvm_insert_meta_points_self_coll(gvx_bvm *m, const float 
 GVX_API gvx_status gvx_bvm_collide(gvx_bvm *self, const gvx_bvm *other, const int32_t offset[3], int mark, uint64_t *d_count,
                            gvx_stream stream);
 
+/* Replaces BitVoxelMap::collideWith(const ProbVoxelMap*, coll_threshold, offset)
+ * (GV/voxelmap/BitVoxelMap.hpp:205-210 -> TemplateVoxelMap.hpp:588-621 ->
+ * kernelCollideVoxelMapsDebug, DefaultCollider::collide(BitVoxel,
+ * ProbabilisticVoxel), GV/voxel/DefaultCollider.hpp:68-73).  Counts voxels i
+ * where other[i]'s occupancy reaches floatToProbability(coll_threshold)
+ * (clamped to [0, 1], GV/voxel/ProbabilisticVoxel.h:40-45) and self[i+off]
+ * holds a meaning other than eBVM_FREE; pairs whose shifted index leaves the
+ * map are skipped; with mark != 0 colliding self voxels get eBVM_COLLISION.
+ * *d_count (device uint64) receives the count. */
+GVX_API gvx_status gvx_bvm_collide_pvm(gvx_bvm *self, const gvx_pvm *other, float coll_threshold,
+                                       const int32_t offset[3], int mark, uint64_t *d_count, gvx_stream stream);
+
 /* ---- Typed collisions ------------------------------------------------------ */
 /* Every call overwrites *d_count (device uint64) with the number of colliding
  * voxels / entries and, where given, d_types (device, 32 bytes = one
@@ -466,6 +478,16 @@ GVX_API gvx_status gvx_blist_set(gvx_blist *l, const uint32_t *d_ids, const uint
  * reference dims (the reference returns SSIZE_MAX). */
 GVX_API gvx_status gvx_blist_collide_bvm(gvx_blist *l, const gvx_bvm *map, const int32_t offset[3], int mark, uint64_t *d_count,
                                  gvx_stream stream);
+/* Replaces BitVoxelList::collideWith(const ProbVoxelMap*, coll_threshold, offset)
+ * (GV/voxellist/BitVoxelList.hpp:63-69 -> TemplateVoxelList.hpp:1170-1213 ->
+ * kernelCollideWithVoxelMap, VoxelListOperations.hpp:146-197, DefaultCollider
+ * GV/voxel/DefaultCollider.hpp:68-73): entry i collides when map voxel
+ * ids[i] + offset lies in the map, its occupancy reaches
+ * floatToProbability(coll_threshold) and the entry holds a meaning other
+ * than eBVM_FREE; with mark != 0 colliding entries get eBVM_COLLISION.
+ * GVX_ERR_INVALID_ARG when the map's dims differ from the list's reference dims. */
+GVX_API gvx_status gvx_blist_collide_pvm(gvx_blist *l, const gvx_pvm *map, float coll_threshold,
+                                         const int32_t offset[3], int mark, uint64_t *d_count, gvx_stream stream);
 /* Replaces BitVoxelList::collideWith(const BitVectorVoxelList*, thr, offset)
  * (BitVoxelList.hpp:79-92 -> collideVoxellists, TemplateVoxelList.hpp:231-289):
  * number of this list's ids present in `other`.  Non-zero offsets are

@@ -564,6 +564,45 @@ void orc_lists_collide_map_omp(const uint32_t *ids, const uint8_t *list_voxels, 
   }
 }
 
+/* BitVoxelMap::collideWith(const ProbVoxelMap*), GV/voxelmap/BitVoxelMap.hpp:205-210
+ * -> collisionCheckWithCounterRelativeTransform (TemplateVoxelMap.hpp:588-621)
+ * -> kernelCollideVoxelMapsDebug (VoxelMapOperations.hpp:129-184) with
+ * DefaultCollider::collide(BitVoxel v1, ProbabilisticVoxel v2)
+ * (GV/voxel/DefaultCollider.hpp:68-73): v2.occupancy >= thr && !v1.noneButEmpty;
+ * v1 = self[i + offset], v2 = other[i]; thr = floatToProbability(coll_threshold). */
+uint64_t orc_bvm_collide_pvm(uint8_t *self, const int8_t *other, uint64_t n, int64_t offset_linear, int thr, int mark) {
+  uint64_t count = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    int64_t j = (int64_t)i + offset_linear;
+    if (j < 0 || j >= (int64_t)n) continue;
+    uint8_t *a = self + (uint64_t)j * BITVOXEL_BYTES;
+    if ((int)other[i] >= thr && !bv_none_but_empty(a)) {
+      ++count;
+      if (mark) a[EBVM_COLLISION >> 3] |= (uint8_t)(1u << (EBVM_COLLISION & 7));
+    }
+  }
+  return count;
+}
+
+/* BitVoxelList::collideWith(const ProbVoxelMap*), GV/voxellist/BitVoxelList.hpp:63-69
+ * -> collisionCheckWithCollider (TemplateVoxelList.hpp:1170-1213) ->
+ * kernelCollideWithVoxelMap (VoxelListOperations.hpp:146-197), same collider:
+ * entry i meets map voxel ids[i] + offset when that lies in the map. */
+uint64_t orc_list_collide_pvm(const uint32_t *ids, uint8_t *list_voxels, uint64_t n, const int8_t *map, uint64_t map_n,
+                              int64_t offset_linear, int thr, int mark) {
+  uint64_t count = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    int64_t j = (int64_t)ids[i] + offset_linear;
+    if (j < 0 || j >= (int64_t)map_n) continue;
+    uint8_t *a = list_voxels + i * BITVOXEL_BYTES;
+    if ((int)map[j] >= thr && !bv_none_but_empty(a)) {
+      ++count;
+      if (mark) a[EBVM_COLLISION >> 3] |= (uint8_t)(1u << (EBVM_COLLISION & 7));
+    }
+  }
+  return count;
+}
+
 /* BitVoxelList::collideWith(BitVectorVoxelList*) -> collideVoxellists,
  * GV/voxellist/TemplateVoxelList.hpp:231-289: number of this list's ids
  * present in the other (sorted) list, thrust::binary_search semantics. */

@@ -96,6 +96,11 @@ def lib():
         _i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
         L.orc_pvm_insert.argtypes = [_i8p, _u32p, ctypes.c_float, _f32p, ctypes.c_uint64, ctypes.c_uint32]
         L.orc_pvm_insert.restype = ctypes.c_int
+        L.orc_bvm_collide_pvm.argtypes = [_u8p, _i8p, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int, ctypes.c_int]
+        L.orc_bvm_collide_pvm.restype = ctypes.c_uint64
+        L.orc_list_collide_pvm.argtypes = [_u32p, _u8p, ctypes.c_uint64, _i8p, ctypes.c_uint64, ctypes.c_int64,
+                                           ctypes.c_int, ctypes.c_int]
+        L.orc_list_collide_pvm.restype = ctypes.c_uint64
         L.orc_float_to_probability.argtypes = [ctypes.c_float]
         L.orc_float_to_probability.restype = ctypes.c_int
         L.orc_dvm_merge_occupied.argtypes = [_u32p, _i8p, _u32p, _u32p, ctypes.c_float]
@@ -140,6 +145,13 @@ def ref_lib():
         R.ref_lists_collide_map.argtypes = [_u32p, _u8p, _u64p, ctypes.c_uint32, _u8p, _u32p,
                                             np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS"), _u64p]
         R.ref_lists_collide_map.restype = ctypes.c_int
+        _i8 = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+        _i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+        R.ref_bvm_collide_pvm.argtypes = [_u8p, _i8, ctypes.c_uint32, ctypes.c_float, ctypes.POINTER(ctypes.c_uint64)]
+        R.ref_bvm_collide_pvm.restype = ctypes.c_int
+        R.ref_list_collide_pvm.argtypes = [_u32p, _u8p, ctypes.c_uint32, _i8, _u32p, _i32, ctypes.c_float,
+                                           ctypes.POINTER(ctypes.c_uint64)]
+        R.ref_list_collide_pvm.restype = ctypes.c_int
         _REF = R
     return _REF
 
@@ -334,6 +346,21 @@ def pvm_insert(pmap: np.ndarray, dims, side: float, xyz, meaning: int) -> bool:
 
 def float_to_probability(val: float) -> int:
     return int(lib().orc_float_to_probability(float(val)))
+
+
+def bvm_collide_pvm(self_map: np.ndarray, pmap: np.ndarray, coll_threshold: float = 1.0, offset_linear: int = 0,
+                    mark: bool = True) -> int:
+    """BitVoxelMap::collideWith(const ProbVoxelMap*): marks self_map in place."""
+    return int(lib().orc_bvm_collide_pvm(self_map, pmap, pmap.shape[0], int(offset_linear),
+                                         float_to_probability(coll_threshold), 1 if mark else 0))
+
+
+def list_collide_pvm(ids, list_vox: np.ndarray, pmap: np.ndarray, coll_threshold: float = 1.0, offset_linear: int = 0,
+                     mark: bool = True) -> int:
+    """BitVoxelList::collideWith(const ProbVoxelMap*): marks list_vox in place."""
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    return int(lib().orc_list_collide_pvm(ids, list_vox, ids.shape[0], pmap, pmap.shape[0], int(offset_linear),
+                                          float_to_probability(coll_threshold), 1 if mark else 0))
 
 
 def dvm_merge_occupied(vmap: np.ndarray, pmap: np.ndarray, dims, offset=(0, 0, 0), threshold: float = 0.5) -> None:

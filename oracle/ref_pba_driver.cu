@@ -209,6 +209,79 @@ int ref_bvm_collide(uint8_t* h_self, const uint8_t* h_other, uint32_t nvox, uint
   return rc;
 }
 
+// kernelCollideVoxelMapsDebug with DefaultCollider(coll_threshold) on a
+// BitVectorVoxel map (self, marked) against a ProbVoxelMap (one int8
+// occupancy per voxel), as BitVoxelMap::collideWith(const ProbVoxelMap*)
+// (GV/voxelmap/BitVoxelMap.hpp:205-210) launches it; zero offset.
+int ref_bvm_collide_pvm(uint8_t* h_self, const int8_t* h_other, uint32_t nvox, float coll_threshold, uint64_t* count) {
+  static_assert(sizeof(ProbabilisticVoxel) == 1, "one occupancy byte per voxel");
+  BitVectorVoxel* a = nullptr;
+  ProbabilisticVoxel* b = nullptr;
+  uint16_t* res = nullptr;
+  const size_t bytes = (size_t)nvox * sizeof(BitVectorVoxel);
+  if (cudaMalloc(&a, bytes) || cudaMalloc(&b, nvox) || cudaMalloc(&res, cMAX_NR_OF_BLOCKS * sizeof(uint16_t))) return -1;
+  cudaMemcpy(a, h_self, bytes, cudaMemcpyHostToDevice);
+  cudaMemcpy(b, h_other, nvox, cudaMemcpyHostToDevice);
+  cudaMemset(res, 0, cMAX_NR_OF_BLOCKS * sizeof(uint16_t));
+  uint32_t blocks, threads;
+  linear_load(nvox, &blocks, &threads);
+  DefaultCollider collider(coll_threshold);
+  kernelCollideVoxelMapsDebug<<<blocks, threads>>>(a, nvox, b, collider, res);
+  int rc = check(cudaDeviceSynchronize());
+  std::vector<uint16_t> h(cMAX_NR_OF_BLOCKS);
+  cudaMemcpy(h.data(), res, cMAX_NR_OF_BLOCKS * sizeof(uint16_t), cudaMemcpyDeviceToHost);
+  uint64_t c = 0;
+  for (uint32_t i = 0; i < blocks; ++i) c += h[i];
+  *count = c;
+  if (!rc) rc = check(cudaMemcpy(h_self, a, bytes, cudaMemcpyDeviceToHost));
+  cudaFree(a);
+  cudaFree(b);
+  cudaFree(res);
+  return rc;
+}
+
+// kernelCollideWithVoxelMap<BitVectorVoxel, ProbabilisticVoxel, DefaultCollider>
+// for one list, as BitVoxelList::collideWith(const ProbVoxelMap*)
+// (GV/voxellist/BitVoxelList.hpp:63-69 -> TemplateVoxelList.hpp:1170-1213)
+// launches it; the list voxels receive the marks.
+int ref_list_collide_pvm(const uint32_t* h_ids, uint8_t* h_list_vox, uint32_t n, const int8_t* h_map,
+                         const uint32_t dims[3], const int32_t offset[3], float coll_threshold, uint64_t* h_count) {
+  const Vector3ui dim(dims[0], dims[1], dims[2]);
+  const Vector3i off(offset[0], offset[1], offset[2]);
+  const uint64_t nvox = (uint64_t)dims[0] * dims[1] * dims[2];
+  ProbabilisticVoxel* map = nullptr;
+  BitVectorVoxel* lvox = nullptr;
+  MapVoxelID* ids = nullptr;
+  uint16_t* res = nullptr;
+  if (cudaMalloc(&map, nvox) || cudaMalloc(&lvox, ((size_t)n + 1) * sizeof(BitVectorVoxel)) ||
+      cudaMalloc(&ids, ((size_t)n + 1) * sizeof(MapVoxelID)) || cudaMalloc(&res, cMAX_NR_OF_BLOCKS * sizeof(uint16_t))) {
+    cudaFree(map); cudaFree(lvox); cudaFree(ids); cudaFree(res);
+    return -1;
+  }
+  int rc = check(cudaMemcpy(map, h_map, nvox, cudaMemcpyHostToDevice));
+  if (!rc) rc = check(cudaMemcpy(lvox, h_list_vox, (size_t)n * sizeof(BitVectorVoxel), cudaMemcpyHostToDevice));
+  if (!rc) rc = check(cudaMemcpy(ids, h_ids, (size_t)n * sizeof(MapVoxelID), cudaMemcpyHostToDevice));
+  uint32_t blocks, threads;
+  linear_load(n, &blocks, &threads);
+  DefaultCollider collider(coll_threshold);
+  if (!rc) {
+    voxellist::kernelCollideWithVoxelMap<<<blocks, threads, sizeof(BitVectorVoxel) * cMAX_THREADS_PER_BLOCK>>>(
+        ids, lvox, n, map, dim, collider, off, res);
+    rc = check(cudaDeviceSynchronize());
+  }
+  std::vector<uint16_t> h(cMAX_NR_OF_BLOCKS);
+  if (!rc) rc = check(cudaMemcpy(h.data(), res, blocks * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+  uint64_t c = 0;
+  for (uint32_t i = 0; i < blocks && !rc; ++i) c += h[i];
+  *h_count = c;
+  if (!rc) rc = check(cudaMemcpy(h_list_vox, lvox, (size_t)n * sizeof(BitVectorVoxel), cudaMemcpyDeviceToHost));
+  cudaFree(map);
+  cudaFree(lvox);
+  cudaFree(ids);
+  cudaFree(res);
+  return rc;
+}
+
 // kernelCollideWithVoxelMap<BitVectorVoxel, BitVectorVoxel, DefaultCollider>
 // (GV/voxellist/kernels/VoxelListOperations.hpp:146-197) over many lists
 // against one BitVectorVoxelMap, one launch per list with the launch sizing of

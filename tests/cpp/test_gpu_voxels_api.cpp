@@ -19,7 +19,7 @@ using namespace gpu_voxels;
 static int g_failures = 0;
 #define CHECK(cond, name)                                            \
   do {                                                               \
-    const bool _ok = (cond);                                         \
+    const bool _ok = static_cast<bool>(cond);                        \
     std::printf("%s %s\n", _ok ? "PASS" : "FAIL", name);             \
     if (!_ok) ++g_failures;                                          \
   } while (0)
@@ -215,6 +215,73 @@ static void prob_map_to_distance_map() {
   gvl->delMap("myDistanceMap");
 }
 
+// addMap returning the map (GV/GpuVoxels.cpp:164-302) and collideWith
+// against a ProbVoxelMap (BitVoxelMap.hpp:205-210, BitVoxelList.hpp:63-69):
+// the expected counts are recomputed on the host from the maps' contents
+// with DefaultCollider's rule (occupancy >= floatToProbability(threshold)
+// and a BitVoxel meaning other than eBVM_FREE).
+static void prob_map_collisions() {
+  GpuVoxelsSharedPtr gvl = GpuVoxels::getInstance();
+  gvl->initialize(96, 80, 72, 1.0f);
+  voxelmap::ProbVoxelMap* env = gvl->addMap(MT_PROBAB_VOXELMAP, "env")->as<voxelmap::ProbVoxelMap>();
+  BitVectorVoxelMap* robot = gvl->addMap(MT_BITVECTOR_VOXELMAP, "robot")->as<BitVectorVoxelMap>();
+  BitVectorVoxelList* robot_list = gvl->addMap(MT_BITVECTOR_VOXELLIST, "robot_list")->as<BitVectorVoxelList>();
+  CHECK(env && robot && robot_list, "addMap(...)->as<T>() returns the new maps");
+  CHECK(!gvl->addMap(MT_PROBAB_VOXELMAP, "env"), "addMap with a taken name: empty pointer");
+  CHECK(!gvl->addMap(MT_BITVECTOR_OCTREE, "tree"), "addMap of a type outside the library: empty pointer");
+  env->insertPointCloud(box_of_points(Vector3f(20, 20, 20), Vector3f(40, 40, 40), 0.9f), eBVM_MAX_OCC_PROB);
+  env->insertPointCloud(box_of_points(Vector3f(30, 30, 30), Vector3f(50, 50, 50), 0.9f), eBVM_MAX_FREE_PROB);
+  const std::vector<Vector3f> arm = box_of_points(Vector3f(25, 25, 25), Vector3f(45, 45, 45), 0.9f);
+  robot->insertPointCloud(arm, BitVoxelMeaning(7));
+  robot_list->insertPointCloud(arm, BitVoxelMeaning(7));
+  const size_t n = robot->getVoxelMapSize();
+  std::vector<int8_t> occ(n);
+  cudaMemcpy(occ.data(), env->getDeviceDataPtr(), n, cudaMemcpyDeviceToHost);
+  std::vector<uint8_t> bits(n * 32);
+  cudaMemcpy(bits.data(), robot->getDeviceDataPtr(), n * 32, cudaMemcpyDeviceToHost);
+  auto expect = [&](float thr, int dx) {
+    float t = std::max(std::min(1.0f, thr), 0.0f);
+    const int p = (int)(int8_t)(t * (127.0f - (-127.0f)) + (-127.0f));
+    size_t c = 0;
+    for (size_t i = 0; i < n; ++i) {
+      const int64_t j = (int64_t)i + dx;
+      if (j < 0 || j >= (int64_t)n || occ[i] < p) continue;
+      const uint8_t* v = &bits[(size_t)j * 32];
+      bool any = (v[0] & ~1u) != 0;
+      for (int k = 1; k < 32; ++k) any = any || v[k] != 0;
+      c += any;
+    }
+    return c;
+  };
+  // list entry at id meets map voxel id + dx
+  auto expect_list = [&](float thr, int dx) {
+    float t = std::max(std::min(1.0f, thr), 0.0f);
+    const int p = (int)(int8_t)(t * (127.0f - (-127.0f)) + (-127.0f));
+    size_t c = 0;
+    for (size_t id = 0; id < n; ++id) {
+      const uint8_t* v = &bits[id * 32];
+      bool any = (v[0] & ~1u) != 0;
+      for (int k = 1; k < 32; ++k) any = any || v[k] != 0;
+      const int64_t j = (int64_t)id + dx;
+      c += any && j >= 0 && j < (int64_t)n && occ[(size_t)j] >= p;
+    }
+    return c;
+  };
+  const size_t want = expect(0.55f, 0);
+  CHECK(want > 0 && want == expect_list(0.55f, 0), "prob-map collision scene overlaps");
+  CHECK(robot_list->collideWith(env, 0.55f) == want, "BitVoxelList::collideWith(ProbVoxelMap*)");
+  CHECK(robot_list->collideWith(env, 0.55f, Vector3i(-2, 1, 0)) == expect_list(0.55f, -2 + 96),
+        "BitVoxelList::collideWith(ProbVoxelMap*) with an offset");
+  CHECK(robot->collideWith(env, 0.55f, Vector3i(3, 0, 0)) == expect(0.55f, 3), "BitVoxelMap::collideWith(ProbVoxelMap*) offset 3");
+  CHECK(robot->collideWith(env, 2.0f) == expect(2.0f, 0), "BitVoxelMap::collideWith(ProbVoxelMap*) threshold clamped to 1");
+  CHECK(robot->collideWith(env, 0.55f) == want, "BitVoxelMap::collideWith(ProbVoxelMap*)");
+  voxelmap::ProbVoxelMap small(Vector3ui(8, 8, 8), 1.0f);
+  CHECK(robot_list->collideWith(&small, 0.55f) == (size_t)SSIZE_MAX, "list vs ProbVoxelMap with other dims: SSIZE_MAX");
+  gvl->delMap("env");
+  gvl->delMap("robot");
+  gvl->delMap("robot_list");
+}
+
 // Free-space bytes and the distance band -> BitVoxelList conversion
 // (DistanceVoxelMap::extract_distances, distance_map_converter) on one site.
 static void distance_consumers() {
@@ -400,6 +467,7 @@ int main() {
   distance_correctness();
   collisions();
   prob_map_to_distance_map();
+  prob_map_collisions();
   std::printf("%d failure(s)\n", g_failures);
   return g_failures;
 }
