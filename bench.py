@@ -13,8 +13,11 @@ sphere/trajectory queries with gradients, many uneven maps).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Multi-GPU: every rank runs its own independent map (weak scaling, no
-collective on the data path); time = max over ranks.
+Multi-GPU (one process per GPU): the headline is weak scaling -- every rank
+voxelises and transforms its own 512^3 map, no collective on the data path;
+the `sharded` section splits the independent units of configs C5 (64 uneven
+maps) and C3 (4096 lists) over the ranks by a cost-balanced partition and
+gathers the results on rank 0 (strong scaling).  Times = max over ranks.
 """
 from __future__ import annotations
 
@@ -523,6 +526,92 @@ def section_c5(hbm_peak):
             "bit_equal_to_loop": bool(exact and exact_q)}
 
 
+def section_sharded(ranks, steps: int, warmup: int):
+    """The independent units of the path split over the ranks (every rank
+    runs this; strong scaling: the total work is fixed as N grows).
+      c5: the 64 uneven maps, voxelise + EDT + 10k trilinear queries per map,
+          maps partitioned by voxel count; one Batch per rank.
+      c3: the 4096 swept-volume lists against the 256^3 scene map, lists
+          partitioned by length; one batched launch per rank.
+    Time = max over ranks of the device time of `steps` steps (barrier and
+    synchronize on both sides); the results are gathered on rank 0 after the
+    timed region and checked against a single-GPU run of all units there."""
+    import torch
+    import gvx
+    import workloads
+    from gvx import shard
+    from gvx.batch import Batch
+    dist = ranks.dist
+    out = {"scaling": "strong", "ranks": ranks.world}
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        ranks.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        ranks.barrier()
+        torch.cuda.synchronize()
+        return ranks.max(a.elapsed_time(b)) / steps
+
+    scenes = workloads.c5_maps()
+    rng = np.random.default_rng(11)
+    queries = [((0.5 + rng.random((10_000, 3)) * (np.asarray(s.dims) - 1)) * s.side).astype(np.float32) for s in scenes]
+    sb = shard.ShardedBatch(scenes, queries, dist)
+    ms = timed(sb.step)
+    full = sb.gather()
+    nvox = sum(int(np.prod(s.dims)) for s in scenes)
+    c5 = {"ms": round(ms, 4), "gvoxel_per_s": round(nvox / (ms / 1e3) / 1e9, 3), "maps_on_rank0": len(sb.mine),
+          "imbalance": round(shard.imbalance(sb.costs, sb.plan), 4)}
+    if ranks.rank == 0:  # the gathered results equal one GPU running every map (no collective here)
+        try:
+            maps = [gvx.DistanceVoxelMap(s.dims, s.side) for s in scenes]
+            b = Batch(maps)
+            pts = torch.as_tensor(np.concatenate([s.points for s in scenes]).astype(np.float32)).cuda()
+            offs = torch.as_tensor(np.concatenate([[0], np.cumsum([s.points.shape[0] for s in scenes])])
+                                   .astype(np.int64)).cuda()
+            b.voxelize_edt(pts, offs)
+            qm = torch.as_tensor(np.concatenate([np.full(q.shape[0], k, np.int32) for k, q in enumerate(queries)])).cuda()
+            d, g = b.query(torch.as_tensor(np.concatenate(queries)).cuda(), qm)
+            c5["equal_to_single_gpu"] = bool(torch.equal(full, torch.cat([d[:, None], g], 1)))
+            del maps, b
+        except Exception as exc:
+            c5["check_error"] = repr(exc)[:200]
+    del sb
+    torch.cuda.empty_cache()
+    out["c5_maps"] = c5
+
+    sc = workloads.c3_scene()
+    bmap = gvx.BitVectorVoxelMap(sc.dims, sc.side)
+    bmap.insertPointCloud(torch.as_tensor(sc.points).cuda(), 1)
+    ids, offs = workloads.c3_lists_device(workloads.list_lengths(), int(np.prod(sc.dims)))
+    owner = torch.repeat_interleave(torch.arange(offs.shape[0] - 1, device="cuda"), offs[1:] - offs[:-1])
+    meaning = 4 + owner % 200
+    vox = torch.zeros(ids.numel(), 32, dtype=torch.uint8, device="cuda")
+    vox.scatter_(1, (meaning // 8).unsqueeze(1), (1 << (meaning % 8)).to(torch.uint8).unsqueeze(1))
+    vox = vox.reshape(-1)
+    sl = shard.ShardedLists(ids, vox, offs.cpu().numpy(), bmap, dist)
+    ms = timed(sl.step)
+    counts = sl.gather()
+    c3 = {"ms": round(ms, 4), "list_ids_per_s": round(ids.numel() / (ms / 1e3), 1), "lists_on_rank0": len(sl.mine),
+          "imbalance": round(shard.imbalance(sl.lengths, sl.plan), 4)}
+    if ranks.rank == 0:
+        try:
+            c3["equal_to_single_gpu"] = bool(torch.equal(counts, gvx.lists_collide_map(ids, vox, offs, bmap)))
+        except Exception as exc:
+            c3["check_error"] = repr(exc)[:200]
+    out["c3_lists"] = c3
+    del sl, ids, vox, bmap
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_sections(args, hbm_peak, pts_host):
     import torch
     out = {}
@@ -751,6 +840,13 @@ def main():
         "gpu_launches": 3 * args.steps,  # occupancy insert, z sweep from bits, fused y->x sweep (+ 2 memsets)
         "clocks": clocks.summary(),
     }
+
+    # ---- the independent units split over the ranks (all ranks) ----------
+    if args.sections == "all" or "sharded" in args.sections.split(","):
+        try:
+            line["sharded"] = section_sharded(ranks, steps=max(3, min(args.steps, 20)), warmup=3)
+        except Exception as exc:  # reported, not fatal; every rank takes the same steps
+            line["sharded"] = {"error": repr(exc)[:300]}
 
     if rank == 0 and not args.no_baselines:
         # ---- gpu-voxels' own kernels on this GPU (oracle/_ref), same map ----
