@@ -641,8 +641,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--sections", default="all", help="comma list of extra sections or 'none'")
-    ap.add_argument("--map", default="c2", choices=["c2", "c3"],
-                    help="headline map: c2 = 512^3 depth scene (default), c3 = 256^3 box scene")
+    ap.add_argument("--map", default="c2", choices=["c2", "c2_352", "c3"],
+                    help="headline map: c2 = 512^3 depth scene (default), c2_352 = the same scene on a 352^3 map "
+                         "(7.3 mm voxels; profiling captures), c3 = 256^3 box scene")
+    ap.add_argument("--profile-sweeps", action="store_true",
+                    help="for ncu captures: insert the map, then launch the y sweep, the x sweep and the fused "
+                         "y->x sweep once each (16-row staging) and exit")
     ap.add_argument("--no-baselines", action="store_true", help="skip the CPU and reference-kernel baselines")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -668,8 +672,23 @@ def main():
     if args.map == "c3":  # the 256^3 @ 1 cm box scene (used for small profiling captures)
         sc = workloads.c3_scene()
         C2_DIMS, C2_SIDE, pts_host = sc.dims, sc.side, sc.points
+    elif args.map == "c2_352":  # the depth scene on a smaller map (profiling captures above L2 size)
+        C2_DIMS, C2_SIDE, pts_host = (352, 352, 352), 2.56 / 352, workloads.c2_points()
     else:
         pts_host = workloads.c2_points()
+    if args.profile_sweeps:
+        dvm = gvx.DistanceVoxelMap(C2_DIMS, C2_SIDE)
+        dvm.set_edt_config(16, 1)
+        pts = torch.as_tensor(pts_host).cuda()
+        for p in (1, 2, 3):  # edt_sweep<Y>, edt_sweep<X>, edt_sweep_yx
+            dvm.clearMap()
+            dvm.insertPointCloud(pts)
+            dvm.edt_pass(0)
+            dvm.edt_pass(p)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_sweeps": list(C2_DIMS)}))
+        ranks.close()
+        return
     pts = torch.as_tensor(pts_host).cuda()
     dvm = gvx.DistanceVoxelMap(C2_DIMS, C2_SIDE)
     nvox = int(np.prod(C2_DIMS))
