@@ -22,6 +22,7 @@ gathers the results on rank 0 (strong scaling).  Times = max over ranks.
 from __future__ import annotations
 
 import argparse
+import atexit
 import json
 import os
 import subprocess
@@ -51,15 +52,21 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling around the timed regions.
+
+    The sampler starts before the warm-up (nvidia-smi takes a few hundred ms
+    to deliver its first line) and stamps every sample with the host clock;
+    `window()` marks a timed region, and the summary uses the samples taken
+    inside the marked regions (or, if a region was shorter than the sampling
+    interval, the sample nearest to each region)."""
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
-        self._stop = threading.Event()
+        self.samples = []  # (host time, fields)
+        self.windows = []
         self._proc = None
 
-    def __enter__(self):
+    def start(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -69,6 +76,10 @@ class ClockSampler:
                                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            atexit.register(self.stop)  # never leave the sampler running
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 3.0:  # first line before the workload starts
+                time.sleep(0.02)
         except Exception:
             self._proc = None
         return self
@@ -77,25 +88,43 @@ class ClockSampler:
         for line in self._proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 8:
-                self.samples.append(parts)
+                self.samples.append((time.time(), parts))
 
-    def __exit__(self, *a):
+    def window(self):
+        """Context manager marking one timed region (host time, synchronised edges)."""
+        sampler = self
+
+        class _W:
+            def __enter__(self):
+                self.t0 = time.time()
+                return self
+
+            def __exit__(self, *a):
+                sampler.windows.append((self.t0, time.time()))
+
+        return _W()
+
+    def stop(self):
         if self._proc is not None:
             self._proc.terminate()
             try:
                 self._proc.wait(timeout=5)
             except Exception:
                 self._proc.kill()
+            self._proc = None
 
     def summary(self):
-        if not self.samples:
+        picked = [p for t, p in self.samples if any(a <= t <= b for a, b in self.windows)]
+        if not picked and self.samples and self.windows:
+            picked = [min(self.samples, key=lambda sp: min(abs(sp[0] - (a + b) / 2) for a, b in self.windows))[1]]
+        if not picked:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        sm = [float(s[1]) for s in picked if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in picked if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i].lower().startswith("active")})
+        reasons = sorted({names[i] for s in picked for i in range(4) if s[4 + i].lower().startswith("active")})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(picked), "timed_windows": len(self.windows)}
 
 
 def _traffic_from_profiles():
@@ -704,13 +733,14 @@ def main():
     dvm.clearMap()
     dvm.insertPointCloud(pts)
     edt_config = dvm.autotune()  # untimed: picks the sweep configuration for this map
+    clocks = ClockSampler(local).start()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
+    with clocks.window():
         ev0.record(stream)
         for _ in range(args.steps):
             step()
@@ -829,10 +859,12 @@ def main():
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ev0.record(stream)
-    e2e_pipelined(args.steps, start=ev0)
-    ev1.record(stream)
-    torch.cuda.synchronize()
+    with clocks.window():
+        ev0.record(stream)
+        e2e_pipelined(args.steps, start=ev0)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    clocks.stop()
     e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
     if not torch.equal(outs[(args.steps - 1) % 2], serial_out):
         raise RuntimeError("double-buffered end-to-end steps returned other distances than the serial steps")
