@@ -405,6 +405,17 @@ def section_c4(hbm_peak):
     ms_fb_default = _time(fwd_bwd, 20)
     qcfg = dvm.autotune_queries(pts, with_grad=False, force=True)
     ms_fb = _time(fwd_bwd, 20)
+    # the same points in cell order (z, y, x of the lower corner; sorted outside the timing):
+    # neighbouring threads then share corner voxels and cache lines
+    cell = torch.floor(pts / sc.side - 0.5).clamp_(min=0).to(torch.int64)
+    key = (cell[:, 2] * sc.dims[1] + cell[:, 1]) * sc.dims[0] + cell[:, 0]
+    pts_sorted = pts[torch.argsort(key)].contiguous()
+
+    def fwd_bwd_sorted():
+        dvm.trilinear(pts_sorted, with_grad=False)
+        return dvm.trilinear_backward(pts_sorted, gout)
+
+    ms_fb_sorted = _time(fwd_bwd_sorted, 20)
     p = pts.clone().requires_grad_(True)
 
     def autograd_step():
@@ -439,6 +450,7 @@ def section_c4(hbm_peak):
             "query_launch_shape": {"threads": qcfg["threads"], "blocks_per_sm": qcfg["blocks_per_sm"],
                                    "fwd_bwd_ms_at_256x16": round(ms_fb_default, 4)},
             "trilinear_achieved_gbs": round(bytes_fb * n / (ms_fb / 1e3) / 1e9, 1),
+            "trilinear_fwd_bwd_ms_cell_sorted": round(ms_fb_sorted, 4),
             "autograd_step_ms": round(ms_ag, 4),
             "traj_fwd_bwd_ms": round(ms_tr, 4),
             "traj_sphere_evals_with_grad_per_s": round(B * T * arm.n_spheres / ms_tr * 1e3, 1),

@@ -63,7 +63,8 @@ __global__ void batch_trilinear_kernel(const BatchMap* __restrict__ maps, const 
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const BatchMap bm = maps[__ldg(map_of + i)];
-    const MapView m{bm.vox, bm.X, bm.Y, bm.Z, bm.side};
+    const MapView m{bm.vox, bm.X, bm.Y, bm.Z, bm.side, (reinterpret_cast<uintptr_t>(bm.vox) & 15u) == 0,
+                    (uint64_t)bm.X * bm.Y * bm.Z};
     const Tri t = trilinear(m, __ldg(xyz + 3 * i), __ldg(xyz + 3 * i + 1), __ldg(xyz + 3 * i + 2));
     dist[i] = t.d * m.side;
     if (grad != nullptr) {

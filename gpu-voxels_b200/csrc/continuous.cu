@@ -253,7 +253,10 @@ unsigned blocks_for(uint64_t items, uint64_t per_block, uint64_t cap_per_sm) {
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((items + per_block - 1) / per_block, (uint64_t)sms() * cap_per_sm));
 }
 
-MapView view(const gvx_dvm* m) { return MapView{m->d_vox, (int)m->dims.x, (int)m->dims.y, (int)m->dims.z, m->side}; }
+MapView view(const gvx_dvm* m) {
+  return MapView{m->d_vox, (int)m->dims.x, (int)m->dims.y, (int)m->dims.z, m->side,
+                 (reinterpret_cast<uintptr_t>(m->d_vox) & 15u) == 0, num_voxels(m->dims)};
+}
 
 }  // namespace
 

@@ -19,14 +19,37 @@ struct MapView {
   const uint32_t* vox;
   int X, Y, Z;
   float side;
+  bool aligned16;  // vox on a 16-byte boundary (the corner-pair loads below need it)
+  uint64_t n;      // voxels in the map (a 16-byte word is read only when it lies inside)
 };
 
-__device__ __forceinline__ float corner_dist(const MapView& m, int i, int j, int k) {
-  const uint32_t v = __ldg(m.vox + ((uint64_t)k * m.Y + j) * m.X + i);
+// Distance (voxel units) from lattice point (i, j, k) to the site `v` holds.
+__device__ __forceinline__ float corner_value(uint32_t v, int i, int j, int k) {
   const int ox = (int)dv_x(v), oy = (int)dv_y(v), oz = (int)dv_z(v);
   if (ox == (int)kUninit || oy == (int)kUninit || oz == (int)kUninit) return sqrtf((float)kMaxObstacleDistance);
   const int dx = i - ox, dy = j - oy, dz = k - oz;
   return sqrtf((float)(dx * dx + dy * dy + dz * dz));
+}
+
+// The two corners (i0, j, k) and (i1, j, k) of a cell edge along x.  They
+// are neighbours in memory (i1 = i0 + 1, or i1 = i0 on a one-voxel axis);
+// when both lie in one aligned 16-byte word (3 of 4 positions) a single
+// 16-byte load fetches them, so a random-order query touches about 5 L1
+// lines per point instead of 8 -- the queries are bound by those gathers.
+__device__ __forceinline__ void corner_pair(const MapView& m, int i0, int i1, int j, int k, float& d0, float& d1) {
+  const uint64_t idx = ((uint64_t)k * m.Y + j) * m.X + i0;
+  const int o = (int)(idx & 3u);
+  uint32_t v0, v1;
+  if (m.aligned16 && i1 == i0 + 1 && o != 3 && idx - o + 4 <= m.n) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4*>(m.vox + (idx - o)));
+    v0 = o == 0 ? q.x : (o == 1 ? q.y : q.z);
+    v1 = o == 0 ? q.y : (o == 1 ? q.z : q.w);
+  } else {
+    v0 = __ldg(m.vox + idx);
+    v1 = __ldg(m.vox + idx + (uint64_t)(i1 - i0));
+  }
+  d0 = corner_value(v0, i0, j, k);
+  d1 = corner_value(v1, i1, j, k);
 }
 
 // Lattice coordinate along one axis: u = p/side - 0.5 clamped to [0, n-1];
@@ -82,10 +105,11 @@ __device__ __forceinline__ Tri trilinear(const MapView& m, Real px, Real py, Rea
   axis_setup(px, m.side, m.X, i0, i1, fx, ax);
   axis_setup(py, m.side, m.Y, j0, j1, fy, ay);
   axis_setup(pz, m.side, m.Z, k0, k1, fz, az);
-  const float d000 = corner_dist(m, i0, j0, k0), d100 = corner_dist(m, i1, j0, k0);
-  const float d010 = corner_dist(m, i0, j1, k0), d110 = corner_dist(m, i1, j1, k0);
-  const float d001 = corner_dist(m, i0, j0, k1), d101 = corner_dist(m, i1, j0, k1);
-  const float d011 = corner_dist(m, i0, j1, k1), d111 = corner_dist(m, i1, j1, k1);
+  float d000, d100, d010, d110, d001, d101, d011, d111;
+  corner_pair(m, i0, i1, j0, k0, d000, d100);
+  corner_pair(m, i0, i1, j1, k0, d010, d110);
+  corner_pair(m, i0, i1, j0, k1, d001, d101);
+  corner_pair(m, i0, i1, j1, k1, d011, d111);
   // interpolate along x, then y, then z
   const float e00 = fmaf(fx, d100 - d000, d000), e10 = fmaf(fx, d110 - d010, d010);
   const float e01 = fmaf(fx, d101 - d001, d001), e11 = fmaf(fx, d111 - d011, d011);

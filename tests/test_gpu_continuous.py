@@ -213,3 +213,32 @@ def test_torch_autograd_functions(scene):
     gq = dvm.traj_cost_backward(arm, q.detach(), 0.05, torch.ones(8, device="cuda"))
     want = (gq * (1 - t)).sum(1)                               # chain rule through the interpolation
     assert torch.allclose(q0.grad, want, rtol=1e-5, atol=1e-6)
+
+
+def test_trilinear_corner_pair_paths(scene):
+    """Corner pairs along x are read with one 16-byte load when both lie in one
+    aligned word inside the map, one at a time otherwise (the pair straddles a
+    word, the word would pass the map's end, or the axis is one voxel wide).
+    Every path gives the FP64 oracle's values: the map's last cells, cells at
+    each x mod 4, and a map one voxel wide in x."""
+    sc, edt, dvm = scene
+    rng = np.random.default_rng(3)
+    hi = (np.asarray(sc.dims) - 0.5) * sc.side
+    edge = hi - rng.random((4000, 3)) * 1.5 * sc.side  # the last cells
+    cells = rng.integers(0, np.asarray(sc.dims) - 1, size=(4000, 3))
+    cells[:, 0] = (cells[:, 0] & ~3) + np.arange(4000) % 4  # i0 at every x mod 4
+    inner = (cells + 0.5 + rng.random((4000, 3))) * sc.side
+    pts = np.concatenate([edge, np.minimum(inner, hi)]).astype(np.float32)
+    d32, g32 = dvm.trilinear(torch.as_tensor(pts))
+    d64, g64 = oracle.trilinear64(edt, sc.dims, sc.side, pts)
+    assert np.abs(d32.cpu().numpy().astype(np.float64) - d64).max() / sc.side <= DIST_MAX_ERR_VOX
+    u = pts.astype(np.float64) / np.float64(np.float32(sc.side)) - 0.5
+    off = ~_near_face(u - np.floor(u), 1e-6)
+    assert np.abs(g32.cpu().numpy().astype(np.float64) - g64)[off].max() <= GRAD_MAX_ERR
+    thin = (1, 40, 30)
+    tp = (rng.random((200, 3)) * thin).astype(np.float32)
+    _, tedt, tdvm = gpu_edt(thin, 1.0, tp)
+    q = (rng.random((3000, 3)) * thin).astype(np.float32)
+    td32, _ = tdvm.trilinear(torch.as_tensor(q))
+    td64, _ = oracle.trilinear64(tedt, thin, 1.0, q)
+    assert np.abs(td32.cpu().numpy().astype(np.float64) - td64).max() <= DIST_MAX_ERR_VOX
