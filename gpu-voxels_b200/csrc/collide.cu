@@ -165,9 +165,11 @@ __global__ void __launch_bounds__(256) lists_collide_map_kernel(const uint32_t* 
 }
 
 // BitVoxel test of a whole 32-byte voxel: a meaning other than eBVM_FREE.
+// A plain (coherent) load: the kernels below may mark this voxel afterwards,
+// so it is not read-only for the kernel's duration.
 __device__ __forceinline__ bool bitvoxel_occupied(const uint32_t* v) {
-  const uint4 lo = __ldg(reinterpret_cast<const uint4*>(v));
-  const uint4 hi = __ldg(reinterpret_cast<const uint4*>(v) + 1);
+  const uint4 lo = *reinterpret_cast<const uint4*>(v);
+  const uint4 hi = *(reinterpret_cast<const uint4*>(v) + 1);
   return ((lo.x & ~1u) | lo.y | lo.z | lo.w | hi.x | hi.y | hi.z | hi.w) != 0u;
 }
 

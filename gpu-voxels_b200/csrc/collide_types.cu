@@ -29,9 +29,18 @@ struct Bits8 {
   uint32_t w[8];
 };
 
+// A voxel the kernel only reads (the other map, the mask): read-only cache.
 __device__ __forceinline__ Bits8 load_voxel(const uint32_t* v) {
   const uint4 a = __ldg(reinterpret_cast<const uint4*>(v));
   const uint4 b = __ldg(reinterpret_cast<const uint4*>(v) + 1);
+  return Bits8{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
+}
+
+// A voxel the kernel may mark afterwards (this map, the list): a plain load,
+// since the read-only cache is only for data no thread writes during the kernel.
+__device__ __forceinline__ Bits8 load_voxel_rw(const uint32_t* v) {
+  const uint4 a = *reinterpret_cast<const uint4*>(v);
+  const uint4 b = *(reinterpret_cast<const uint4*>(v) + 1);
   return Bits8{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
 }
 
@@ -68,7 +77,7 @@ __global__ void __launch_bounds__(256) bvm_types_kernel(uint32_t* __restrict__ s
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     uint32_t* sv = self + i * kBitVoxelWords;
-    const Bits8 a = load_voxel(sv);
+    const Bits8 a = load_voxel_rw(sv);
     Bits8 t;
     bool hit;
     if (mode == 0) {
@@ -111,7 +120,7 @@ __global__ void __launch_bounds__(256) list_types_kernel(const uint32_t* __restr
                                : ((float)reinterpret_cast<const int8_t*>(map)[j] >= fthr);
     if (!occ) continue;
     uint32_t* lv = lvox + i * kBitVoxelWords;
-    const Bits8 a = load_voxel(lv);
+    const Bits8 a = load_voxel_rw(lv);
     if (mask != nullptr) {
       uint32_t meet = 0;
 #pragma unroll
