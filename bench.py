@@ -157,7 +157,9 @@ class Ranks:
         if self.world > 1:
             import torch.distributed as dist
             from datetime import timedelta
-            dist.init_process_group(backend, timeout=timedelta(seconds=120))
+            # bounded: after the collective steps rank 0 alone runs the baselines and the
+            # config sections (about a minute) while the other ranks wait in close()
+            dist.init_process_group(backend, timeout=timedelta(seconds=900))
             self.dist = dist
 
     def barrier(self) -> None:
