@@ -288,8 +288,10 @@ gvx_status gvx_bvm_create(const gvx_dims* dims, float voxel_side, gvx_bvm** out)
   const uint64_t bytes = num_voxels(*dims) * kBitVoxelBytes;
   cudaError_t e = cudaMalloc(&m->d_vox, bytes);
   if (e == cudaSuccess) e = cudaMemset(m->d_vox, 0, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&m->d_occ, (num_voxels(*dims) + 31) / 32 * sizeof(uint32_t));
   if (e != cudaSuccess) {
     if (m->d_vox) cudaFree(m->d_vox);
+    if (m->d_occ) cudaFree(m->d_occ);
     delete m;
     return cuda_status(e, "cudaMalloc(BitVectorVoxelMap)");
   }
@@ -302,6 +304,7 @@ gvx_status gvx_bvm_destroy(gvx_bvm* m) {
   cudaError_t e = m->d_vox ? cudaFree(m->d_vox) : cudaSuccess;
   if (m->d_flags) cudaFree(m->d_flags);
   if (m->d_colliding) cudaFree(m->d_colliding);
+  if (m->d_occ) cudaFree(m->d_occ);
   delete m;
   return cuda_status(e, "cudaFree(BitVectorVoxelMap)");
 }
@@ -869,7 +872,8 @@ gvx_status gvx_lists_collide_bvm(const uint32_t* d_ids, uint8_t* d_voxels, const
   if (n_lists == 0) return GVX_OK;
   return cuda_status(launch_lists_collide_map(d_ids, d_voxels, d_offsets, n_lists, n_total, map->d_vox,
                                               num_voxels(map->dims), mark,
-                                              reinterpret_cast<unsigned long long*>(d_counts), as_stream(stream)),
+                                              reinterpret_cast<unsigned long long*>(d_counts), as_stream(stream),
+                                              map->d_occ),
                      "batched list collision");
 }
 

@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 
 #include "gvx_internal.cuh"
@@ -115,51 +116,181 @@ __global__ void __launch_bounds__(256) list_collide_map_kernel(const uint32_t* _
 }
 
 // Batched form: many CSR lists in one launch, per-list counts.  A warp walks
-// 16 entries per step; the list of each entry is found from the list of the
-// warp's first entry, and hits are aggregated per list before the atomic.
+// 16 entries per group (lane pairs share an entry, as above) and owns a
+// contiguous range of groups, so the list of its first entry is found by one
+// binary search and the lists of later entries by a monotone advance; four
+// groups' gathers are issued before any is used.  Hits are aggregated per
+// list per warp with __match_any_sync before the atomic.
 __global__ void __launch_bounds__(256) lists_collide_map_kernel(const uint32_t* __restrict__ ids, uint32_t* __restrict__ lvox,
                                                                 const uint64_t* __restrict__ offsets, uint32_t n_lists,
                                                                 uint64_t n_total, const uint32_t* __restrict__ map,
                                                                 uint64_t map_n, int mark,
                                                                 unsigned long long* __restrict__ counts) {
+  constexpr int kU = 4;
   const int lane = threadIdx.x & 31;
   const bool low = (lane & 1) == 0;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  for (uint64_t base = gw * 16; base < n_total; base += warps * 16) {
-    // list of the warp's first entry: last k with offsets[k] <= base
-    uint32_t lo = 0, hi = n_lists;  // invariant: offsets[lo] <= base < offsets[hi]
+  const uint64_t groups = (n_total + 15) / 16;
+  const uint64_t per = (groups + warps - 1) / warps;
+  const uint64_t g_begin = gw * per, g_end = min(groups, g_begin + per);
+  if (g_begin >= g_end) return;
+  // the list of the warp's first entry: last k with offsets[k] <= entry
+  uint32_t list = 0;
+  {
+    uint32_t lo = 0, hi = n_lists;
+    const uint64_t first = g_begin * 16;
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
-      if (__ldg(offsets + mid) <= base) lo = mid; else hi = mid;
+      if (__ldg(offsets + mid) <= first) lo = mid; else hi = mid;
     }
-    const uint64_t k = base + (lane >> 1);
-    bool ok = k < n_total;
-    uint32_t list = lo;
-    if (ok) {
-      while (list + 1 < n_lists && __ldg(offsets + list + 1) <= k) ++list;
+    list = lo;
+  }
+  for (uint64_t g = g_begin; g < g_end; g += kU) {
+    uint4 a[kU], b[kU];
+    bool ok[kU];
+    uint64_t k[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      k[u] = (g + u) * 16 + (lane >> 1);
+      ok[u] = g + u < g_end && k[u] < n_total;
+      a[u] = make_uint4(0, 0, 0, 0);
+      b[u] = make_uint4(0, 0, 0, 0);
+      if (ok[u]) {
+        const uint64_t j = __ldg(ids + k[u]);
+        ok[u] = j < map_n;
+        a[u] = *(reinterpret_cast<const uint4*>(lvox + k[u] * kBitVoxelWords) + (lane & 1));
+        if (ok[u]) b[u] = __ldg(reinterpret_cast<const uint4*>(map + j * kBitVoxelWords) + (lane & 1));
+      }
     }
-    int64_t j = 0;
-    uint4 a = make_uint4(0, 0, 0, 0), b = make_uint4(0, 0, 0, 0);
-    if (ok) {
-      j = (int64_t)__ldg(ids + k);
-      ok = j < (int64_t)map_n;
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      // this lane's list: at or after the list of the warp's previous entries
+      uint32_t my = list;
+      const uint64_t kk = min(k[u], n_total - 1);
+      while (my + 1 < n_lists && __ldg(offsets + my + 1) <= kk) ++my;
+      list = __shfl_sync(kFull, my, 30);  // the group's last entry: a lower bound for the next group
+      uint32_t ma = half_bits(a[u], low), mb = half_bits(b[u], low);
+      ma |= __shfl_xor_sync(kFull, ma, 1);
+      mb |= __shfl_xor_sync(kFull, mb, 1);
+      const bool hit = ok[u] && ma != 0u && mb != 0u && low;
+      if (hit && mark) lvox[k[u] * kBitVoxelWords] = a[u].x | (1u << kCollisionBit);
+      const unsigned hit_mask = __ballot_sync(kFull, hit);
+      if (hit_mask) {
+        const unsigned same = __match_any_sync(kFull, my);
+        const unsigned mine = same & hit_mask;
+        if (hit && (__ffs(mine) - 1) == lane) atomicAdd(counts + my, (unsigned long long)__popc(mine));
+      }
     }
-    if (ok) {
-      a = *(reinterpret_cast<const uint4*>(lvox + k * kBitVoxelWords) + (lane & 1));
-      b = __ldg(reinterpret_cast<const uint4*>(map + (uint64_t)j * kBitVoxelWords) + (lane & 1));
+  }
+}
+
+// Bits at the even positions of x, packed into the low 16 bits.
+__device__ __forceinline__ uint32_t even_bits(uint32_t x) {
+  x &= 0x55555555u;
+  x = (x | (x >> 1)) & 0x33333333u;
+  x = (x | (x >> 2)) & 0x0F0F0F0Fu;
+  x = (x | (x >> 4)) & 0x00FF00FFu;
+  return (x | (x >> 8)) & 0x0000FFFFu;
+}
+
+// One bit per map voxel: set where the voxel holds a meaning other than
+// eBVM_FREE (DefaultCollider's test on that side, GV/voxel/DefaultCollider.hpp:
+// 76-81).  A warp reduces 32 voxels (1 KB, two 512-byte load instructions of
+// lane pairs) to one word; four words in flight per warp.
+__global__ void __launch_bounds__(256) bvm_occ_bits_kernel(const uint32_t* __restrict__ map, uint64_t n,
+                                                           uint32_t* __restrict__ bits) {
+  constexpr int kU = 4;
+  const int lane = threadIdx.x & 31;
+  const bool low = (lane & 1) == 0;
+  const uint64_t words = (n + 31) / 32;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (uint64_t w0 = gw * kU; w0 < words; w0 += warps * kU) {
+    uint4 h[kU][2];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        const uint64_t v = (w0 + u) * 32 + half * 16 + (lane >> 1);  // voxel of this lane pair
+        h[u][half] = v < n ? __ldcs(reinterpret_cast<const uint4*>(map + v * kBitVoxelWords) + (lane & 1))
+                           : make_uint4(0, 0, 0, 0);
+      }
     }
-    uint32_t ma = half_bits(a, low), mb = half_bits(b, low);
-    ma |= __shfl_xor_sync(kFull, ma, 1);
-    mb |= __shfl_xor_sync(kFull, mb, 1);
-    const bool hit = ok && ma != 0u && mb != 0u && low;
-    if (hit && mark) lvox[k * kBitVoxelWords] = a.x | (1u << kCollisionBit);
-    // aggregate hits of lanes that share a list
-    const unsigned hit_mask = __ballot_sync(kFull, hit);
-    if (hit_mask) {
-      const unsigned same = __match_any_sync(kFull, list);
-      const unsigned mine = same & hit_mask;
-      if (hit && (__ffs(mine) - 1) == lane) atomicAdd(counts + list, (unsigned long long)__popc(mine));
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      uint32_t word = 0;
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        uint32_t m = half_bits(h[u][half], low);
+        m |= __shfl_xor_sync(kFull, m, 1);
+        word |= even_bits(__ballot_sync(kFull, m != 0u)) << (16 * half);
+      }
+      if (lane == 0 && w0 + u < words) bits[w0 + u] = word;
+    }
+  }
+}
+
+// The batched form against those bits: entries as in lists_collide_map_kernel
+// (lane pairs read the entry's 32-byte voxel, contiguous ranges of 16-entry
+// groups per warp), the map side one bit lookup (the bit array stays in L2).
+__global__ void __launch_bounds__(256) lists_collide_bits_kernel(const uint32_t* __restrict__ ids,
+                                                                 uint32_t* __restrict__ lvox,
+                                                                 const uint64_t* __restrict__ offsets, uint32_t n_lists,
+                                                                 uint64_t n_total, const uint32_t* __restrict__ bits,
+                                                                 uint64_t map_n, int mark,
+                                                                 unsigned long long* __restrict__ counts) {
+  constexpr int kU = 4;
+  const int lane = threadIdx.x & 31;
+  const bool low = (lane & 1) == 0;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint64_t groups = (n_total + 15) / 16;
+  const uint64_t per = (groups + warps - 1) / warps;
+  const uint64_t g_begin = gw * per, g_end = min(groups, g_begin + per);
+  if (g_begin >= g_end) return;
+  uint32_t list = 0;
+  {
+    uint32_t lo = 0, hi = n_lists;
+    const uint64_t first = g_begin * 16;
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (__ldg(offsets + mid) <= first) lo = mid; else hi = mid;
+    }
+    list = lo;
+  }
+  for (uint64_t g = g_begin; g < g_end; g += kU) {
+    uint4 a[kU];
+    bool occ[kU];
+    uint64_t k[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      k[u] = (g + u) * 16 + (lane >> 1);
+      const bool ok = g + u < g_end && k[u] < n_total;
+      a[u] = make_uint4(0, 0, 0, 0);
+      occ[u] = false;
+      if (ok) {
+        const uint64_t j = __ldg(ids + k[u]);
+        a[u] = *(reinterpret_cast<const uint4*>(lvox + k[u] * kBitVoxelWords) + (lane & 1));
+        occ[u] = j < map_n && ((__ldg(bits + (j >> 5)) >> (j & 31)) & 1u);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      uint32_t my = list;
+      const uint64_t kk = min(k[u], n_total - 1);
+      while (my + 1 < n_lists && __ldg(offsets + my + 1) <= kk) ++my;
+      list = __shfl_sync(kFull, my, 30);
+      uint32_t ma = half_bits(a[u], low);
+      ma |= __shfl_xor_sync(kFull, ma, 1);
+      const bool hit = occ[u] && ma != 0u && low;
+      if (hit && mark) lvox[k[u] * kBitVoxelWords] = a[u].x | (1u << kCollisionBit);
+      const unsigned hit_mask = __ballot_sync(kFull, hit);
+      if (hit_mask) {
+        const unsigned same = __match_any_sync(kFull, my);
+        const unsigned mine = same & hit_mask;
+        if (hit && (__ffs(mine) - 1) == lane) atomicAdd(counts + my, (unsigned long long)__popc(mine));
+      }
     }
   }
 }
@@ -251,6 +382,19 @@ __global__ void __launch_bounds__(256) list_collide_list_kernel(const uint32_t* 
   block_count_add(hits, count);
 }
 
+// Blocks of `kernel` (256 threads) resident on the device at once, queried once
+// per kernel: kernels whose warps own contiguous ranges must not run in waves.
+template <auto kKernel>
+unsigned resident_blocks() {
+  static std::atomic<int> per_sm{0};  // one cache per kernel
+  int v = per_sm.load(std::memory_order_relaxed);
+  if (v == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kKernel, 256, 0) != cudaSuccess || v < 1) v = 1;
+    per_sm.store(v, std::memory_order_relaxed);
+  }
+  return (unsigned)(v * sms());
+}
+
 unsigned grid_cap(uint64_t work_items, int per_block) {
   const uint64_t want = (work_items + per_block - 1) / per_block;
   return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sms() * 8));
@@ -280,10 +424,22 @@ cudaError_t launch_list_collide_map(const uint32_t* d_ids, uint8_t* d_list_vox, 
 
 cudaError_t launch_lists_collide_map(const uint32_t* d_ids, uint8_t* d_vox, const uint64_t* d_offsets, uint32_t n_lists,
                                      uint64_t n_total, const uint8_t* d_map, uint64_t map_n, int mark,
-                                     unsigned long long* d_counts, cudaStream_t s) {
+                                     unsigned long long* d_counts, cudaStream_t s, uint32_t* d_occ) {
   cudaError_t e = cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * n_lists, s);
   if (e != cudaSuccess || n_total == 0 || n_lists == 0) return e;
-  lists_collide_map_kernel<<<grid_cap(n_total, 8 * 16), 256, 0, s>>>(
+  if (d_occ != nullptr && 2 * n_total >= map_n) {
+    // many entries per voxel: one streaming read of the map beats a 32-byte
+    // random gather per entry
+    bvm_occ_bits_kernel<<<grid_cap((map_n + 31) / 32, 8 * 4), 256, 0, s>>>(reinterpret_cast<const uint32_t*>(d_map),
+                                                                           map_n, d_occ);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const unsigned grid = std::min(grid_cap(n_total, 8 * 16), resident_blocks<lists_collide_bits_kernel>());
+    lists_collide_bits_kernel<<<grid, 256, 0, s>>>(
+        d_ids, reinterpret_cast<uint32_t*>(d_vox), d_offsets, n_lists, n_total, d_occ, map_n, mark, d_counts);
+    return cudaGetLastError();
+  }
+  const unsigned grid = std::min(grid_cap(n_total, 8 * 16), resident_blocks<lists_collide_map_kernel>());
+  lists_collide_map_kernel<<<grid, 256, 0, s>>>(
       d_ids, reinterpret_cast<uint32_t*>(d_vox), d_offsets, n_lists, n_total, reinterpret_cast<const uint32_t*>(d_map),
       map_n, mark, d_counts);
   return cudaGetLastError();

@@ -62,6 +62,9 @@ struct gvx_bvm {
   uint8_t* d_flags = nullptr;
   uint64_t flags_cap = 0;
   uint32_t* d_colliding = nullptr;
+  // batched list collisions: one bit per voxel, set where the voxel holds a
+  // meaning other than eBVM_FREE (refilled from the map by every such call)
+  uint32_t* d_occ = nullptr;
 };
 
 struct gvx_pvm {
@@ -238,9 +241,12 @@ cudaError_t launch_list_collide_pvm(const uint32_t* d_ids, uint8_t* d_list_vox, 
                                     cudaStream_t s);
 cudaError_t launch_list_collide_map(const uint32_t* d_ids, uint8_t* d_list_vox, uint64_t n, const uint8_t* d_map,
                                     uint64_t map_n, int64_t off, int mark, unsigned long long* d_count, cudaStream_t s);
+// d_occ (optional, (map_n + 31) / 32 words): when given and the lists hold at
+// least half as many entries as the map has voxels, the map is first reduced to
+// one occupancy bit per voxel and the entries test those bits.
 cudaError_t launch_lists_collide_map(const uint32_t* d_ids, uint8_t* d_vox, const uint64_t* d_offsets, uint32_t n_lists,
                                      uint64_t n_total, const uint8_t* d_map, uint64_t map_n, int mark,
-                                     unsigned long long* d_counts, cudaStream_t s);
+                                     unsigned long long* d_counts, cudaStream_t s, uint32_t* d_occ = nullptr);
 cudaError_t launch_list_collide_list(const uint32_t* d_a, uint64_t na, const uint32_t* d_b, uint64_t nb,
                                      unsigned long long* d_count, cudaStream_t s);
 

@@ -498,7 +498,11 @@ GVX_API gvx_status gvx_blist_collide_blist(const gvx_blist *l, const gvx_blist *
 /* Batched list-vs-map collision (no reference counterpart; the reference
  * runs one launch per list): n_lists CSR lists over concatenated arrays,
  * list k = entries [d_offsets[k], d_offsets[k+1]).  Ids must be < the map's
- * voxel count to be tested.  d_counts: n_lists uint64, overwritten.  One launch. */
+ * voxel count to be tested.  d_counts: n_lists uint64, overwritten.  One
+ * launch; when the lists hold at least half as many entries as the map has
+ * voxels, two: the map is first reduced to one occupancy bit per voxel (a
+ * buffer of voxels / 8 bytes kept with the map handle) and the entries test
+ * those bits, so calls on one map must not overlap on the GPU. */
 GVX_API gvx_status gvx_lists_collide_bvm(const uint32_t *d_ids, uint8_t *d_voxels, const uint64_t *d_offsets, uint32_t n_lists,
                                  uint64_t n_total, const gvx_bvm *map, int mark, uint64_t *d_counts, gvx_stream stream);
 

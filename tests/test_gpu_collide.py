@@ -151,3 +151,48 @@ def test_batched_lists_equal_per_list_counts():
     got = gvx.lists_collide_map(torch.as_tensor(ids.astype(np.int64)).to(torch.int32).cuda(),
                                 torch.as_tensor(vox).cuda(), torch.as_tensor(offs.astype(np.int64)).cuda(), gm)
     assert np.array_equal(got.cpu().numpy().astype(np.uint64), want)
+
+
+@pytest.mark.parametrize("dims", [(64, 64, 64), (24, 20, 17)])
+def test_batched_lists_both_paths_with_marks(dims):
+    """The batched call gathers a map voxel per entry (64^3: fewer entries than
+    half the voxels) or first reduces the map to occupancy bits (24x20x17:
+    many entries per voxel); both give the oracle's counts and marks, with
+    empty lists, free-only entries and ids beyond the map."""
+    nvox = int(np.prod(dims))
+    rng = np.random.default_rng(21)
+    lengths = np.concatenate([[0, 3], rng.integers(10, 2500, size=40), [0, 1]])
+    ids, offs = [], [0]
+    for L in lengths:
+        v = np.unique(rng.integers(0, nvox + 50, size=int(L))).astype(np.uint32)
+        ids.append(v)
+        offs.append(offs[-1] + v.shape[0])
+    ids = np.concatenate(ids)
+    offs = np.asarray(offs, np.uint64)
+    vox = np.zeros((ids.shape[0], 32), np.uint8)
+    vox[:, 1] = 1  # meaning 8
+    free = rng.random(ids.shape[0]) < 0.1
+    vox[free] = 0
+    vox[free, 0] = 1  # eBVM_FREE only: never collides
+    vox = vox.reshape(-1)
+    mp = (rng.random((nvox // 3, 3)) * dims).astype(np.float32)
+    # the map: occupied points, then free-only points
+    gmap = _gbvm(dims, mp, 1)
+    free_pts = (np.random.default_rng(99).random((nvox // 10, 3)) * dims).astype(np.float32)
+    om = _obvm(dims, mp, 1)
+    oracle.bvm_insert(om, dims, 1.0, free_pts, 0)
+    gmap.insertPointCloud(torch.as_tensor(free_pts), 0)
+    assert np.array_equal(gmap.voxels().cpu().numpy(), om)
+    want_vox = vox.copy()
+    want = []
+    for k in range(len(lengths)):
+        a, b = int(offs[k]), int(offs[k + 1])
+        seg = want_vox[a * 32:b * 32].copy()
+        want.append(oracle.list_collide_map(ids[a:b], seg, om, 0, True))
+        want_vox[a * 32:b * 32] = seg
+    assert (2 * ids.shape[0] >= nvox) == (dims != (64, 64, 64))
+    dv = torch.as_tensor(vox).cuda()
+    got = gvx.lists_collide_map(torch.as_tensor(ids.astype(np.int64)).to(torch.int32).cuda(), dv,
+                                torch.as_tensor(offs.astype(np.int64)).cuda(), gmap, mark=True)
+    assert got.cpu().numpy().tolist() == want and sum(want) > 0
+    assert np.array_equal(dv.cpu().numpy(), want_vox)
