@@ -379,16 +379,20 @@ def section_c3(hbm_peak):
     ms_ll = _time(per_list, 1, warm=1)
     # The batched call reduces the map to one occupancy bit per voxel (one
     # streaming read, 32 B per voxel, plus the bits written) when the lists
-    # hold at least half as many entries as the map has voxels, then reads
-    # each entry's id and 32-byte voxel once (36 B per id); otherwise it
-    # gathers a 32-byte map voxel per entry (68 B per id).
+    # hold at least half as many entries as the map has voxels; then every
+    # entry's id is read (4 B) and its 32-byte voxel only where the map bit is
+    # set (every list voxel here holds a meaning, so those entries are the
+    # hits).  Otherwise it gathers a 32-byte map voxel per entry (68 B per id).
     map_n = int(np.prod(sc.dims))
     bits_path = 2 * n_ids >= map_n
-    alg_bytes = 36.0 * n_ids + 32.0 * map_n + 4.0 * ((map_n + 31) // 32) if bits_path else 68.0 * n_ids
+    hits_total = int(counts.sum().item())
+    alg_bytes = (4.0 * n_ids + 32.0 * map_n + 4.0 * ((map_n + 31) // 32) + 32.0 * hits_total if bits_path
+                 else 68.0 * n_ids)
     ach = alg_bytes / (ms_lb / 1e3) / 1e9
     res.update({"list_ids": int(n_ids), "lists_batched_ms": round(ms_lb, 4),
                 "list_ids_per_s": round(n_ids / ms_lb * 1e3, 1),
-                "lists_path": "map occupancy bits (36 B/id + 32 B/voxel)" if bits_path else "map gather (68 B/id)",
+                "lists_path": ("map occupancy bits (4 B/id + 32 B/voxel + 32 B per entry on an occupied voxel)"
+                               if bits_path else "map gather (68 B/id)"),
                 "lists_algorithmic_bytes": int(alg_bytes), "lists_achieved_gbs": round(ach, 1),
                 "lists_frac_of_hbm": round(ach / hbm_peak, 4),
                 "lists_per_list_loop_ms": round(ms_ll, 2), "lists_speedup_vs_loop": round(ms_ll / ms_lb, 1),

@@ -231,68 +231,123 @@ __global__ void __launch_bounds__(256) bvm_occ_bits_kernel(const uint32_t* __res
   }
 }
 
-// The batched form against those bits: entries as in lists_collide_map_kernel
-// (lane pairs read the entry's 32-byte voxel, contiguous ranges of 16-entry
-// groups per warp), the map side one bit lookup (the bit array stays in L2).
+// The batched form against those bits.  Each lane takes 4 consecutive
+// entries (one 16-byte id load when the ids are 16-byte aligned), a warp 128
+// per group, over a contiguous range of groups.  An entry can collide only
+// where its map bit is set, so the main loop reads just the ids (prefetched
+// one step ahead) and their bits (the bit array stays in L2); the entries
+// whose bit is set go to a per-warp queue in shared memory with a lower bound
+// of their list, and 32 at a time the warp reads their 32-byte voxels, marks
+// and counts the hits (list found by a short advance from the bound).
+constexpr int kListQueue = 64;  // per-warp candidate queue (two rounds of 32)
+
+__device__ __forceinline__ void flush_candidates(const uint64_t* __restrict__ cand_k, const uint32_t* __restrict__ cand_lb,
+                                                 int count, uint32_t* __restrict__ lvox,
+                                                 const uint64_t* __restrict__ offsets, uint32_t n_lists, int mark,
+                                                 unsigned long long* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  bool hit = false;
+  uint32_t my = 0;
+  if (lane < count) {
+    const uint64_t k = cand_k[lane];
+    my = cand_lb[lane];
+    while (my + 1 < n_lists && __ldg(offsets + my + 1) <= k) ++my;
+    uint32_t* v = lvox + k * kBitVoxelWords;
+    const uint4 lo4 = *reinterpret_cast<const uint4*>(v);
+    const uint4 hi4 = *(reinterpret_cast<const uint4*>(v) + 1);
+    hit = ((lo4.x & ~1u) | lo4.y | lo4.z | lo4.w | hi4.x | hi4.y | hi4.z | hi4.w) != 0u;
+    if (hit && mark) v[0] = lo4.x | (1u << kCollisionBit);
+  }
+  const unsigned hit_mask = __ballot_sync(kFull, hit);
+  if (hit_mask) {
+    const unsigned same = __match_any_sync(kFull, my);
+    const unsigned mine = same & hit_mask;
+    if (hit && (__ffs(mine) - 1) == lane) atomicAdd(counts + my, (unsigned long long)__popc(mine));
+  }
+}
+
 __global__ void __launch_bounds__(256) lists_collide_bits_kernel(const uint32_t* __restrict__ ids,
                                                                  uint32_t* __restrict__ lvox,
                                                                  const uint64_t* __restrict__ offsets, uint32_t n_lists,
                                                                  uint64_t n_total, const uint32_t* __restrict__ bits,
-                                                                 uint64_t map_n, int mark,
+                                                                 uint64_t map_n, int mark, int ids16,
                                                                  unsigned long long* __restrict__ counts) {
-  constexpr int kU = 4;
-  const int lane = threadIdx.x & 31;
-  const bool low = (lane & 1) == 0;
+  constexpr int kE = 4;       // entries per lane and group
+  constexpr int kG = 32 * kE;
+  __shared__ uint64_t s_k[8][kListQueue];
+  __shared__ uint32_t s_lb[8][kListQueue];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t* cand_k = s_k[warp];
+  uint32_t* cand_lb = s_lb[warp];
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const uint64_t groups = (n_total + 15) / 16;
+  const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  const uint64_t groups = (n_total + kG - 1) / kG;
   const uint64_t per = (groups + warps - 1) / warps;
   const uint64_t g_begin = gw * per, g_end = min(groups, g_begin + per);
   if (g_begin >= g_end) return;
+  // list of the warp's first entry: last k with offsets[k] <= entry
   uint32_t list = 0;
   {
     uint32_t lo = 0, hi = n_lists;
-    const uint64_t first = g_begin * 16;
+    const uint64_t first = g_begin * kG;
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
       if (__ldg(offsets + mid) <= first) lo = mid; else hi = mid;
     }
     list = lo;
   }
-  for (uint64_t g = g_begin; g < g_end; g += kU) {
-    uint4 a[kU];
-    bool occ[kU];
-    uint64_t k[kU];
+  auto load_ids = [&](uint64_t g, uint32_t (&j)[kE]) {
+    const uint64_t k0 = g * kG + (uint64_t)lane * kE;
+    if (g < g_end && ids16 && k0 + kE <= n_total) {
+      const uint4 q = __ldg(reinterpret_cast<const uint4*>(ids + k0));
+      j[0] = q.x; j[1] = q.y; j[2] = q.z; j[3] = q.w;
+    } else {
 #pragma unroll
-    for (int u = 0; u < kU; ++u) {
-      k[u] = (g + u) * 16 + (lane >> 1);
-      const bool ok = g + u < g_end && k[u] < n_total;
-      a[u] = make_uint4(0, 0, 0, 0);
-      occ[u] = false;
-      if (ok) {
-        const uint64_t j = __ldg(ids + k[u]);
-        a[u] = *(reinterpret_cast<const uint4*>(lvox + k[u] * kBitVoxelWords) + (lane & 1));
-        occ[u] = j < map_n && ((__ldg(bits + (j >> 5)) >> (j & 31)) & 1u);
+      for (int e = 0; e < kE; ++e) j[e] = (g < g_end && k0 + e < n_total) ? __ldg(ids + k0 + e) : 0xFFFFFFFFu;
+    }
+  };
+  int queued = 0;  // warp-uniform
+  uint32_t jn[kE];
+  load_ids(g_begin, jn);
+  for (uint64_t g = g_begin; g < g_end; ++g) {
+    uint32_t j[kE];
+#pragma unroll
+    for (int e = 0; e < kE; ++e) j[e] = jn[e];
+    load_ids(g + 1, jn);  // the next group's ids in flight while this one is tested
+    unsigned occ = 0;
+#pragma unroll
+    for (int e = 0; e < kE; ++e)
+      occ |= (unsigned)(j[e] < map_n && ((__ldg(bits + (j[e] >> 5)) >> (j[e] & 31)) & 1u)) << e;
+    const uint64_t k0 = g * kG + (uint64_t)lane * kE;
+#pragma unroll
+    for (int e = 0; e < kE; ++e) {
+      const bool c = (occ >> e) & 1u;
+      const unsigned cm = __ballot_sync(kFull, c);
+      if (cm) {  // append this round's candidates to the queue
+        if (c) {
+          const int slot = queued + __popc(cm & ((1u << lane) - 1u));
+          cand_k[slot] = k0 + e;
+          cand_lb[slot] = list;
+        }
+        queued += __popc(cm);
+        __syncwarp();
+        if (queued >= 32) {
+          flush_candidates(cand_k, cand_lb, 32, lvox, offsets, n_lists, mark, counts);
+          __syncwarp();
+          queued -= 32;
+          if (lane < queued) {  // the remainder moves to the front
+            cand_k[lane] = cand_k[32 + lane];
+            cand_lb[lane] = cand_lb[32 + lane];
+          }
+          __syncwarp();
+        }
       }
     }
-#pragma unroll
-    for (int u = 0; u < kU; ++u) {
-      uint32_t my = list;
-      const uint64_t kk = min(k[u], n_total - 1);
-      while (my + 1 < n_lists && __ldg(offsets + my + 1) <= kk) ++my;
-      list = __shfl_sync(kFull, my, 30);
-      uint32_t ma = half_bits(a[u], low);
-      ma |= __shfl_xor_sync(kFull, ma, 1);
-      const bool hit = occ[u] && ma != 0u && low;
-      if (hit && mark) lvox[k[u] * kBitVoxelWords] = a[u].x | (1u << kCollisionBit);
-      const unsigned hit_mask = __ballot_sync(kFull, hit);
-      if (hit_mask) {
-        const unsigned same = __match_any_sync(kFull, my);
-        const unsigned mine = same & hit_mask;
-        if (hit && (__ffs(mine) - 1) == lane) atomicAdd(counts + my, (unsigned long long)__popc(mine));
-      }
-    }
+    // the bound for the next group: the list of its first entry
+    const uint64_t next = min((g + 1) * kG, n_total - 1);
+    while (list + 1 < n_lists && __ldg(offsets + list + 1) <= next) ++list;
   }
+  if (queued > 0) flush_candidates(cand_k, cand_lb, queued, lvox, offsets, n_lists, mark, counts);
 }
 
 // BitVoxel test of a whole 32-byte voxel: a meaning other than eBVM_FREE.
@@ -433,9 +488,10 @@ cudaError_t launch_lists_collide_map(const uint32_t* d_ids, uint8_t* d_vox, cons
     bvm_occ_bits_kernel<<<grid_cap((map_n + 31) / 32, 8 * 4), 256, 0, s>>>(reinterpret_cast<const uint32_t*>(d_map),
                                                                            map_n, d_occ);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const unsigned grid = std::min(grid_cap(n_total, 8 * 16), resident_blocks<lists_collide_bits_kernel>());
-    lists_collide_bits_kernel<<<grid, 256, 0, s>>>(
-        d_ids, reinterpret_cast<uint32_t*>(d_vox), d_offsets, n_lists, n_total, d_occ, map_n, mark, d_counts);
+    const unsigned grid = std::min(grid_cap(n_total, 8 * 128), resident_blocks<lists_collide_bits_kernel>());
+    const int ids16 = (reinterpret_cast<uintptr_t>(d_ids) & 15u) == 0;
+    lists_collide_bits_kernel<<<grid, 256, 0, s>>>(d_ids, reinterpret_cast<uint32_t*>(d_vox), d_offsets, n_lists,
+                                                   n_total, d_occ, map_n, mark, ids16, d_counts);
     return cudaGetLastError();
   }
   const unsigned grid = std::min(grid_cap(n_total, 8 * 16), resident_blocks<lists_collide_map_kernel>());

@@ -153,12 +153,14 @@ def test_batched_lists_equal_per_list_counts():
     assert np.array_equal(got.cpu().numpy().astype(np.uint64), want)
 
 
-@pytest.mark.parametrize("dims", [(64, 64, 64), (24, 20, 17)])
-def test_batched_lists_both_paths_with_marks(dims):
+@pytest.mark.parametrize("dims,shifted", [((64, 64, 64), False), ((24, 20, 17), False), ((24, 20, 17), True)])
+def test_batched_lists_both_paths_with_marks(dims, shifted):
     """The batched call gathers a map voxel per entry (64^3: fewer entries than
     half the voxels) or first reduces the map to occupancy bits (24x20x17:
-    many entries per voxel); both give the oracle's counts and marks, with
-    empty lists, free-only entries and ids beyond the map."""
+    many entries per voxel; its ids are read 16 bytes at a time when aligned,
+    4 at a time when the id array starts 4 bytes off -- `shifted`); every path
+    gives the oracle's counts and marks, with empty lists, free-only entries
+    and ids beyond the map."""
     nvox = int(np.prod(dims))
     rng = np.random.default_rng(21)
     lengths = np.concatenate([[0, 3], rng.integers(10, 2500, size=40), [0, 1]])
@@ -192,7 +194,9 @@ def test_batched_lists_both_paths_with_marks(dims):
         want_vox[a * 32:b * 32] = seg
     assert (2 * ids.shape[0] >= nvox) == (dims != (64, 64, 64))
     dv = torch.as_tensor(vox).cuda()
-    got = gvx.lists_collide_map(torch.as_tensor(ids.astype(np.int64)).to(torch.int32).cuda(), dv,
-                                torch.as_tensor(offs.astype(np.int64)).cuda(), gmap, mark=True)
+    dids = torch.as_tensor(np.concatenate([[0], ids]).astype(np.int64)).to(torch.int32).cuda()
+    dids = dids[1:] if shifted else dids[1:].clone()
+    assert (dids.data_ptr() % 16 == 4) == shifted
+    got = gvx.lists_collide_map(dids, dv, torch.as_tensor(offs.astype(np.int64)).cuda(), gmap, mark=True)
     assert got.cpu().numpy().tolist() == want and sum(want) > 0
     assert np.array_equal(dv.cpu().numpy(), want_vox)
