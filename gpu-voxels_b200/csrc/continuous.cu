@@ -180,20 +180,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_kernel(MapView 
 }
 
 // Adjoint of the hinge cost.  For an active sphere s on link j,
-//   d cost / d q_k = -grad d(c_s) . (z_k x (c_s - o_k))   for k <= j,
-// which sums per joint to -z_k . (M_k - o_k x G_k) with suffix sums over links
-// M_k = sum c_s x g_s, G_k = sum g_s.  One warp per waypoint, FK recomputed.
-// The moment sums run in FP64: M_k and o_k x G_k are of the order of the
-// arm's reach while their difference is of the order of the lever arm, so
-// FP32 sums would lose that ratio in relative accuracy; the spatial gradients
-// g_s stay FP32 (the trilinear query's own precision).
+//   d cost / d q_k = -grad d(c_s) . (z_k x (c_s - o_k))   for k <= j.
+// One warp per waypoint, FK recomputed: each lane evaluates its spheres once
+// and adds every joint's term to a per-joint accumulator in FP64 (the moment
+// arm c_s - o_k formed in double, so nothing large cancels); the spatial
+// gradient g_s stays FP32 (the trilinear query's own precision).  A fixed xor
+// butterfly sums the accumulators over the warp, so the result is
+// deterministic.
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapView m, gvx_arm arm,
                                                                            const float* __restrict__ q, uint64_t n_traj,
                                                                            uint32_t n_wp, float margin,
                                                                            const float* __restrict__ gcost,
                                                                            float* __restrict__ gq) {
   __shared__ WarpFK s_fk[kWarpsPerBlock];
-  __shared__ double s_link[kWarpsPerBlock][GVX_MAX_JOINTS][6];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int J = arm.n_joints;
   const uint64_t n_items = n_traj * n_wp;
@@ -201,47 +200,37 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) traj_cost_bwd_kernel(MapV
   for (uint64_t item = (uint64_t)blockIdx.x * kWarpsPerBlock + warp; item < n_items; item += total_warps) {
     const uint64_t traj = item / n_wp;
     warp_fk(arm, q + item * J, s_fk[warp]);
-    for (int j = 0; j < J; ++j) {
-      // per-link sums of c x g and g over this lane's active spheres
-      double mc[3] = {0.0, 0.0, 0.0}, gg[3] = {0.0, 0.0, 0.0};
-      for (int s = lane; s < arm.n_spheres; s += 32) {
-        if (arm.link[s] != j) continue;
-        double c[3];
-        sphere_centre(arm, s_fk[warp], s, c);
-        const Tri t = trilinear(m, c[0], c[1], c[2]);
-        if (margin - (t.d * m.side - arm.r[s]) > 0.0f) {
-          const double gx = t.gx, gy = t.gy, gz = t.gz;
-          mc[0] += c[1] * gz - c[2] * gy;
-          mc[1] += c[2] * gx - c[0] * gz;
-          mc[2] += c[0] * gy - c[1] * gx;
-          gg[0] += gx; gg[1] += gy; gg[2] += gz;
-        }
-      }
+    double acc[GVX_MAX_JOINTS];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
+    for (int k = 0; k < GVX_MAX_JOINTS; ++k) acc[k] = 0.0;
+    for (int s = lane; s < arm.n_spheres; s += 32) {
+      double c[3];
+      sphere_centre(arm, s_fk[warp], s, c);
+      const Tri t = trilinear(m, c[0], c[1], c[2]);
+      if (margin - (t.d * m.side - arm.r[s]) > 0.0f) {
+        const int js = arm.link[s];
+        const double gx = t.gx, gy = t.gy, gz = t.gz;
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          mc[i] += __shfl_xor_sync(kFull, mc[i], o);
-          gg[i] += __shfl_xor_sync(kFull, gg[i], o);
+        for (int k = 0; k < GVX_MAX_JOINTS; ++k) {
+          if (k > js) break;  // joints beyond the sphere's link do not move it
+          const double* o = s_fk[warp].o[k];
+          const double* z = s_fk[warp].z[k];
+          const double lx = c[0] - o[0], ly = c[1] - o[1], lz = c[2] - o[2];
+          acc[k] -= gx * (z[1] * lz - z[2] * ly) + gy * (z[2] * lx - z[0] * lz) + gz * (z[0] * ly - z[1] * lx);
         }
-      }
-      if (lane == 0) {
-        for (int i = 0; i < 3; ++i) { s_link[warp][j][i] = mc[i]; s_link[warp][j][3 + i] = gg[i]; }
       }
     }
-    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < GVX_MAX_JOINTS; ++k) {
+      if (k >= J) break;  // warp-uniform
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(kFull, acc[k], o);
+    }
     if (lane == 0) {
-      const float g = __ldg(gcost + traj);
-      double M[3] = {0.0, 0.0, 0.0}, G[3] = {0.0, 0.0, 0.0};
-      for (int k = J - 1; k >= 0; --k) {
-        for (int i = 0; i < 3; ++i) { M[i] += s_link[warp][k][i]; G[i] += s_link[warp][k][3 + i]; }
-        const double* o = s_fk[warp].o[k];
-        const double* z = s_fk[warp].z[k];
-        const double v0 = M[0] - (o[1] * G[2] - o[2] * G[1]);
-        const double v1 = M[1] - (o[2] * G[0] - o[0] * G[2]);
-        const double v2 = M[2] - (o[0] * G[1] - o[1] * G[0]);
-        gq[item * J + k] = (float)(-g * (z[0] * v0 + z[1] * v1 + z[2] * v2));
-      }
+      const double g = __ldg(gcost + traj);
+#pragma unroll
+      for (int k = 0; k < GVX_MAX_JOINTS; ++k)
+        if (k < J) gq[item * J + k] = (float)(g * acc[k]);
     }
     __syncwarp();
   }
