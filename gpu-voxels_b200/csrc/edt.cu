@@ -434,19 +434,28 @@ __device__ __forceinline__ float small_to_float(int v) { return biased((uint32_t
 
 // A site in the column frame: packed entry (a | row << 10 | c << 20) plus
 // twice its row and its squared offset from the column as exact floats
-// (offset < 2^21).  A0, C0: the column's coordinates, biased.
+// (offset < 2^21).  A0, C0: the column's coordinates, biased.  kOwnA: the
+// site's a equals the column's, so the offset is dc^2 alone (the same float:
+// da = 0 exactly).  That holds in pass Y when pass Z took the occupancy-bit
+// route (every input voxel UNINIT or its own site): pass Z's sites then share
+// the voxel's x and y.
 struct Col {
   uint32_t e;
   float r2, d;
 };
 
+template <bool kOwnA>
 __device__ __forceinline__ Col make_col(uint32_t e, float A0, float C0) {
   Col s;
   s.e = e;
   s.r2 = biased((e >> 9) & 0x7feu) - kBias;  // 2 * row
-  const float da = biased(e & 0x3ffu) - A0;
   const float dc = biased(e >> 20) - C0;
-  s.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));  // exact: integers below 2^21
+  if (kOwnA) {
+    s.d = __fmul_rn(dc, dc);
+  } else {
+    const float da = biased(e & 0x3ffu) - A0;
+    s.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));  // exact: integers below 2^21
+  }
   return s;
 }
 
@@ -463,17 +472,20 @@ __device__ __forceinline__ Col make_col(uint32_t e, float A0, float C0) {
 // integer with |num| < 2^21 and den an even integer in [2, 2046] (rows below
 // 1024, the later site second).  Markstein's correction (P. Markstein,
 // "Computation of elementary functions on the IBM RISC System/6000
-// processor", IBM J. Res. Develop. 34(1), 1990): with y the reciprocal of den
-// rounded to nearest and q0 within an ulp of num/den, the residual
-// r = num - q0*den is exact in one fma and fma(r, y, q0) is num/den rounded to
-// nearest.  y comes from the hardware's approximate reciprocal and one Newton
-// step.  No quotient of this domain is a tie (num/den either has at most 21
-// significant bits or is not a finite binary fraction).  gvx_check_bisector_quotient
-// compares every (num, den) of the domain with the IEEE divide on the device.
+// processor", IBM J. Res. Develop. 34(1), 1990): with q0 close to Q = num/den
+// the residual r = num - q0*den is exact in one fma, and fma(r, y, q0) with
+// y ~ 1/den is Q plus (Q - q0) * (y*den - 1).  Here y is the hardware's
+// approximate reciprocal alone (relative error about 2^-23) and q0 = num*y,
+// so |Q - q0| < 2^-22 |Q| and the fma's exact value is within 2^-21 ulp of
+// Q.  Q is never that close to a rounding midpoint: num has at most 21
+// significant bits, so Q is not a 25-bit binary fraction (no ties), and a
+// midpoint m = (2k+1) 2^(e-24) differs from num/den by a nonzero multiple of
+// 2^(e-24)/den, at least 2^-12 ulp for den <= 2046.  The fma therefore rounds
+// to RN(Q).  gvx_check_bisector_quotient compares every (num, den) of the
+// domain with the IEEE divide on the device.
 __device__ __forceinline__ float quotient_rn(float num, float den) {
-  float y0;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(den));
-  const float y = __fmaf_rn(__fmaf_rn(-den, y0, 1.0f), y0, y0);
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(den));
   const float q0 = __fmul_rn(num, y);
   const float r = __fmaf_rn(-q0, den, num);
   return __fmaf_rn(r, y, q0);
@@ -533,8 +545,9 @@ struct SweepCfg {
 // the first kept depth (lowest t) is exactly where the sequential loop stops.
 // Lane 31 only supplies the entry below lane 30's, so a round covers 31
 // depths.  All 32 lanes call this; only lane o's state changes (sec_e: the
-// packed entry below the top, decoded only when it becomes the top).
-template <class Cfg>
+// packed entry below the top, decoded only when it becomes the top).  Pass Y
+// only.
+template <class Cfg, bool kOwnA>
 __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint32_t* ring_base, const uint2* gstk_base, int L,
                                           int& n, int& lo, const Col& cur, Col& top, float& top_i, uint32_t& sec_e,
                                           float& sec_i, float& i2) {
@@ -544,7 +557,7 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint32_t* r
   const uint32_t ce = __shfl_sync(kFullMask, cur.e, o);
   const float oA0 = __shfl_sync(kFullMask, A0, o);  // lane o's column, biased
   const float oC0 = __shfl_sync(kFullMask, C0, o);
-  const Col oc = make_col(ce, oA0, oC0);
+  const Col oc = make_col<kOwnA>(ce, oA0, oC0);
   uint32_t* ringE = ring_base + o;
   float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
   const uint2* gstk = gstk_base + (size_t)o * L;
@@ -560,7 +573,7 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint32_t* r
       e = p.x;
       I = __uint_as_float(p.y);
     }
-    const Col ec = make_col(e, oA0, oC0);
+    const Col ec = make_col<kOwnA>(e, oA0, oC0);
     const float b = bisect(ec, oc);
     const bool keep = j <= 0 || I < b;
     const unsigned kb = __ballot_sync(kFullMask, keep) & 0x7fffffffu;
@@ -583,7 +596,7 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint32_t* r
       if (lane == o) {
         n = start - t + 1;
         lo = min(lo, new_lo);
-        top = make_col(e_top, oA0, oC0);
+        top = make_col<kOwnA>(e_top, oA0, oC0);
         top_i = i_top;
         i2 = b_top;
         sec_e = e_sec;
@@ -641,8 +654,9 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
 // Sweep); wbase = the warp's kWarpWords of shared memory; stack = L * 64
 // words of workspace: entry d of lane l is the pair (site, bisector with the
 // entry below) at ((uint2*)stack)[l * L + d] -- each lane's stack contiguous,
-// so its spills, refills and window reads fill whole sectors.
-template <bool kXPass, int kRows>
+// so its spills, refills and window reads fill whole sectors.  kOwnA (pass
+// Y only): every site's a equals its column's (see make_col).
+template <bool kXPass, int kRows, bool kOwnA = false>
 __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t* __restrict__ stack, int X, int Y,
                                            int Z, long long item, uint32_t* wbase) {
   using Cfg = SweepCfg<kRows>;
@@ -721,9 +735,13 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
       cur.e = a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u);
       cur.r2 = row2f;
       {
-        const float da = biased(a) - A0;
         const float dc = biased(v >> 20) - C0;
-        cur.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));
+        if (!kXPass && kOwnA) {
+          cur.d = __fmul_rn(dc, dc);
+        } else {
+          const float da = biased(a) - A0;
+          cur.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));
+        }
       }
       // Before a row's pops the top is the site of the last earlier row that
       // had one, so this bisector does not wait for the pops of earlier rows;
@@ -738,7 +756,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
               break;
             }
             --n;
-            top = make_col(sec_e, A0, C0);
+            top = make_col<!kXPass && kOwnA>(sec_e, A0, C0);
             top_i = sec_i;
             // The entry below the new top: its ring slot, or below the ring
             // the workspace (a predicated load; no divergent branch).  With
@@ -761,7 +779,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           while (deep_lanes) {
             const int o = __ffs(deep_lanes) - 1;
             deep_lanes &= deep_lanes - 1;
-            coop_pops<Cfg>(o, A0, C0, wbase + 2 * Cfg::kTileWords, gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
+            coop_pops<Cfg, kOwnA>(o, A0, C0, wbase + 2 * Cfg::kTileWords, gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
                            sec_e, sec_i, i2);
           }
         }
@@ -1150,7 +1168,9 @@ __device__ __forceinline__ unsigned next_item(unsigned* head) {
   return __shfl_sync(kFullMask, g, 0);
 }
 
-// sync = [done: Z words][head][err], zeroed before the launch.
+// sync = [done: Z words][head][err][pass Z's other-sites flag]; done, head
+// and err zeroed before the launch.  A zero flag means every site lies in its
+// own z column, and pass Y skips the zero x offset (sweep_item's kOwnA).
 template <int kRows>
 __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     edt_sweep_yx(uint32_t* __restrict__ map, uint32_t* __restrict__ stacks, unsigned* __restrict__ sync, int X, int Y,
@@ -1163,11 +1183,13 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
   unsigned* done = sync;
   unsigned* head = sync + Z;
   unsigned* err = head + 1;
+  const bool own = sync[Z + 2] == 0u;
   const unsigned ny = ((unsigned)X * Z + 31u) / 32u, nall = ny + ((unsigned)Y * Z + 31u) / 32u;
   for (unsigned g = next_item(head); g < nall; g = next_item(head)) {
     unsigned za, zb;
     if (g < ny) {
-      sweep_item<false, kRows>(map, stack, X, Y, Z, g, wbase);
+      if (own) sweep_item<false, kRows, true>(map, stack, X, Y, Z, g, wbase);
+      else sweep_item<false, kRows, false>(map, stack, X, Y, Z, g, wbase);
       item_slices(g, X, Z, za, zb);
       publish_slices(done, za, zb);
     } else {
@@ -1472,7 +1494,10 @@ cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t s
                                 const EdtConfig& cfg) {
   if (scratch_words < edt_scratch_words_min(d)) return cudaErrorInvalidValue;
   uint32_t* bits = d_scratch + edt_sync_words((int)d.z);
-  cudaError_t e = cudaMemsetAsync(bits, 0, occ_words((int)d.x, (int)d.y, (int)d.z) * sizeof(uint32_t), s);
+  // the occupancy bits and, in the same memset, pass Z's other-sites flag
+  // (every site is its own: the fused sweep's pass Y may skip the x offset)
+  uint32_t* other = d_scratch + d.z + 2;
+  cudaError_t e = cudaMemsetAsync(other, 0, (bits - other + occ_words((int)d.x, (int)d.y, (int)d.z)) * sizeof(uint32_t), s);
   if (e != cudaSuccess) return e;
   if (n > 0) {
     const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)device_sms() * 16);

@@ -101,7 +101,8 @@ GVX_API gvx_status gvx_dvm_voxelize_edt(gvx_dvm *m, const float *d_xyz, uint64_t
  * every voxel is UNINIT or its own site: occupancy bits read from the map,
  * then the sweep over the bits; otherwise the general sweep), 1 = the y sweep,
  * 2 = the x sweep (one launch each), 3 = the y and x sweeps
- * as the single fused launch gvx_dvm_edt uses (0 then 3 == gvx_dvm_edt;
+ * as the single fused launch gvx_dvm_edt uses, which takes pass 0's output
+ * and its record of the route it took (0 then 3 == gvx_dvm_edt;
  * 0, 1, 2 gives the same result).  Pass 0 alone equals the reference's
  * phase 1 (kernelPBAphase1FloodZ, GV/voxelmap/kernels/VoxelMapOperationsPBA.hpp:63-124). */
 GVX_API gvx_status gvx_dvm_edt_pass(gvx_dvm *m, int pass, gvx_stream stream);
