@@ -1204,8 +1204,9 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
 
 // The same schedule over every map of a batch: the queue holds all maps' Y
 // items, then all maps' X items.  maps[k].sync_off locates map k's slice
-// counters in `sync`; the queue head and error word follow them.
-template <int kRows>
+// counters in `sync`; the queue head and error word follow them.  kOwn: every
+// map's pass Z took the occupancy-bit route (sweep_item's kOwnA).
+template <int kRows, bool kOwn>
 __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     edt_sweep_yx_batch(const BatchMap* __restrict__ maps, const long long* __restrict__ prefix_y,
                        const long long* __restrict__ prefix_x, uint32_t n_maps, unsigned total_y, unsigned total_x,
@@ -1229,7 +1230,7 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     unsigned* done = sync + m.sync_off;
     unsigned za, zb;
     if (!x_item) {
-      sweep_item<false, kRows>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+      sweep_item<false, kRows, kOwn>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
       item_slices(item, m.X, m.Z, za, zb);
       publish_slices(done, za, zb);
     } else {
@@ -1387,13 +1388,13 @@ int sweep_rows() {
   return g_sweep_rows;
 }
 
-template <int kRows>
+template <int kRows, bool kOwn>
 cudaError_t launch_yx_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s) {
   using Cfg = SweepCfg<kRows>;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
-  auto kern = edt_sweep_yx_batch<kRows>;
+  auto kern = edt_sweep_yx_batch<kRows, kOwn>;
   long long blocks = 0;
-  cudaError_t e = kernel_setup<edt_sweep_yx_batch<kRows>>(Cfg::kWarps * 32, smem, &blocks);
+  cudaError_t e = kernel_setup<edt_sweep_yx_batch<kRows, kOwn>>(Cfg::kWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
   blocks = std::min<long long>(blocks, it.stack_warps / Cfg::kWarps);
   blocks = std::min<long long>(blocks, (it.total[1] + it.total[2] + Cfg::kWarps - 1) / Cfg::kWarps);
@@ -1410,9 +1411,10 @@ template <int kRows>
 long long batch_stack_warps() {
   using Cfg = SweepCfg<kRows>;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
-  long long blocks = 0;
-  if (kernel_setup<edt_sweep_yx_batch<kRows>>(Cfg::kWarps * 32, smem, &blocks) != cudaSuccess) return -1;
-  return blocks * Cfg::kWarps;
+  long long blocks = 0, own_blocks = 0;
+  if (kernel_setup<edt_sweep_yx_batch<kRows, false>>(Cfg::kWarps * 32, smem, &blocks) != cudaSuccess) return -1;
+  if (kernel_setup<edt_sweep_yx_batch<kRows, true>>(Cfg::kWarps * 32, smem, &own_blocks) != cudaSuccess) return -1;
+  return std::max(blocks, own_blocks) * Cfg::kWarps;
 }
 
 // Every (num, den) of the bisector domain: den = 2 * (blockIdx.y + 1), num
@@ -1541,8 +1543,9 @@ cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems&
   blocks = std::max<long long>(1, std::min<long long>(blocks, (it.total[0] + kZWarps - 1) / kZWarps));
   edt_pass_z_bits_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0], zw);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32>(d_table, it, s)
-                                                 : launch_yx_batch<16>(d_table, it, s);
+  // every site comes from the occupancy bits: its own
+  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32, true>(d_table, it, s)
+                                                 : launch_yx_batch<16, true>(d_table, it, s);
 }
 
 cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s, int rows) {
@@ -1554,8 +1557,8 @@ cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cuda
   edt_pass_z_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0]);
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32>(d_table, it, s)
-                                                 : launch_yx_batch<16>(d_table, it, s);
+  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32, false>(d_table, it, s)
+                                                 : launch_yx_batch<16, false>(d_table, it, s);
 }
 
 }  // namespace gvx
