@@ -120,10 +120,14 @@ gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** o
   gvx_batch* b = new (std::nothrow) gvx_batch();
   if (b == nullptr) return fail(GVX_ERR_OOM, "host allocation failed");
   b->maps.assign(maps, maps + n_maps);
-  std::vector<long long> prefix(3 * (size_t)(n_maps + 1), 0);
-  for (int p = 0; p < 3; ++p) {
-    for (uint32_t k = 0; k < n_maps; ++k)
-      prefix[p * (n_maps + 1) + k + 1] = prefix[p * (n_maps + 1) + k] + edt_pass_items(maps[k]->dims, p);
+  std::vector<long long> prefix(4 * (size_t)(n_maps + 1), 0);
+  for (int p = 0; p < 4; ++p) {
+    for (uint32_t k = 0; k < n_maps; ++k) {
+      const gvx_dims& d = maps[k]->dims;
+      const long long items = p < 3 ? edt_pass_items(d, p)  // occupancy tasks: z items x 32-row chunks
+                                    : edt_pass_items(d, 0) * (long long)((d.z + 31) / 32);
+      prefix[p * (n_maps + 1) + k + 1] = prefix[p * (n_maps + 1) + k] + items;
+    }
     b->items.total[p] = prefix[p * (n_maps + 1) + n_maps];
   }
   b->items.n_maps = n_maps;
@@ -142,7 +146,7 @@ gvx_status gvx_batch_create(gvx_dvm* const* maps, uint32_t n_maps, gvx_batch** o
     delete b;
     return cuda_status(e, "batch table");
   }
-  for (int p = 0; p < 3; ++p) b->items.d_prefix[p] = b->d_prefix + p * (size_t)(n_maps + 1);
+  for (int p = 0; p < 4; ++p) b->items.d_prefix[p] = b->d_prefix + p * (size_t)(n_maps + 1);
   b->items.d_stacks = b->d_stacks;
   b->items.stack_warps = stack_warps;
   b->items.stack_len = stack_len;

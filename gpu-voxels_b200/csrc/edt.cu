@@ -901,6 +901,9 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   cp_async_wait_all();
 }
 
+// A map's other-sites flag in a batch: word Z + 2 of its workspace, as for one map.
+__device__ __forceinline__ uint32_t* batch_other(const BatchMap& m) { return m.scratch + m.Z + 2; }
+
 // Map owning warp item g of a batch pass: last k with prefix[k] <= g.
 __device__ __forceinline__ uint32_t batch_owner(const long long* __restrict__ prefix, uint32_t n, long long g) {
   uint32_t lo = 0, hi = n;
@@ -933,6 +936,7 @@ __global__ void __launch_bounds__(kZWarps * 32, 3) edt_pass_z_batch(const BatchM
   for (long long g = (long long)blockIdx.x * kZWarps + warp; g < total; g += (long long)gridDim.x * kZWarps) {
     const uint32_t k = batch_owner(prefix, n_maps, g);
     const BatchMap m = maps[k];
+    if (*batch_other(m) == 0u) continue;  // the bits pass took this map
     const long long item = g - __ldg(prefix + k);
     pass_z_item(m.vox, m.X, m.Y, m.Z, item, s_z + (size_t)warp * kZWarpWords,
                 m.scratch + edt_sync_words(m.Z) + (uint64_t)item * zcarry_item_words(m.Z));
@@ -949,6 +953,7 @@ __device__ __forceinline__ uint32_t* batch_occ(const BatchMap& m) { return m.scr
 
 __global__ void occ_clear_batch_kernel(const BatchMap* __restrict__ maps) {
   const BatchMap m = maps[blockIdx.y];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *batch_other(m) = 0u;  // every site will be its own
   uint32_t* bits = batch_occ(m);
   const uint64_t n = occ_words(m.X, m.Y, m.Z);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -986,18 +991,15 @@ __global__ void occ_insert_batch_kernel(const BatchMap* __restrict__ maps, uint3
 // row (L >> 3) + 4 (L & 7): the warp's 32 words as one 128-byte store.
 // Consecutive warps take consecutive items of the same rows.  vec: map and
 // rows 16-byte aligned.
-__global__ void __launch_bounds__(256) occ_from_map_kernel(const uint32_t* __restrict__ map, uint32_t* __restrict__ bits,
-                                                           int X, int Y, int Z, uint32_t* __restrict__ other_sites,
-                                                           int vec) {
+// One task of occ_from_map: returns whether this lane saw another site.
+__device__ __forceinline__ bool occ_from_map_task(const uint32_t* __restrict__ map, uint32_t* __restrict__ bits, int X,
+                                                  int Y, int Z, long long t, long long items, bool vec) {
   const int lane = threadIdx.x & 31;
   const int g = lane >> 3, q = lane & 7;
-  const long long items = (long long)z_items(X, Y);
-  const long long tasks = items * ((Z + 31) >> 5);
   const uint32_t layer = (uint32_t)X * (uint32_t)Y;
-  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
   const bool x_aligned = (X & 31) == 0;  // an item's 32 columns lie in one y row
   bool other = false;
-  for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tasks; t += warps) {
+  {
     const int chunk = (int)(t / items);
     const uint32_t item = (uint32_t)(t - (long long)chunk * items);
     const int zc = chunk * 32;
@@ -1060,17 +1062,54 @@ __global__ void __launch_bounds__(256) occ_from_map_kernel(const uint32_t* __res
     const int zs = zc + g + 4 * q;
     if (zs < Z) bits[(uint64_t)item * Z + zs] = word;
   }
-  if (__any_sync(kFullMask, other) && lane == 0) atomicOr(other_sites, 1u);
+  return other;
+}
+
+__global__ void __launch_bounds__(256) occ_from_map_kernel(const uint32_t* __restrict__ map, uint32_t* __restrict__ bits,
+                                                           int X, int Y, int Z, uint32_t* __restrict__ other_sites,
+                                                           int vec) {
+  const long long items = (long long)z_items(X, Y);
+  const long long tasks = items * ((Z + 31) >> 5);
+  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  bool other = false;
+  for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < tasks; t += warps)
+    other |= occ_from_map_task(map, bits, X, Y, Z, t, items, vec != 0);
+  if (__any_sync(kFullMask, other) && (threadIdx.x & 31) == 0) atomicOr(other_sites, 1u);
+}
+
+// The same over every map of a batch: map k owns tasks [prefix[k],
+// prefix[k+1]); its bits go to its own workspace past the counters, its
+// other-sites flag to word Z + 2 of its workspace (cleared by
+// batch_flags_clear_kernel before).
+__global__ void __launch_bounds__(256) occ_from_map_batch_kernel(const BatchMap* __restrict__ maps,
+                                                                 const long long* __restrict__ prefix,
+                                                                 uint32_t n_maps, long long total) {
+  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long g = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < total; g += warps) {
+    const uint32_t k = batch_owner(prefix, n_maps, g);
+    const BatchMap m = maps[k];
+    const bool vec = (reinterpret_cast<uintptr_t>(m.vox) & 15u) == 0 && ((uint64_t)m.X * m.Y) % 4 == 0;
+    const bool other =
+        occ_from_map_task(m.vox, batch_occ(m), m.X, m.Y, m.Z, g - __ldg(prefix + k), (long long)z_items(m.X, m.Y), vec);
+    if (__any_sync(kFullMask, other) && (threadIdx.x & 31) == 0) atomicOr(batch_other(m), 1u);
+  }
+}
+
+__global__ void batch_flags_clear_kernel(const BatchMap* __restrict__ maps, uint32_t n_maps) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n_maps) *batch_other(maps[k]) = 0u;
 }
 
 __global__ void __launch_bounds__(kZWarps * 32) edt_pass_z_bits_batch(const BatchMap* __restrict__ maps,
                                                                        const long long* __restrict__ prefix,
-                                                                       uint32_t n_maps, long long total, int zw) {
+                                                                       uint32_t n_maps, long long total, int zw,
+                                                                       int skip_other) {
   extern __shared__ __align__(16) uint32_t s_z[];  // [kZWarps][2 * zw]
   const int warp = threadIdx.x >> 5;
   for (long long g = (long long)blockIdx.x * kZWarps + warp; g < total; g += (long long)gridDim.x * kZWarps) {
     const uint32_t k = batch_owner(prefix, n_maps, g);
     const BatchMap m = maps[k];
+    if (skip_other && *batch_other(m) != 0u) continue;  // the general pass takes this map
     pass_z_bits_item(m.vox, batch_occ(m), m.X, m.Y, m.Z, g - __ldg(prefix + k), s_z + (size_t)warp * 2 * zw, zw);
     __syncwarp();
   }
@@ -1204,9 +1243,10 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
 
 // The same schedule over every map of a batch: the queue holds all maps' Y
 // items, then all maps' X items.  maps[k].sync_off locates map k's slice
-// counters in `sync`; the queue head and error word follow them.  kOwn: every
-// map's pass Z took the occupancy-bit route (sweep_item's kOwnA).
-template <int kRows, bool kOwn>
+// counters in `sync`; the queue head and error word follow them.  Pass Y of a
+// map whose pass Z took the occupancy-bit route (its other-sites flag clear)
+// runs sweep_item's kOwnA form.
+template <int kRows>
 __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     edt_sweep_yx_batch(const BatchMap* __restrict__ maps, const long long* __restrict__ prefix_y,
                        const long long* __restrict__ prefix_x, uint32_t n_maps, unsigned total_y, unsigned total_x,
@@ -1230,7 +1270,8 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     unsigned* done = sync + m.sync_off;
     unsigned za, zb;
     if (!x_item) {
-      sweep_item<false, kRows, kOwn>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+      if (*batch_other(m) == 0u) sweep_item<false, kRows, true>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+      else sweep_item<false, kRows, false>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
       item_slices(item, m.X, m.Z, za, zb);
       publish_slices(done, za, zb);
     } else {
@@ -1388,13 +1429,13 @@ int sweep_rows() {
   return g_sweep_rows;
 }
 
-template <int kRows, bool kOwn>
+template <int kRows>
 cudaError_t launch_yx_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s) {
   using Cfg = SweepCfg<kRows>;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
-  auto kern = edt_sweep_yx_batch<kRows, kOwn>;
+  auto kern = edt_sweep_yx_batch<kRows>;
   long long blocks = 0;
-  cudaError_t e = kernel_setup<edt_sweep_yx_batch<kRows, kOwn>>(Cfg::kWarps * 32, smem, &blocks);
+  cudaError_t e = kernel_setup<edt_sweep_yx_batch<kRows>>(Cfg::kWarps * 32, smem, &blocks);
   if (e != cudaSuccess) return e;
   blocks = std::min<long long>(blocks, it.stack_warps / Cfg::kWarps);
   blocks = std::min<long long>(blocks, (it.total[1] + it.total[2] + Cfg::kWarps - 1) / Cfg::kWarps);
@@ -1411,10 +1452,9 @@ template <int kRows>
 long long batch_stack_warps() {
   using Cfg = SweepCfg<kRows>;
   const int smem = Cfg::kWarps * Cfg::kWarpWords * 4;
-  long long blocks = 0, own_blocks = 0;
-  if (kernel_setup<edt_sweep_yx_batch<kRows, false>>(Cfg::kWarps * 32, smem, &blocks) != cudaSuccess) return -1;
-  if (kernel_setup<edt_sweep_yx_batch<kRows, true>>(Cfg::kWarps * 32, smem, &own_blocks) != cudaSuccess) return -1;
-  return std::max(blocks, own_blocks) * Cfg::kWarps;
+  long long blocks = 0;
+  if (kernel_setup<edt_sweep_yx_batch<kRows>>(Cfg::kWarps * 32, smem, &blocks) != cudaSuccess) return -1;
+  return blocks * Cfg::kWarps;
 }
 
 // Every (num, den) of the bisector domain: den = 2 * (blockIdx.y + 1), num
@@ -1519,16 +1559,10 @@ cudaError_t launch_voxelize_edt(uint32_t* d_vox, uint32_t* d_scratch, uint64_t s
   return e == cudaSuccess ? launch_edt_pass(d_vox, d_scratch, scratch_words, d, 2, s, cfg.rows) : e;
 }
 
-cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems& it, const float* d_xyz,
-                                      const uint64_t* d_offsets, uint64_t n_total, cudaStream_t s, int rows) {
-  occ_clear_batch_kernel<<<dim3(64, it.n_maps), 256, 0, s>>>(d_table);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  if (n_total > 0) {
-    const unsigned blocks = (unsigned)std::min<uint64_t>((n_total + 255) / 256, (uint64_t)device_sms() * 16);
-    occ_insert_batch_kernel<<<blocks, 256, 0, s>>>(d_table, it.n_maps, d_xyz, d_offsets, n_total);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
+// The occupancy-bit pass Z over a batch (one persistent launch); skip_other:
+// leave maps whose other-sites flag is set to the general pass.
+cudaError_t launch_z_bits_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s, int skip_other) {
+  cudaError_t e;
   e = kernel_setup<edt_pass_z_bits_batch>(kZWarps * 32, kZBitsSmemMax, nullptr);
   if (e != cudaSuccess) return e;
   const int zw = z_bits_words((int)it.z_max);
@@ -1541,24 +1575,50 @@ cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems&
   if ((e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
   long long blocks = (long long)std::max(per_sm, 1) * std::max(sm, 1);
   blocks = std::max<long long>(1, std::min<long long>(blocks, (it.total[0] + kZWarps - 1) / kZWarps));
-  edt_pass_z_bits_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0], zw);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  // every site comes from the occupancy bits: its own
-  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32, true>(d_table, it, s)
-                                                 : launch_yx_batch<16, true>(d_table, it, s);
+  edt_pass_z_bits_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0], zw,
+                                                                      skip_other);
+  return cudaGetLastError();
 }
 
+cudaError_t launch_voxelize_edt_batch(const BatchMap* d_table, const BatchItems& it, const float* d_xyz,
+                                      const uint64_t* d_offsets, uint64_t n_total, cudaStream_t s, int rows) {
+  occ_clear_batch_kernel<<<dim3(64, it.n_maps), 256, 0, s>>>(d_table);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (n_total > 0) {
+    const unsigned blocks = (unsigned)std::min<uint64_t>((n_total + 255) / 256, (uint64_t)device_sms() * 16);
+    occ_insert_batch_kernel<<<blocks, 256, 0, s>>>(d_table, it.n_maps, d_xyz, d_offsets, n_total);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if ((e = launch_z_bits_batch(d_table, it, s, 0)) != cudaSuccess) return e;
+  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32>(d_table, it, s)
+                                                 : launch_yx_batch<16>(d_table, it, s);
+}
+
+// Batched EDT of filled maps.  Pass Z as for one map: each map's occupancy
+// bits and other-sites flag from its voxels, then the bits pass for the maps
+// whose voxels are all UNINIT or their own sites and the general pass for the
+// others (each launch skips the other maps).
 cudaError_t launch_edt_batch(const BatchMap* d_table, const BatchItems& it, cudaStream_t s, int rows) {
+  batch_flags_clear_kernel<<<(it.n_maps + 255) / 256, 256, 0, s>>>(d_table, it.n_maps);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, occ_from_map_batch_kernel, 256, 0)) != cudaSuccess)
+    return e;
+  const long long occ_blocks = std::max<long long>(
+      1, std::min<long long>((it.total[3] + 7) / 8, (long long)device_sms() * std::max(per_sm, 1)));
+  occ_from_map_batch_kernel<<<(unsigned)occ_blocks, 256, 0, s>>>(d_table, it.d_prefix[3], it.n_maps, it.total[3]);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = launch_z_bits_batch(d_table, it, s, 1)) != cudaSuccess) return e;
   const int smem = kZWarps * kZWarpWords * 4;
   long long blocks = 0;
-  cudaError_t e = kernel_setup<edt_pass_z_batch>(kZWarps * 32, smem, &blocks);
-  if (e != cudaSuccess) return e;
+  if ((e = kernel_setup<edt_pass_z_batch>(kZWarps * 32, smem, &blocks)) != cudaSuccess) return e;
   blocks = std::max<long long>(1, std::min<long long>(blocks, (it.total[0] + kZWarps - 1) / kZWarps));
   edt_pass_z_batch<<<(unsigned)blocks, kZWarps * 32, smem, s>>>(d_table, it.d_prefix[0], it.n_maps, it.total[0]);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32, false>(d_table, it, s)
-                                                 : launch_yx_batch<16, false>(d_table, it, s);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return (rows == 0 ? sweep_rows() : rows) == 32 ? launch_yx_batch<32>(d_table, it, s)
+                                                 : launch_yx_batch<16>(d_table, it, s);
 }
 
 }  // namespace gvx

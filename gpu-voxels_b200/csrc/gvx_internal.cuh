@@ -103,12 +103,13 @@ struct BatchMap {
 };
 
 // Work-item layout of the batched EDT: for pass p, map k owns warp items
-// [prefix[p][k], prefix[p][k+1]).  The fused Y -> X launch keeps one stack of
+// [prefix[p][k], prefix[p][k+1]); prefix[3] numbers the occupancy-bit tasks
+// of pass Z on filled maps (32 columns x 32 rows each).  The fused Y -> X launch keeps one stack of
 // stack_len rows (64 words each) per resident warp in d_stacks and its slice
 // counters, queue head and error word in d_sync (sync_words + 2 words).
 struct BatchItems {
-  long long* d_prefix[3];
-  long long total[3];
+  long long* d_prefix[4];
+  long long total[4];
   uint32_t n_maps;
   uint32_t* d_stacks;
   long long stack_warps;

@@ -120,3 +120,30 @@ def test_batch_thin_maps_items_span_slices():
         oracle.pba(want, dims)
         assert np.array_equal(got_fused[k], want), f"voxelize_edt map {k} {dims}"
         assert np.array_equal(to_u32(maps[k].data()), want), f"edt map {k} {dims}"
+
+
+def test_batch_edt_per_map_route_own_and_other_sites():
+    """Batch.edt on filled maps picks pass Z's route per map: the occupancy-bit
+    pass when every voxel is UNINIT or its own site, the general pass
+    otherwise (each launch skips the other maps).  A batch mixing freshly
+    inserted maps with maps that still hold an earlier transform (every voxel
+    its nearest site) equals the oracle map by map, and so does a second EDT
+    of the whole batch, where every map holds other sites."""
+    scenes = _scenes(6, seed=13)
+    maps = [gvx.DistanceVoxelMap(d, s) for d, s, _ in scenes]
+    b = Batch(maps)
+    pts, offs = _cat(scenes)
+    b.clear()
+    b.insert(pts, offs)
+    b.edt()
+    for k in range(0, len(maps), 2):  # even maps back to their inserted state
+        maps[k].clearMap()
+        maps[k].insertPointCloud(torch.as_tensor(scenes[k][2].astype(np.float32)).cuda())
+    for rep in range(2):
+        inputs = [to_u32(m.data()).copy() for m in maps]
+        b.edt()
+        assert b.edt_check() == 0
+        for k, (dims, _, _) in enumerate(scenes):
+            want = inputs[k].copy()
+            oracle.pba(want, dims)
+            assert np.array_equal(to_u32(maps[k].data()), want), f"pass {rep} map {k} {dims}"
