@@ -548,7 +548,7 @@ struct SweepCfg {
 // packed entry below the top, decoded only when it becomes the top).  Pass Y
 // only.
 template <class Cfg, bool kOwnA>
-__device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint32_t* ring_base, const uint2* gstk_base, int L,
+__device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint2* ring_base, const uint2* gstk_base, int L,
                                           int& n, int& lo, const Col& cur, Col& top, float& top_i, uint32_t& sec_e,
                                           float& sec_i, float& i2) {
   const int lane = threadIdx.x & 31;
@@ -558,16 +558,16 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint32_t* r
   const float oA0 = __shfl_sync(kFullMask, A0, o);  // lane o's column, biased
   const float oC0 = __shfl_sync(kFullMask, C0, o);
   const Col oc = make_col<kOwnA>(ce, oA0, oC0);
-  uint32_t* ringE = ring_base + o;
-  float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
+  uint2* ring = ring_base + o;
   const uint2* gstk = gstk_base + (size_t)o * L;
   for (int start = on - 1;; start -= 31) {
     const int j = start - lane;
     const int jc = max(j, 0);
     // the ring slot, replaced by the workspace entry below the ring (a
     // predicated load, so one decode and no divergent branch)
-    uint32_t e = ringE[(jc & (Cfg::kRing - 1)) * 32];
-    float I = ringI[(jc & (Cfg::kRing - 1)) * 32];
+    const uint2 rq = ring[(jc & (Cfg::kRing - 1)) * 32];
+    uint32_t e = rq.x;
+    float I = __uint_as_float(rq.y);
     if (jc < olo) {
       const uint2 p = gstk[jc];
       e = p.x;
@@ -585,8 +585,7 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint32_t* r
       const int u_last = min(t + Cfg::kRing - 2, 31);
       const int new_lo = max(start - u_last, 0);
       if (lane >= t && lane <= u_last && j >= 0 && jc < olo) {
-        ringE[(jc & (Cfg::kRing - 1)) * 32] = e;
-        ringI[(jc & (Cfg::kRing - 1)) * 32] = I;
+        ring[(jc & (Cfg::kRing - 1)) * 32] = make_uint2(e, __float_as_uint(I));
       }
       const uint32_t e_top = __shfl_sync(kFullMask, e, t);
       const float i_top = __shfl_sync(kFullMask, I, t);
@@ -684,8 +683,8 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   const bool vec16 = !kXPass && s.one_slice && s.valid == 32 && (X & 3) == 0;
   uint32_t* tile0 = wbase;
   uint32_t* tile1 = wbase + Cfg::kTileWords;
-  uint32_t* ringE = wbase + 2 * Cfg::kTileWords + lane;  // slot k: ringE[k * 32]
-  float* ringI = reinterpret_cast<float*>(ringE + Cfg::kRing * 32);
+  // the ring: slot k of this lane = (site, bisector) at ring[k * 32]
+  uint2* ring = reinterpret_cast<uint2*>(wbase + 2 * Cfg::kTileWords) + lane;
   uint2* gstk = reinterpret_cast<uint2*>(stack) + (size_t)lane * L;  // this lane's stack, depth d: gstk[d]
   const float A0 = biased((uint32_t)s.a);  // this lane's column coordinate, biased
   const float C0 = biased((uint32_t)s.z);
@@ -762,8 +761,9 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
             // the workspace (a predicated load; no divergent branch).  With
             // n < 2 it is never read: the next push replaces it.
             const int d = n - 2;
-            sec_e = ringE[(d & (Cfg::kRing - 1)) * 32];
-            sec_i = ringI[(d & (Cfg::kRing - 1)) * 32];
+            const uint2 rq = ring[(d & (Cfg::kRing - 1)) * 32];
+            sec_e = rq.x;
+            sec_i = __uint_as_float(rq.y);
             if (d >= 0 && d < lo) {
               const uint2 p = gstk[d];
               sec_e = p.x;
@@ -779,7 +779,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           while (deep_lanes) {
             const int o = __ffs(deep_lanes) - 1;
             deep_lanes &= deep_lanes - 1;
-            coop_pops<Cfg, kOwnA>(o, A0, C0, wbase + 2 * Cfg::kTileWords, gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
+            coop_pops<Cfg, kOwnA>(o, A0, C0, reinterpret_cast<uint2*>(wbase + 2 * Cfg::kTileWords), gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
                            sec_e, sec_i, i2);
           }
         }
@@ -791,11 +791,10 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           const int slot = (n & (Cfg::kRing - 1)) * 32;  // push the current site
           const int ev = n - Cfg::kRing;             // the depth this slot held
           if (ev >= lo && ev >= spill) {             // evicted before it reached the workspace
-            gstk[ev] = make_uint2(ringE[slot], __float_as_uint(ringI[slot]));
+            gstk[ev] = ring[slot];
             spill = ev + 1;
           }
-          ringE[slot] = cur.e;
-          ringI[slot] = i2;
+          ring[slot] = make_uint2(cur.e, __float_as_uint(i2));
           lo = max(lo, ev + 1);
           ++n;
           sec_e = top.e;
@@ -811,7 +810,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   }
   // the ring's entries that never reached the workspace
   spill = min(spill, n);
-  for (int d = spill; d < n; ++d) gstk[d] = make_uint2(ringE[(d & (Cfg::kRing - 1)) * 32], __float_as_uint(ringI[(d & (Cfg::kRing - 1)) * 32]));
+  for (int d = spill; d < n; ++d) gstk[d] = ring[(d & (Cfg::kRing - 1)) * 32];
   cp_async_wait_all();
   __syncwarp();
 
