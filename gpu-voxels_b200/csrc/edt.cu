@@ -432,6 +432,11 @@ constexpr float kBias = 12582912.0f;
 __device__ __forceinline__ float biased(uint32_t v) { return __uint_as_float(0x4B400000u | v); }
 __device__ __forceinline__ float small_to_float(int v) { return biased((uint32_t)v) - kBias; }
 
+// a - b per component in one packed instruction: fma(b, -1, a) rounds once,
+// the same as the scalar subtraction.
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+
+
 // A site in the column frame: packed entry (a | row << 10 | c << 20) plus
 // twice its row and its squared offset from the column as exact floats
 // (offset < 2^21).  A0, C0: the column's coordinates, biased.  kOwnA: the
@@ -449,12 +454,12 @@ __device__ __forceinline__ Col make_col(uint32_t e, float A0, float C0) {
   Col s;
   s.e = e;
   s.r2 = biased((e >> 9) & 0x7feu) - kBias;  // 2 * row
-  const float dc = biased(e >> 20) - C0;
   if (kOwnA) {
+    const float dc = biased(e >> 20) - C0;
     s.d = __fmul_rn(dc, dc);
   } else {
-    const float da = biased(e & 0x3ffu) - A0;
-    s.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));  // exact: integers below 2^21
+    const float2 dd = sub2(make_float2(biased(e & 0x3ffu), biased(e >> 20)), make_float2(A0, C0));
+    s.d = __fmaf_rn(dd.x, dd.x, __fmul_rn(dd.y, dd.y));  // exact: integers below 2^21
   }
   return s;
 }
@@ -492,7 +497,8 @@ __device__ __forceinline__ float quotient_rn(float num, float den) {
 }
 
 __device__ __forceinline__ float bisect(const Col& s1, const Col& s2) {
-  const float q = quotient_rn(__fsub_rn(s2.d, s1.d), __fsub_rn(s2.r2, s1.r2));
+  const float2 df = sub2(make_float2(s2.d, s2.r2), make_float2(s1.d, s1.r2));
+  const float q = quotient_rn(df.x, df.y);
   return __fadd_rn(__fmul_rn(__fadd_rn(s1.r2, s2.r2), 0.25f), q);
 }
 
@@ -734,12 +740,12 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
       cur.e = a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u);
       cur.r2 = row2f;
       {
-        const float dc = biased(v >> 20) - C0;
         if (!kXPass && kOwnA) {
+          const float dc = biased(v >> 20) - C0;
           cur.d = __fmul_rn(dc, dc);
         } else {
-          const float da = biased(a) - A0;
-          cur.d = __fmaf_rn(da, da, __fmul_rn(dc, dc));
+          const float2 dd = sub2(make_float2(biased(a), biased(v >> 20)), make_float2(A0, C0));
+          cur.d = __fmaf_rn(dd.x, dd.x, __fmul_rn(dd.y, dd.y));
         }
       }
       // Before a row's pops the top is the site of the last earlier row that
