@@ -439,26 +439,32 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b
 
 // A site in the column frame: packed entry (a | row << 10 | c << 20) plus
 // twice its row and its squared offset from the column as exact floats
-// (offset < 2^21).  A0, C0: the column's coordinates, biased.  kOwnA: the
-// site's a equals the column's, so the offset is dc^2 alone (the same float:
-// da = 0 exactly).  That holds in pass Y when pass Z took the occupancy-bit
-// route (every input voxel UNINIT or its own site): pass Z's sites then share
-// the voxel's x and y.
+// (offset < 2^21).  A0, C0: the column's coordinates, biased.
+//
+// kOwn: pass Z took the occupancy-bit route (every input voxel UNINIT or its
+// own site), so every site pass Y reads shares its voxel's x and y, and every
+// site pass X reads shares its voxel's x.  The map's own entries then serve as
+// stack entries: pass Y's frame order is the map order, its site's row field
+// already equals the row and its a offset is 0 (the squared offset is dc^2
+// alone, the same float); pass X keeps map order (row = x in bits 0-9, a = y
+// in bits 10-19), so its sites go back to the map unchanged.
 struct Col {
   uint32_t e;
   float r2, d;
 };
 
-template <bool kOwnA>
+template <bool kXPass, bool kOwn>
 __device__ __forceinline__ Col make_col(uint32_t e, float A0, float C0) {
+  constexpr bool kMapX = kXPass && kOwn;
   Col s;
   s.e = e;
-  s.r2 = biased((e >> 9) & 0x7feu) - kBias;  // 2 * row
-  if (kOwnA) {
+  s.r2 = biased(kMapX ? ((e << 1) & 0x7feu) : ((e >> 9) & 0x7feu)) - kBias;  // 2 * row
+  if (!kXPass && kOwn) {
     const float dc = biased(e >> 20) - C0;
     s.d = __fmul_rn(dc, dc);
   } else {
-    const float2 dd = sub2(make_float2(biased(e & 0x3ffu), biased(e >> 20)), make_float2(A0, C0));
+    const float2 dd =
+        sub2(make_float2(biased(kMapX ? ((e >> 10) & 0x3ffu) : (e & 0x3ffu)), biased(e >> 20)), make_float2(A0, C0));
     s.d = __fmaf_rn(dd.x, dd.x, __fmul_rn(dd.y, dd.y));  // exact: integers below 2^21
   }
   return s;
@@ -563,7 +569,7 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint2* ring
   const uint32_t ce = __shfl_sync(kFullMask, cur.e, o);
   const float oA0 = __shfl_sync(kFullMask, A0, o);  // lane o's column, biased
   const float oC0 = __shfl_sync(kFullMask, C0, o);
-  const Col oc = make_col<kOwnA>(ce, oA0, oC0);
+  const Col oc = make_col<false, kOwnA>(ce, oA0, oC0);
   uint2* ring = ring_base + o;
   const uint2* gstk = gstk_base + (size_t)o * L;
   for (int start = on - 1;; start -= 31) {
@@ -579,7 +585,7 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint2* ring
       e = p.x;
       I = __uint_as_float(p.y);
     }
-    const Col ec = make_col<kOwnA>(e, oA0, oC0);
+    const Col ec = make_col<false, kOwnA>(e, oA0, oC0);
     const float b = bisect(ec, oc);
     const bool keep = j <= 0 || I < b;
     const unsigned kb = __ballot_sync(kFullMask, keep) & 0x7fffffffu;
@@ -601,7 +607,7 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint2* ring
       if (lane == o) {
         n = start - t + 1;
         lo = min(lo, new_lo);
-        top = make_col<kOwnA>(e_top, oA0, oC0);
+        top = make_col<false, kOwnA>(e_top, oA0, oC0);
         top_i = i_top;
         i2 = b_top;
         sec_e = e_sec;
@@ -659,8 +665,8 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
 // Sweep); wbase = the warp's kWarpWords of shared memory; stack = L * 64
 // words of workspace: entry d of lane l is the pair (site, bisector with the
 // entry below) at ((uint2*)stack)[l * L + d] -- each lane's stack contiguous,
-// so its spills, refills and window reads fill whole sectors.  kOwnA (pass
-// Y only): every site's a equals its column's (see make_col).
+// so its spills, refills and window reads fill whole sectors.  kOwnA: pass Z
+// took the occupancy-bit route (make_col's kOwn).
 template <bool kXPass, int kRows, bool kOwnA = false>
 __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t* __restrict__ stack, int X, int Y,
                                            int Z, long long item, uint32_t* wbase) {
@@ -737,7 +743,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
       const uint32_t a = kXPass ? ((v >> 10) & 0x3ffu) : (v & 0x3ffu);
       const bool has = a != kUninit;
       Col cur;
-      cur.e = a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u);
+      cur.e = kOwnA ? v : (a | ((uint32_t)(r0 + r) << 10) | (v & 0xFFF00000u));
       cur.r2 = row2f;
       {
         if (!kXPass && kOwnA) {
@@ -761,7 +767,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
               break;
             }
             --n;
-            top = make_col<!kXPass && kOwnA>(sec_e, A0, C0);
+            top = make_col<kXPass, kOwnA>(sec_e, A0, C0);
             top_i = sec_i;
             // The entry below the new top: its ring slot, or below the ring
             // the workspace (a predicated load; no divergent branch).  With
@@ -855,7 +861,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   // The voxel value a top entry gives, in map order (pass X swaps the
   // entry's first two fields back).
   auto out_of = [](uint32_t te) -> uint32_t {
-    return kXPass ? (((te >> 10) & 0x3ffu) | ((te & 0x3ffu) << 10) | (te & 0xFFF00000u)) : te;
+    return (kXPass && !kOwnA) ? (((te >> 10) & 0x3ffu) | ((te & 0x3ffu) << 10) | (te & 0xFFF00000u)) : te;
   };
   uint32_t out = kDvUninit;
   float top_b = 0.f;  // bisector of the top with the entry below
@@ -1215,7 +1221,8 @@ __device__ __forceinline__ unsigned next_item(unsigned* head) {
 
 // sync = [done: Z words][head][err][pass Z's other-sites flag]; done, head
 // and err zeroed before the launch.  A zero flag means every site lies in its
-// own z column, and pass Y skips the zero x offset (sweep_item's kOwnA).
+// own z column, and both passes take the map's entries as stack entries
+// (sweep_item's kOwnA).
 template <int kRows>
 __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     edt_sweep_yx(uint32_t* __restrict__ map, uint32_t* __restrict__ stacks, unsigned* __restrict__ sync, int X, int Y,
@@ -1240,7 +1247,10 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     } else {
       const unsigned item = g - ny;
       item_slices(item, Y, Z, za, zb);
-      if (wait_slices(done, za, zb, X, err)) sweep_item<true, kRows>(map, stack, X, Y, Z, item, wbase);
+      if (wait_slices(done, za, zb, X, err)) {
+        if (own) sweep_item<true, kRows, true>(map, stack, X, Y, Z, item, wbase);
+        else sweep_item<true, kRows, false>(map, stack, X, Y, Z, item, wbase);
+      }
     }
     __syncwarp();
   }
@@ -1248,9 +1258,9 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
 
 // The same schedule over every map of a batch: the queue holds all maps' Y
 // items, then all maps' X items.  maps[k].sync_off locates map k's slice
-// counters in `sync`; the queue head and error word follow them.  Pass Y of a
-// map whose pass Z took the occupancy-bit route (its other-sites flag clear)
-// runs sweep_item's kOwnA form.
+// counters in `sync`; the queue head and error word follow them.  Both passes
+// of a map whose pass Z took the occupancy-bit route (its other-sites flag
+// clear) run sweep_item's kOwnA form.
 template <int kRows>
 __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
     edt_sweep_yx_batch(const BatchMap* __restrict__ maps, const long long* __restrict__ prefix_y,
@@ -1281,7 +1291,10 @@ __global__ void __launch_bounds__(SweepCfg<kRows>::kWarps * 32, 3)
       publish_slices(done, za, zb);
     } else {
       item_slices(item, m.Y, m.Z, za, zb);
-      if (wait_slices(done, za, zb, m.X, err)) sweep_item<true, kRows>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+      if (wait_slices(done, za, zb, m.X, err)) {
+        if (*batch_other(m) == 0u) sweep_item<true, kRows, true>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+        else sweep_item<true, kRows, false>(m.vox, stack, m.X, m.Y, m.Z, item, wbase);
+      }
     }
     __syncwarp();
   }
