@@ -556,13 +556,11 @@ struct SweepCfg {
 // test depends only on e_j, I_j and cur, so lane t tests depth start - t and
 // the first kept depth (lowest t) is exactly where the sequential loop stops.
 // Lane 31 only supplies the entry below lane 30's, so a round covers 31
-// depths.  All 32 lanes call this; only lane o's state changes (sec_e: the
-// packed entry below the top, decoded only when it becomes the top).  Pass Y
+// depths.  All 32 lanes call this; only lane o's state changes.  Pass Y
 // only.
 template <class Cfg, bool kOwnA>
 __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint2* ring_base, const uint2* gstk_base, int L,
-                                          int& n, int& lo, const Col& cur, Col& top, float& top_i, uint32_t& sec_e,
-                                          float& sec_i, float& i2) {
+                                          int& n, int& lo, const Col& cur, Col& top, float& top_i, float& i2) {
   const int lane = threadIdx.x & 31;
   const int on = __shfl_sync(kFullMask, n, o);
   const int olo = __shfl_sync(kFullMask, lo, o);
@@ -602,16 +600,12 @@ __device__ __forceinline__ void coop_pops(int o, float A0, float C0, uint2* ring
       const uint32_t e_top = __shfl_sync(kFullMask, e, t);
       const float i_top = __shfl_sync(kFullMask, I, t);
       const float b_top = __shfl_sync(kFullMask, b, t);
-      const uint32_t e_sec = __shfl_sync(kFullMask, e, t + 1);
-      const float i_sec = __shfl_sync(kFullMask, I, t + 1);
       if (lane == o) {
         n = start - t + 1;
         lo = min(lo, new_lo);
         top = make_col<false, kOwnA>(e_top, oA0, oC0);
         top_i = i_top;
         i2 = b_top;
-        sec_e = e_sec;
-        sec_i = i_sec;
       }
       __syncwarp();  // the refill before lane o's next ring access
       return;
@@ -726,11 +720,10 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   int n = 0;      // stack depth
   int lo = 0;     // lowest depth in the ring
   int spill = 0;  // depths below it have their workspace copy
-  // The top decoded; the entry below it packed (decoded when a pop makes it
-  // the top).  top_i = bisector(second, top), sec_i = bisector(third, second).
+  // The top decoded, with top_i = bisector(second, top); a pop reads the new
+  // top (site, bisector) from the ring, or below the ring from the workspace.
   Col top{0u, 0.f, 0.f};
-  uint32_t sec_e = 0u;
-  float top_i = 0.f, sec_i = 0.f;
+  float top_i = 0.f;
   for (int c = 0; c < nchunks; ++c) {
     cp_async_wait1();
     __syncwarp();
@@ -767,20 +760,13 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
               break;
             }
             --n;
-            top = make_col<kXPass, kOwnA>(sec_e, A0, C0);
-            top_i = sec_i;
-            // The entry below the new top: its ring slot, or below the ring
-            // the workspace (a predicated load; no divergent branch).  With
-            // n < 2 it is never read: the next push replaces it.
-            const int d = n - 2;
-            const uint2 rq = ring[(d & (Cfg::kRing - 1)) * 32];
-            sec_e = rq.x;
-            sec_i = __uint_as_float(rq.y);
-            if (d >= 0 && d < lo) {
-              const uint2 p = gstk[d];
-              sec_e = p.x;
-              sec_i = __uint_as_float(p.y);
-            }
+            // the new top: its ring slot, or below the ring the workspace (a
+            // predicated load; no divergent branch)
+            const int d = n - 1;
+            uint2 q = ring[(d & (Cfg::kRing - 1)) * 32];
+            if (d < lo) q = gstk[d];
+            top = make_col<kXPass, kOwnA>(q.x, A0, C0);
+            top_i = __uint_as_float(q.y);
             i2 = bisect(top, cur);
           }
         }
@@ -792,7 +778,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
             const int o = __ffs(deep_lanes) - 1;
             deep_lanes &= deep_lanes - 1;
             coop_pops<Cfg, kOwnA>(o, A0, C0, reinterpret_cast<uint2*>(wbase + 2 * Cfg::kTileWords), gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
-                           sec_e, sec_i, i2);
+                           i2);
           }
         }
         if (has) {
@@ -809,8 +795,6 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           ring[slot] = make_uint2(cur.e, __float_as_uint(i2));
           lo = max(lo, ev + 1);
           ++n;
-          sec_e = top.e;
-          sec_i = top_i;
           top = cur;
           top_i = i2;
         }
