@@ -625,7 +625,15 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
     if (vec16) {  // one slice, 32 lanes, 16-byte aligned: 8 lanes per row
       const uint32_t* src = s.map + s.col0 + (uint64_t)r0 * s.X;
       const int part = lane & 7;
-      for (int r = lane >> 3; r < rows; r += 4) cp_async16(tile + r * 32 + part * 4, src + (uint64_t)r * s.X + part * 4);
+      if (rows == kRows) {  // a whole chunk: the copies unrolled
+#pragma unroll
+        for (int k = 0; k < kRows / 4; ++k) {
+          const int r = (lane >> 3) + 4 * k;
+          cp_async16(tile + r * 32 + part * 4, src + (uint64_t)r * s.X + part * 4);
+        }
+      } else {
+        for (int r = lane >> 3; r < rows; r += 4) cp_async16(tile + r * 32 + part * 4, src + (uint64_t)r * s.X + part * 4);
+      }
     } else if (lane < s.valid) {
       const uint32_t* src = s.map + s.col + (uint64_t)r0 * s.X;
       for (int r = 0; r < rows; ++r) cp_async4(tile + r * 32 + lane, src + (uint64_t)r * s.X);
@@ -638,9 +646,17 @@ __device__ __forceinline__ void stage_chunk(uint32_t* tile, const Sweep& s, int 
     if (s.one_slice) {  // rows t are X apart
       if (xl < rows) {
         const uint32_t* src = s.map + s.col0 + r0 + xl;
-        for (int t = t0; t < 32; t += 32 / kRows) {
-          if (t < s.valid) cp_async4(tile + xl * 33 + t, src + (uint64_t)t * s.X);
-          else tile[xl * 33 + t] = kDvUninit;
+        if (s.valid == 32) {  // every column live: the copies unrolled
+#pragma unroll
+          for (int k = 0; k < kRows; ++k) {
+            const int t = t0 + k * (32 / kRows);
+            cp_async4(tile + xl * 33 + t, src + (uint64_t)t * s.X);
+          }
+        } else {
+          for (int t = t0; t < 32; t += 32 / kRows) {
+            if (t < s.valid) cp_async4(tile + xl * 33 + t, src + (uint64_t)t * s.X);
+            else tile[xl * 33 + t] = kDvUninit;
+          }
         }
       }
     } else {
@@ -788,7 +804,7 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           lo = min(lo, n);
           const int slot = (n & (Cfg::kRing - 1)) * 32;  // push the current site
           const int ev = n - Cfg::kRing;             // the depth this slot held
-          if (ev >= lo && ev >= spill) {             // evicted before it reached the workspace
+          if (ev >= spill) {  // evicted before it reached the workspace (spill >= lo always)
             gstk[ev] = ring[slot];
             spill = ev + 1;
           }
@@ -881,9 +897,15 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
       __syncwarp();
       const int xl = lane >> 2, t0 = lane & 3;
       if (s.one_slice) {  // rows t are X apart
-        if (xl < rows)
-          for (int t = t0; t < s.valid; t += 4)
-            map[(uint64_t)s.col0 + (uint64_t)t * X + r0 + xl] = xstage[xl * Cfg::kStagePitch + t];
+        if (xl < rows) {
+          uint32_t* dst = map + (uint64_t)s.col0 + r0 + xl;
+          if (s.valid == 32) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) dst[(uint64_t)(t0 + 4 * k) * X] = xstage[xl * Cfg::kStagePitch + t0 + 4 * k];
+          } else {
+            for (int t = t0; t < s.valid; t += 4) dst[(uint64_t)t * X] = xstage[xl * Cfg::kStagePitch + t];
+          }
+        }
       } else {
         for (int t = t0; t < 32; t += 4) {  // the same trip count on every lane (row_start shuffles)
           const uint32_t rs = row_start(s, t);
