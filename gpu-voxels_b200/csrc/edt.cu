@@ -547,6 +547,7 @@ struct SweepCfg {
   static constexpr int kWarpWords = kPhase2Words > kPhase3Words ? kPhase2Words : kPhase3Words;
   static_assert((kWin & (kWin - 1)) == 0, "window slots are depth mod kWin");
   static_assert((kRing & (kRing - 1)) == 0, "ring slots are depth mod kRing");
+  static_assert(kTileWords % 4 == 0, "the second tile and the ring take 16-byte copies and 8-byte slots");
   static_assert(kStageWords % 2 == 0 && kWarpWords % 2 == 0, "8-byte window entries need even offsets");
 };
 
