@@ -794,8 +794,8 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
           while (deep_lanes) {
             const int o = __ffs(deep_lanes) - 1;
             deep_lanes &= deep_lanes - 1;
-            coop_pops<Cfg, kOwnA>(o, A0, C0, reinterpret_cast<uint2*>(wbase + 2 * Cfg::kTileWords), gstk - (size_t)lane * L, L, n, lo, cur, top, top_i,
-                           i2);
+            coop_pops<Cfg, kOwnA>(o, A0, C0, reinterpret_cast<uint2*>(wbase + 2 * Cfg::kTileWords),
+                                  gstk - (size_t)lane * L, L, n, lo, cur, top, top_i, i2);
           }
         }
         if (has) {
@@ -859,8 +859,8 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
     }
     return win[(d & (kWin - 1)) * 32];
   };
-  // The voxel value a top entry gives, in map order (pass X swaps the
-  // entry's first two fields back).
+  // The voxel value a top entry gives, in map order (pass X in its general
+  // form swaps the entry's first two fields back).
   auto out_of = [](uint32_t te) -> uint32_t {
     return (kXPass && !kOwnA) ? (((te >> 10) & 0x3ffu) | ((te & 0x3ffu) << 10) | (te & 0xFFF00000u)) : te;
   };
