@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(256) lists_collide_bits_kernel(const uint32_t*
                                                                  uint32_t* __restrict__ lvox,
                                                                  const uint64_t* __restrict__ offsets, uint32_t n_lists,
                                                                  uint64_t n_total, const uint32_t* __restrict__ bits,
-                                                                 uint64_t map_n, int mark, int ids16,
+                                                                 uint64_t map_n, int mark,
                                                                  unsigned long long* __restrict__ counts) {
   constexpr int kE = 4;       // entries per lane and group
   constexpr int kG = 32 * kE;
@@ -296,15 +296,12 @@ __global__ void __launch_bounds__(256) lists_collide_bits_kernel(const uint32_t*
     }
     list = lo;
   }
+  // Entry e of lane l in group g is g * kG + e * 32 + l: each load covers 32
+  // consecutive entries of a sorted list, so its bit lookups fall in few lines.
   auto load_ids = [&](uint64_t g, uint32_t (&j)[kE]) {
-    const uint64_t k0 = g * kG + (uint64_t)lane * kE;
-    if (g < g_end && ids16 && k0 + kE <= n_total) {
-      const uint4 q = __ldg(reinterpret_cast<const uint4*>(ids + k0));
-      j[0] = q.x; j[1] = q.y; j[2] = q.z; j[3] = q.w;
-    } else {
+    const uint64_t k0 = g * kG + (uint64_t)lane;
 #pragma unroll
-      for (int e = 0; e < kE; ++e) j[e] = (g < g_end && k0 + e < n_total) ? __ldg(ids + k0 + e) : 0xFFFFFFFFu;
-    }
+    for (int e = 0; e < kE; ++e) j[e] = (g < g_end && k0 + e * 32 < n_total) ? __ldg(ids + k0 + e * 32) : 0xFFFFFFFFu;
   };
   int queued = 0;  // warp-uniform
   uint32_t jn[kE];
@@ -318,7 +315,7 @@ __global__ void __launch_bounds__(256) lists_collide_bits_kernel(const uint32_t*
 #pragma unroll
     for (int e = 0; e < kE; ++e)
       occ |= (unsigned)(j[e] < map_n && ((__ldg(bits + (j[e] >> 5)) >> (j[e] & 31)) & 1u)) << e;
-    const uint64_t k0 = g * kG + (uint64_t)lane * kE;
+    const uint64_t k0 = g * kG + (uint64_t)lane;
 #pragma unroll
     for (int e = 0; e < kE; ++e) {
       const bool c = (occ >> e) & 1u;
@@ -326,7 +323,7 @@ __global__ void __launch_bounds__(256) lists_collide_bits_kernel(const uint32_t*
       if (cm) {  // append this round's candidates to the queue
         if (c) {
           const int slot = queued + __popc(cm & ((1u << lane) - 1u));
-          cand_k[slot] = k0 + e;
+          cand_k[slot] = k0 + e * 32;
           cand_lb[slot] = list;
         }
         queued += __popc(cm);
@@ -489,9 +486,8 @@ cudaError_t launch_lists_collide_map(const uint32_t* d_ids, uint8_t* d_vox, cons
                                                                            map_n, d_occ);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const unsigned grid = std::min(grid_cap(n_total, 8 * 128), resident_blocks<lists_collide_bits_kernel>());
-    const int ids16 = (reinterpret_cast<uintptr_t>(d_ids) & 15u) == 0;
     lists_collide_bits_kernel<<<grid, 256, 0, s>>>(d_ids, reinterpret_cast<uint32_t*>(d_vox), d_offsets, n_lists,
-                                                   n_total, d_occ, map_n, mark, ids16, d_counts);
+                                                   n_total, d_occ, map_n, mark, d_counts);
     return cudaGetLastError();
   }
   const unsigned grid = std::min(grid_cap(n_total, 8 * 16), resident_blocks<lists_collide_map_kernel>());
