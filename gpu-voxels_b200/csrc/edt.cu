@@ -723,14 +723,15 @@ __device__ __forceinline__ void sweep_item(uint32_t* __restrict__ map, uint32_t*
   // Rows advance in lockstep (the per-row work runs on all 32 lanes); the pops
   // a row triggers run as a loop over just the lanes that need them.  The ring
   // keeps each entry's bisector with the entry below, so a pop reads the new
-  // (second, bisector) pair instead of recomputing it.
+  // top's (site, bisector) pair instead of recomputing the bisector.
   stage_chunk<kXPass, kRows>(tile0, s, 0, vec16);
   cp_async_commit();
   if (nchunks > 1) stage_chunk<kXPass, kRows>(tile1, s, 1, vec16);
   cp_async_commit();
 
   // The stack lives in the ring (depths [lo, n)) and in the workspace
-  // (depths [0, spill)); lo <= spill whenever both ranges matter.  An entry
+  // (depths [0, spill)); lo <= spill always (so a depth below the ring has its
+  // workspace copy, and the eviction test needs only spill).  An entry
   // is written to the workspace only when a push evicts it from the ring (and
   // the ring's remainder once phase 2 ends), so entries pushed and popped
   // within the ring's reach never leave the chip.
